@@ -1,0 +1,67 @@
+/*
+ * so3gpu.h -- device-pointer extension API of libso3gpu (B200, sm_100a).
+ *
+ * The drop-in entry points of so3_core.h / so3_conv.h accept host or device
+ * pointers and block until the result is in the caller's buffer.  This API
+ * is the asynchronous form: device pointers only, work enqueued on the
+ * context's CUDA stream, no host synchronisation.  Resident per-device
+ * resources (Wigner Delta(pi/2) tables, FFT plans, index tables) are shared
+ * by all contexts of a device; each context owns its own scratch, so contexts
+ * on different streams may run concurrently.
+ *
+ * Status codes: 0 success, 1 invalid parameter, 2 CUDA error, 3 unsupported
+ * configuration, 4 out of device memory.  The message of the last failure on
+ * the calling thread is so3gpu_last_error().
+ */
+#ifndef SO3GPU_H
+#define SO3GPU_H
+
+#include <stddef.h>
+
+#include "so3/so3_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct so3gpu_context so3gpu_context;
+
+/* stream: a cudaStream_t (NULL = legacy default stream). */
+so3gpu_context *so3gpu_context_create(int device, void *stream);
+void so3gpu_context_destroy(so3gpu_context *ctx);
+int so3gpu_context_set_stream(so3gpu_context *ctx, void *stream);
+
+/* Builds the resident tables and plans the transform with these parameters
+ * needs (blocking).  Call it before capturing transforms in a CUDA graph. */
+int so3gpu_prepare(so3gpu_context *ctx, const so3_parameters_t *parameters);
+/* Device scratch (bytes) one transform with these parameters uses. */
+size_t so3gpu_workspace_size(const so3_parameters_t *parameters);
+
+/* Same transforms as so3_core_*_via_ssht, on device pointers. */
+int so3gpu_inverse(so3gpu_context *ctx, void *f, const void *flmn, const so3_parameters_t *parameters);
+int so3gpu_forward(so3gpu_context *ctx, void *flmn, const void *f, const so3_parameters_t *parameters);
+int so3gpu_inverse_real(so3gpu_context *ctx, double *f, const void *flmn,
+                        const so3_parameters_t *parameters);
+int so3gpu_forward_real(so3gpu_context *ctx, void *flmn, const double *f,
+                        const so3_parameters_t *parameters);
+
+/* Same as so3_conv_s2toso3_harmonic_convolution / so3_conv_harmonic_convolution. */
+int so3gpu_s2toso3_harmonic_convolution(so3gpu_context *ctx, void *hlmn, const so3_parameters_t *h_parameters,
+                                        const void *flm, const void *glm);
+int so3gpu_harmonic_convolution(so3gpu_context *ctx, void *hlmn, const so3_parameters_t *h_parameters,
+                                const void *flmn, const so3_parameters_t *f_parameters, const void *glmn,
+                                const so3_parameters_t *g_parameters);
+
+/* Diagnostics. */
+int so3gpu_last_status(void);
+const char *so3gpu_last_error(void);
+/* mode 0 (default): errors in the drop-in entry points print and exit(1) like
+ * the reference; mode 1: they record the status and return. */
+void so3gpu_set_error_mode(int mode);
+/* Number of kernels this library has launched since load (all devices). */
+long long so3gpu_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,153 @@
+// Internal declarations shared by the CUDA translation units of libso3gpu.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstddef>
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "fft_core.cuh"
+#include "so3/so3_types.h"
+
+namespace so3g {
+
+// ---------------------------------------------------------------- errors
+// Status codes returned by every internal entry point.
+enum Status : int {
+  kOk = 0,
+  kInvalidParameter = 1,
+  kCudaError = 2,
+  kUnsupported = 3,
+  kOutOfMemory = 4,
+};
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);  // records msg, returns code
+#define SO3G_CUDA(call)                                                               \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess)                                                            \
+      return ::so3g::fail(::so3g::kCudaError, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// Counter of kernel launches issued by this library (all devices).
+extern std::atomic<long long> g_launches;
+#define SO3G_LAUNCHED() (::so3g::g_launches.fetch_add(1, std::memory_order_relaxed))
+
+// ---------------------------------------------------------------- geometry
+// Scratch layout: W[plane][row][col], complex FP64, col stride 1, row stride
+// RS (>= 2L, multiple of 8 so every row starts on a 128-byte boundary), plane
+// stride PS = RS * nb.  Plane index = n + plane0 (plane0 = N-1 for complex
+// signals, 0 for real ones, which keep n >= 0 only).  Column index c = m+L-1.
+struct Geometry {
+  int L, N, L0;
+  int mw;       // 1 MW, 0 MWSS
+  int real;     // reality flag of the transform being run
+  int na, nb;   // alpha / beta samples
+  int P;        // DFT length over alpha and over the extended beta circle (= na)
+  int ng;       // gamma samples 2N-1
+  int nplanes;  // 2N-1 (complex) or N (real)
+  int plane0;
+  long RS, PS;
+  int Pc;       // weight-convolution length (power of two >= 4L-3)
+};
+Geometry make_geometry(const so3_parameters_t& p, int real);
+
+// Plane index -> "virtual base" offset into the caller's flmn array, such that
+// element (l, m, n) sits at base[n] + l*l + l + m (entries with l < |n| are
+// absent in compact storage).  Encodes storage and n-order.
+std::vector<long long> block_bases(const so3_parameters_t& p, int real);
+
+// ---------------------------------------------------------------- tables
+// Quarter Delta(pi/2) planes of every degree l < Lcap, plane l at offset
+// l(l+1)(2l+1)/6, row-major (m' rows, m columns, both 0..l).  Planes do not
+// depend on the band limit, so one table serves every L <= Lcap.
+struct DlTable {
+  int Lcap = 0;
+  double* d = nullptr;
+};
+__host__ __device__ inline long long dl_plane_offset(int l) {
+  return (long long)l * (l + 1) * (2 * l + 1) / 6;
+}
+
+struct DevPlan {
+  FftPlan plan{};
+  double2* mem = nullptr;  // owns roots/mroots/chirp/kern
+};
+
+struct Device {
+  int device = 0;
+  std::mutex mu;
+  DlTable dl[2];                                 // per dl_method
+  std::map<int, std::unique_ptr<DevPlan>> ffts;  // by length
+  std::map<int, double2*> conv_kernels;          // weight kernel by L (MW/MWSS identical)
+  std::map<std::string, long long*> bases;       // block bases by parameter key
+};
+
+// Grow-only device scratch owned by one caller context (never shared between
+// contexts, so contexts on different streams do not race).
+struct Workspace {
+  void* ws = nullptr;
+  size_t ws_bytes = 0;
+};
+Device* device_state(int device);  // lazily created per CUDA device
+
+int ensure_dl(Device* D, int L, int method, cudaStream_t s, const double** out);
+int ensure_fft(Device* D, int n, FftPlan* out);
+int ensure_conv_kernel(Device* D, const Geometry& g, const double2** out);
+int ensure_bases(Device* D, const so3_parameters_t& p, int real, const long long** out);
+int ensure_ws(Workspace* W, size_t bytes, void** out);
+size_t workspace_bytes(const so3_parameters_t& p, int real);
+
+// ---------------------------------------------------------------- launches
+int launch_build_dl_trapani(double* table, int L0cap, int Lcap, cudaStream_t s);
+int launch_build_dl_risbo(double* table, int Lcap, double* work, cudaStream_t s);
+
+struct ModeInfo {
+  int n_mode;  // so3_n_mode_t
+  int N;
+};
+__host__ __device__ inline bool plane_skipped(int mode, int N, int n) {
+  if (mode == SO3_N_MODE_EVEN) return (n & 1) != 0;
+  if (mode == SO3_N_MODE_ODD) return (n & 1) == 0;
+  if (mode == SO3_N_MODE_MAXIMUM) return (n < 0 ? -n : n) < N - 1;
+  return false;
+}
+
+int launch_inverse_contract(const Geometry& g, int n_mode, const double2* flmn, const long long* bases,
+                            const double* dl, double2* W, int sym_n0, cudaStream_t s);
+int launch_forward_contract(const Geometry& g, int n_mode, const double2* W, const long long* bases,
+                            const double* dl, double2* flmn, int storage_compact, cudaStream_t s);
+
+int launch_inv_beta(const Geometry& g, const FftPlan& pP, double2* W, cudaStream_t s);
+int launch_inv_alpha(const Geometry& g, const FftPlan& pP, double2* W, cudaStream_t s);
+int launch_inv_gamma(const Geometry& g, const FftPlan& pg, const double2* W, void* f, cudaStream_t s);
+int launch_fwd_gamma(const Geometry& g, const FftPlan& pg, const void* f, double2* W, cudaStream_t s);
+int launch_fwd_alpha(const Geometry& g, const FftPlan& pP, double2* W, cudaStream_t s);
+int launch_fwd_beta_conv(const Geometry& g, const FftPlan& pP, const FftPlan& pc, const double2* wr,
+                         double2* W, cudaStream_t s);
+
+int launch_s2toso3(const so3_parameters_t& hp, const long long* bases, const double2* flm, const double2* glm,
+                   double2* hlmn, cudaStream_t s);
+int launch_harmonic_convolution(const so3_parameters_t& hp, const so3_parameters_t& fp,
+                                const so3_parameters_t& gp, const long long* hb, const long long* fb,
+                                const long long* gb, const double2* flmn, const double2* glmn, double2* hlmn,
+                                cudaStream_t s);
+int launch_zero(void* p, size_t bytes, cudaStream_t s);
+
+// ---------------------------------------------------------------- drivers
+// Lock-protected creation of the per-device read-only resources a transform
+// with parameters p needs; safe to call before stream capture.
+int prepare(Device* D, const so3_parameters_t& p, int real, cudaStream_t s);
+int run_inverse(Device* D, Workspace* wk, const so3_parameters_t& p, const void* flmn_d, void* f_d, int real,
+                cudaStream_t s);
+int run_forward(Device* D, Workspace* wk, const so3_parameters_t& p, const void* f_d, void* flmn_d, int real,
+                cudaStream_t s);
+const std::string& last_error();
+int validate(const so3_parameters_t& p, int real);
+
+}  // namespace so3g

@@ -52,6 +52,18 @@ int so3gpu_harmonic_convolution(so3gpu_context *ctx, void *hlmn, const so3_param
                                 const void *flmn, const so3_parameters_t *f_parameters, const void *glmn,
                                 const so3_parameters_t *g_parameters);
 
+/* Per-stage timing with CUDA events on the context's stream (off by
+ * default).  so3gpu_stage_times waits for the recorded events, returns the
+ * accumulated milliseconds and launch counts per stage since the previous
+ * call (stages: 0 inverse contraction, 1 inverse beta, 2 inverse alpha,
+ * 3 inverse gamma, 4 forward gamma, 5 forward alpha, 6 forward beta and
+ * quadrature convolution, 7 forward contraction) and resets them. */
+int so3gpu_stage_timing(so3gpu_context *ctx, int enable);
+int so3gpu_stage_times(so3gpu_context *ctx, double *total_ms, long long *counts, int n);
+/* Measured FP64 fused multiply-add throughput of the device in TFLOP/s
+ * (2 flops per FMA), from a register-resident FMA chain kernel. */
+double so3gpu_measure_fp64_peak(int device);
+
 /* Diagnostics. */
 int so3gpu_last_status(void);
 const char *so3gpu_last_error(void);

@@ -82,6 +82,9 @@ SIGNATURES = {
     "so3gpu_forward_real": (_I, [_VP, _VP, _VP, _P]),
     "so3gpu_s2toso3_harmonic_convolution": (_I, [_VP, _VP, _P, _VP, _VP]),
     "so3gpu_harmonic_convolution": (_I, [_VP, _VP, _P, _VP, _P, _VP, _P]),
+    "so3gpu_stage_timing": (_I, [_VP, _I]),
+    "so3gpu_stage_times": (_I, [_VP, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong), _I]),
+    "so3gpu_measure_fp64_peak": (ctypes.c_double, [_I]),
     "so3gpu_last_status": (_I, []),
     "so3gpu_last_error": (ctypes.c_char_p, []),
     "so3gpu_set_error_mode": (None, [_I]),

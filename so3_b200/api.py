@@ -72,6 +72,20 @@ def _s(p) -> Params:
     return p.to_struct() if isinstance(p, SO3Parameters) else p
 
 
+def _checked(p) -> Params:
+    """Struct for a transform call.  The C sampling helpers exit the process on
+    an invalid sampling scheme, storage or n-order (reference behaviour), so
+    the Python layer rejects those first."""
+    q = _s(p)
+    if q.sampling_scheme not in (0, 1):
+        raise SO3Error("status 1: Invalid sampling scheme.")
+    if q.storage not in (0, 1):
+        raise SO3Error("status 1: Invalid storage method.")
+    if q.n_order not in (0, 1):
+        raise SO3Error("status 1: Invalid n-order.")
+    return q
+
+
 def _ptr(a: np.ndarray):
     return a.ctypes.data_as(ctypes.c_void_p)
 
@@ -154,7 +168,7 @@ def is_elmn_non_zero(el, m, n, p) -> bool:
 # ------------------------------------------------------------ transforms (host)
 def inverse(flmn: np.ndarray, p) -> np.ndarray:
     """bindings.pyx:315-336: flmn -> samples (complex, or real when p.reality)."""
-    q = _s(p)
+    q = _checked(p)
     lib = _lib.load()
     flmn = np.ascontiguousarray(flmn, dtype=np.complex128)
     if q.reality:
@@ -169,7 +183,7 @@ def inverse(flmn: np.ndarray, p) -> np.ndarray:
 
 def forward(f: np.ndarray, p) -> np.ndarray:
     """bindings.pyx:338-357: samples -> flmn; a real array needs p.reality."""
-    q = _s(p)
+    q = _checked(p)
     lib = _lib.load()
     flmn = np.zeros(flmn_size(q), np.complex128)
     if np.isrealobj(f):
@@ -292,6 +306,29 @@ class Context:
                                                          glm.data_ptr()):
             _lib.check("so3gpu_s2toso3_harmonic_convolution")
         return out
+
+
+    def stage_timing(self, enable: bool = True):
+        self._lib.so3gpu_stage_timing(self._c, 1 if enable else 0)
+
+    def stage_times(self):
+        """{stage name: (total ms, launches)} since the previous call."""
+        ms = (ctypes.c_double * 16)()
+        cnt = (ctypes.c_longlong * 16)()
+        if self._lib.so3gpu_stage_times(self._c, ms, cnt, 16):
+            _lib.check("stage_times")
+        return {name: (ms[i], cnt[i]) for i, name in enumerate(STAGES) if cnt[i]}
+
+
+STAGES = ["inv_contract", "inv_beta", "inv_alpha", "inv_gamma", "fwd_gamma", "fwd_alpha", "fwd_beta_conv",
+          "fwd_contract"]
+
+
+def measure_fp64_peak(device: int = 0) -> float:
+    """Measured FP64 FMA throughput (TFLOP/s) of the device."""
+    v = _lib.load().so3gpu_measure_fp64_peak(device)
+    _lib.check("measure_fp64_peak")
+    return v
 
 
 def workspace_size(p) -> int:

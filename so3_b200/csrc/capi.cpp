@@ -436,6 +436,36 @@ int so3gpu_harmonic_convolution(so3gpu_context* c, void* hlmn, const so3_paramet
   return t_status = rc;
 }
 
+int so3gpu_stage_timing(so3gpu_context* c, int enable) {
+  if (!c) return t_status = so3g::fail(so3g::kInvalidParameter, "null context");
+  c->wk.timer.on = enable != 0;
+  return t_status = 0;
+}
+
+int so3gpu_stage_times(so3gpu_context* c, double* total_ms, long long* counts, int n) {
+  if (!c || !total_ms || !counts) return t_status = so3g::fail(so3g::kInvalidParameter, "null argument");
+  DeviceScope ds(c->device);
+  if (int rc = so3g::timer_collect(&c->wk.timer)) return t_status = rc;
+  for (int i = 0; i < n && i < so3g::kStCount; i++) {
+    total_ms[i] = c->wk.timer.total_ms[i];
+    counts[i] = c->wk.timer.count[i];
+    c->wk.timer.total_ms[i] = 0.0;
+    c->wk.timer.count[i] = 0;
+  }
+  return t_status = 0;
+}
+
+double so3gpu_measure_fp64_peak(int device) {
+  DeviceScope ds(device);
+  double tf = 0.0;
+  if (so3g::measure_fp64_fma_rate(&tf)) {
+    t_status = so3g::kCudaError;
+    return 0.0;
+  }
+  t_status = 0;
+  return tf;
+}
+
 int so3gpu_last_status(void) { return t_status; }
 const char* so3gpu_last_error(void) { return so3g::last_error().c_str(); }
 void so3gpu_set_error_mode(int mode) { g_error_mode.store(mode ? 1 : 0); }

@@ -40,11 +40,23 @@ int run_inverse(Device* D, Workspace* wk, const so3_parameters_t& p, const void*
   if (int rc = ensure_ws(wk, workspace_bytes(p, real), &ws)) return rc;
   double2* W = static_cast<double2*>(ws);
   const int sym_n0 = real && p.N == 1;
-  if (int rc = launch_inverse_contract(r.g, p.n_mode, static_cast<const double2*>(flmn_d), r.bases, r.dl, W, sym_n0, s))
-    return rc;
-  if (int rc = launch_inv_beta(r.g, r.pP, W, s)) return rc;
-  if (int rc = launch_inv_alpha(r.g, r.pP, W, s)) return rc;
-  return launch_inv_gamma(r.g, r.pg, W, f_d, s);
+  StageTimer* T = &wk->timer;
+  cudaEvent_t ev;
+  int rc;
+  timer_begin(T, s, &ev);
+  rc = launch_inverse_contract(r.g, p.n_mode, static_cast<const double2*>(flmn_d), r.bases, r.dl, W, sym_n0, s);
+  if (rc) return rc;
+  timer_end(T, s, kStInvContract, ev);
+  timer_begin(T, s, &ev);
+  if ((rc = launch_inv_beta(r.g, r.pP, W, s))) return rc;
+  timer_end(T, s, kStInvBeta, ev);
+  timer_begin(T, s, &ev);
+  if ((rc = launch_inv_alpha(r.g, r.pP, W, s))) return rc;
+  timer_end(T, s, kStInvAlpha, ev);
+  timer_begin(T, s, &ev);
+  if ((rc = launch_inv_gamma(r.g, r.pg, W, f_d, s))) return rc;
+  timer_end(T, s, kStInvGamma, ev);
+  return kOk;
 }
 
 int run_forward(Device* D, Workspace* wk, const so3_parameters_t& p, const void* f_d, void* flmn_d, int real,
@@ -54,11 +66,24 @@ int run_forward(Device* D, Workspace* wk, const so3_parameters_t& p, const void*
   void* ws = nullptr;
   if (int rc = ensure_ws(wk, workspace_bytes(p, real), &ws)) return rc;
   double2* W = static_cast<double2*>(ws);
-  if (int rc = launch_fwd_gamma(r.g, r.pg, f_d, W, s)) return rc;
-  if (int rc = launch_fwd_alpha(r.g, r.pP, W, s)) return rc;
-  if (int rc = launch_fwd_beta_conv(r.g, r.pP, r.pc, r.wr, W, s)) return rc;
-  return launch_forward_contract(r.g, p.n_mode, W, r.bases, r.dl, static_cast<double2*>(flmn_d),
-                                 p.storage == SO3_STORAGE_COMPACT, s);
+  StageTimer* T = &wk->timer;
+  cudaEvent_t ev;
+  int rc;
+  timer_begin(T, s, &ev);
+  if ((rc = launch_fwd_gamma(r.g, r.pg, f_d, W, s))) return rc;
+  timer_end(T, s, kStFwdGamma, ev);
+  timer_begin(T, s, &ev);
+  if ((rc = launch_fwd_alpha(r.g, r.pP, W, s))) return rc;
+  timer_end(T, s, kStFwdAlpha, ev);
+  timer_begin(T, s, &ev);
+  if ((rc = launch_fwd_beta_conv(r.g, r.pP, r.pc, r.wr, W, s))) return rc;
+  timer_end(T, s, kStFwdBetaConv, ev);
+  timer_begin(T, s, &ev);
+  rc = launch_forward_contract(r.g, p.n_mode, W, r.bases, r.dl, static_cast<double2*>(flmn_d),
+                               p.storage == SO3_STORAGE_COMPACT, s);
+  if (rc) return rc;
+  timer_end(T, s, kStFwdContract, ev);
+  return kOk;
 }
 
 }  // namespace so3g

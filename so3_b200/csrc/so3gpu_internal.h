@@ -88,11 +88,36 @@ struct Device {
   std::map<std::string, long long*> bases;       // block bases by parameter key
 };
 
+// Per-stage CUDA-event timing (optional, per caller context).
+enum Stage : int {
+  kStInvContract = 0,
+  kStInvBeta,
+  kStInvAlpha,
+  kStInvGamma,
+  kStFwdGamma,
+  kStFwdAlpha,
+  kStFwdBetaConv,
+  kStFwdContract,
+  kStCount = 16
+};
+struct StageTimer {
+  bool on = false;
+  std::vector<cudaEvent_t> pool;  // free events
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+  double total_ms[kStCount] = {};
+  long long count[kStCount] = {};
+};
+// Marks the start of `stage` on stream s; call mark_end after the launch.
+void timer_begin(StageTimer* t, cudaStream_t s, cudaEvent_t* ev);
+void timer_end(StageTimer* t, cudaStream_t s, int stage, cudaEvent_t start);
+int timer_collect(StageTimer* t);  // synchronises on the recorded events
+
 // Grow-only device scratch owned by one caller context (never shared between
 // contexts, so contexts on different streams do not race).
 struct Workspace {
   void* ws = nullptr;
   size_t ws_bytes = 0;
+  StageTimer timer;
 };
 Device* device_state(int device);  // lazily created per CUDA device
 
@@ -138,6 +163,7 @@ int launch_harmonic_convolution(const so3_parameters_t& hp, const so3_parameters
                                 const long long* gb, const double2* flmn, const double2* glmn, double2* hlmn,
                                 cudaStream_t s);
 int launch_zero(void* p, size_t bytes, cudaStream_t s);
+int measure_fp64_fma_rate(double* tflops);
 
 // ---------------------------------------------------------------- drivers
 // Lock-protected creation of the per-device read-only resources a transform

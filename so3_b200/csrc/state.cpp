@@ -120,6 +120,45 @@ Device* device_state(int device) {
   return raw;
 }
 
+static cudaEvent_t take_event(StageTimer* t) {
+  if (!t->pool.empty()) {
+    cudaEvent_t e = t->pool.back();
+    t->pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+void timer_begin(StageTimer* t, cudaStream_t s, cudaEvent_t* ev) {
+  *ev = nullptr;
+  if (!t || !t->on) return;
+  *ev = take_event(t);
+  cudaEventRecord(*ev, s);
+}
+
+void timer_end(StageTimer* t, cudaStream_t s, int stage, cudaEvent_t start) {
+  if (!t || !t->on || !start) return;
+  cudaEvent_t e = take_event(t);
+  cudaEventRecord(e, s);
+  t->pending.push_back({stage, {start, e}});
+}
+
+int timer_collect(StageTimer* t) {
+  for (auto& pe : t->pending) {
+    SO3G_CUDA(cudaEventSynchronize(pe.second.second));
+    float ms = 0.f;
+    SO3G_CUDA(cudaEventElapsedTime(&ms, pe.second.first, pe.second.second));
+    t->total_ms[pe.first] += ms;
+    t->count[pe.first] += 1;
+    t->pool.push_back(pe.second.first);
+    t->pool.push_back(pe.second.second);
+  }
+  t->pending.clear();
+  return kOk;
+}
+
 int ensure_ws(Workspace* W, size_t bytes, void** out) {
   if (bytes > W->ws_bytes) {
     if (W->ws) cudaFree(W->ws);

@@ -147,6 +147,9 @@ def test_invalid_parameters_return_status():
     p.sampling_scheme = 7
     with pytest.raises(so3.SO3Error, match="status 1"):
         so3.inverse(np.zeros(8 * 8 * 7, complex), p)
+    p = params(8, 4, mode=9)
+    with pytest.raises(so3.SO3Error, match="status 1"):
+        so3.inverse(np.zeros(8 * 8 * 7, complex), p)
     p = params(8, 4, steerable=1)
     with pytest.raises(so3.SO3Error, match="status 3"):
         so3.inverse(np.zeros(8 * 8 * 7, complex), p)

@@ -8,24 +8,43 @@
 // in-tree :1589-1617):
 //   f_lmn = i^{m-n} sum_{m'=0}^{l} Delta^l_{m'm} Delta^l_{m'n} G[n][m'][m].
 //
-// Negative m, n use Delta^l_{m',-k} = (-1)^{l+m'} Delta^l_{m'k}: one product
-// w = Delta_{m'|m|} Delta_{m'|n|} feeds the four sign combinations
-// (+m,+n), (-m,+n), (+m,-n), (-m,-n); combinations with exactly one negative
-// index carry (-1)^{l+m'}, split as (-1)^l folded into the operand that
-// depends on l and (-1)^{m'} into the one that depends on m'.
-//
-// CTA = 4 warps.  Lanes span 32 consecutive |m| (coalesced loads of Delta rows
-// and of coefficient/spectral rows); each warp owns 8 values of the output
-// index (m' for the inverse, l for the forward); blockIdx.z = |n|.
+// Both are three-operand contractions (every pair of the free indices shares
+// an operand), so no plain GEMM exists for one signal; the kernels are built
+// for the FP64 pipe:
+//  * Negative m, n use Delta^l_{m',-k} = (-1)^{l+m'} Delta^l_{m'k}: one product
+//    w = Delta_{m'|m|} Delta_{m'|n|} feeds the four sign combinations (+m,+n),
+//    (-m,+n), (+m,-n), (-m,-n) (9 FP64 instructions per 4 complex MACs).  The
+//    (-1)^{l+m'} of combinations with one negative index is split between the
+//    operand that carries l and the one that carries m'.
+//  * CTA tile: 32 output rows (m' for the inverse, l for the forward) x 32 |m|
+//    x 2 |n|.  The reduction index (l, resp. m') is walked in chunks of 4,
+//    staged in shared memory with cp.async, double buffered.
+//  * Lanes form an 8 (rows) x 4 (|m|) grid, warps step |m| by 4: a warp reads
+//    32 distinct Delta_{m'|m|} (2 wavefronts with the 36-double row pitch),
+//    8 distinct Delta_{m'|n|} pairs and 4 distinct coefficient quadruples
+//    (1 wavefront each), for 72 FP64 instructions per lane.
+//  * Grid order |n|-pair fastest, then rows, then |m|: CTAs resident at the
+//    same time share one Delta tile column and one coefficient slice in L2.
 #include "so3gpu_internal.h"
 
 namespace so3g {
 
 namespace {
-constexpr int kWarps = 4;
-constexpr int kPer = 8;                  // output rows per warp
-constexpr int kTile = kWarps * kPer;     // 32 output rows per CTA
+constexpr int kThreads = 256;
+constexpr int kRows = 32;    // output rows per CTA (m' or l)
+constexpr int kCols = 32;    // |m| per CTA
+constexpr int kNG = 2;       // |n| per CTA
+constexpr int kChunk = 4;    // reduction steps per shared-memory stage
+constexpr int kPitch = 36;   // doubles per staged Delta row (32 + 4: conflict-free)
+constexpr int kPer = kRows / 8;  // rows per lane
 constexpr double kInv8Pi2 = 0.012665147955292221430803304553147533;  // 1/(8 pi^2)
+
+struct Slab {
+  double B[kChunk][kRows][kPitch];  // Delta^l_{row, |m|}
+  double A[kChunk][kRows][kNG];     // Delta^l_{row, |n|}  (times (2l+1)/(8 pi^2) in the inverse)
+  double2 H[kChunk][kCols][kNG][4]; // coefficients / spectra, sign-folded
+};
+constexpr size_t kSmem = 2 * sizeof(Slab);
 
 __device__ __forceinline__ double2 ipow_mul(double2 v, int k) {  // v * i^k
   switch (k & 3) {
@@ -33,6 +52,58 @@ __device__ __forceinline__ double2 ipow_mul(double2 v, int k) {  // v * i^k
     case 1: return make_double2(-v.y, v.x);
     case 2: return make_double2(-v.x, -v.y);
     default: return make_double2(v.y, -v.x);
+  }
+}
+__device__ __forceinline__ double2 sc(double2 v, double s) { return make_double2(v.x * s, v.y * s); }
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(valid ? 8 : 0));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+// 4 sign combinations s: bit0 -> m negative, bit1 -> n negative.  scale
+// multiplies every product (the (2l+1)/(8 pi^2) of the inverse, 1 in the
+// forward); oddneg flips the sign of the combinations with one negative index
+// ((-1)^l in the inverse, (-1)^{m'} in the forward); symmu != 0 rebuilds the
+// -m coefficient of a real signal with N == 1 from the +m one.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(valid ? 16 : 0));
+}
+
+template <int NSIGN, bool SYM>
+__device__ __forceinline__ void mac_chunk(const Slab& S, int lc, int warp, int lm, int lu, double scale, bool oddneg,
+                                          int mu, double2 (&acc)[kPer][kNG][4]) {
+  const int col = 4 * warp + lu;
+  double2 h[kNG][4];
+#pragma unroll
+  for (int j = 0; j < kNG; j++) {
+#pragma unroll
+    for (int s = 0; s < NSIGN; s++) h[j][s] = S.H[lc][col][j][s];
+    if (SYM) h[j][1] = (mu & 1) ? make_double2(-h[j][0].x, h[j][0].y) : make_double2(h[j][0].x, -h[j][0].y);
+  }
+  const double sneg = oddneg ? -scale : scale;
+#pragma unroll
+  for (int i = 0; i < kPer; i++) {
+    const int row = lm + 8 * i;
+    const double b = S.B[lc][row][col];
+    const double2 a = *reinterpret_cast<const double2*>(&S.A[lc][row][0]);
+    const double p0 = b * a.x, p1 = b * a.y;
+    const double w0 = p0 * scale, w1 = p1 * scale, v0 = p0 * sneg, v1 = p1 * sneg;
+#pragma unroll
+    for (int s = 0; s < NSIGN; s++) {
+      const bool one_neg = (s == 1) || (s == 2);
+      const double x0 = one_neg ? v0 : w0, x1 = one_neg ? v1 : w1;
+      acc[i][0][s].x = fma(x0, h[0][s].x, acc[i][0][s].x);
+      acc[i][0][s].y = fma(x0, h[0][s].y, acc[i][0][s].y);
+      acc[i][1][s].x = fma(x1, h[1][s].x, acc[i][1][s].x);
+      acc[i][1][s].y = fma(x1, h[1][s].y, acc[i][1][s].y);
+    }
   }
 }
 }  // namespace
@@ -46,79 +117,113 @@ struct InvArgs {
   long long RS, PS;
 };
 
-__global__ void __launch_bounds__(128) inverse_contract_kernel(InvArgs a) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int mu = blockIdx.x * 32 + lane;
-  const int mp0 = blockIdx.y * kTile + warp * kPer;
-  const int nu = blockIdx.z;
+// ------------------------------------------------------------------ inverse
+template <int NSIGN>
+__global__ void __launch_bounds__(kThreads, 1) inverse_contract_kernel(InvArgs a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  Slab* st = reinterpret_cast<Slab*>(smraw);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, lm = lane & 7, lu = lane >> 3;
+  const int nu0 = blockIdx.x * kNG, mp0 = blockIdx.y * kRows, mu0 = blockIdx.z * kCols;
   const int L = a.L;
-  const bool neg_n = !a.real && nu > 0;  // a distinct -nu plane exists
-  const bool skipped = plane_skipped(a.n_mode, a.N, nu);  // +nu and -nu share parity and |n|
+  bool act[kNG];
+#pragma unroll
+  for (int j = 0; j < kNG; j++) act[j] = (nu0 + j < a.N) && !plane_skipped(a.n_mode, a.N, nu0 + j);
 
-  double2 acc[kPer][4];
+  double2 acc[kPer][kNG][4];
 #pragma unroll
   for (int i = 0; i < kPer; i++)
 #pragma unroll
-    for (int s = 0; s < 4; s++) acc[i][s] = make_double2(0.0, 0.0);
+    for (int j = 0; j < kNG; j++)
+#pragma unroll
+      for (int s = 0; s < 4; s++) acc[i][j][s] = make_double2(0.0, 0.0);
 
-  if (!skipped) {
-    const long long bp = a.base[a.plane0 + nu];
-    const long long bn = neg_n ? a.base[a.plane0 - nu] : 0;
-    int lstart = max(max(a.L0, nu), max((int)(blockIdx.y * kTile), (int)(blockIdx.x * 32)));
-    for (int l = lstart; l < L; l++) {
-      const bool mu_ok = mu <= l;
-      const double c = (2.0 * l + 1.0) * kInv8Pi2;
-      const double sl = (l & 1) ? -c : c;
-      const long long row = (long long)l * l + l;
-      double2 h[4] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
-      if (mu_ok) {
-        double2 pp = __ldg(a.flmn + bp + row + mu);
-        double2 mp_ = __ldg(a.flmn + bp + row - mu);
-        if (a.sym_n0) {  // real signal, N == 1: f_{l,-m,0} = (-1)^m conj f_{l,m,0}
-          mp_ = (mu & 1) ? make_double2(-pp.x, pp.y) : make_double2(pp.x, -pp.y);
-        }
-        h[0] = make_double2(c * pp.x, c * pp.y);
-        h[1] = make_double2(sl * mp_.x, sl * mp_.y);
-        if (neg_n) {
-          double2 pm = __ldg(a.flmn + bn + row + mu);
-          double2 mm = __ldg(a.flmn + bn + row - mu);
-          h[2] = make_double2(sl * pm.x, sl * pm.y);
-          h[3] = make_double2(c * mm.x, c * mm.y);
-        }
-      }
-      const double* P = a.dl + dl_plane_offset(l);
-      const int ld = l + 1;
+  const int lstart = max(max(a.L0, nu0), max(mp0, mu0));
+  const int mu_own = mu0 + 4 * warp + lu;
+  long long bsel[kNG][2];  // flmn block bases of +|n| and -|n|
 #pragma unroll
-      for (int i = 0; i < kPer; i++) {
-        const int mp = mp0 + i;
-        if (mp <= l && mu_ok) {
-          const double w = __ldg(P + (long long)mp * ld + mu) * __ldg(P + (long long)mp * ld + nu);
-#pragma unroll
-          for (int s = 0; s < 4; s++) {
-            acc[i][s].x = fma(w, h[s].x, acc[i][s].x);
-            acc[i][s].y = fma(w, h[s].y, acc[i][s].y);
-          }
-        }
+  for (int j = 0; j < kNG; j++) {
+    const int nu = min(nu0 + j, a.N - 1);
+    bsel[j][0] = a.base[a.plane0 + nu];
+    bsel[j][1] = NSIGN == 4 ? a.base[a.plane0 - nu] : 0;
+  }
+  const int nchunk = lstart < L ? (L - lstart + kChunk - 1) / kChunk : 0;
+
+  auto stage = [&](int c, Slab& S) {
+    const int lbase = lstart + c * kChunk;
+    for (int idx = tid; idx < kChunk * kRows * kCols; idx += kThreads) {
+      const int lc = idx / (kRows * kCols), rem = idx - lc * kRows * kCols, r = rem / kCols, col = rem - r * kCols;
+      const int l = lbase + lc;
+      const bool ok = l < L && mp0 + r <= l && mu0 + col <= l;
+      const double* src = ok ? a.dl + dl_plane_offset(l) + (long long)(mp0 + r) * (l + 1) + mu0 + col : a.dl;
+      cp_async8(&S.B[lc][r][col], src, ok);
+    }
+    for (int idx = tid; idx < kChunk * kRows * kNG; idx += kThreads) {
+      const int lc = idx / (kRows * kNG), rem = idx - lc * kRows * kNG, r = rem / kNG, j = rem - r * kNG;
+      const int l = lbase + lc, nu = nu0 + j;
+      const bool ok = l < L && act[j] && mp0 + r <= l && nu <= l;
+      const double* src = ok ? a.dl + dl_plane_offset(l) + (long long)(mp0 + r) * (l + 1) + nu : a.dl;
+      cp_async8(&S.A[lc][r][j], src, ok);
+    }
+    for (int idx = tid; idx < kChunk * kCols * kNG * NSIGN; idx += kThreads) {
+      const int lc = idx / (kCols * kNG * NSIGN), rem = idx - lc * kCols * kNG * NSIGN;
+      const int col = rem / (kNG * NSIGN), rem2 = rem - col * kNG * NSIGN, j = rem2 / NSIGN, sg = rem2 - j * NSIGN;
+      const int l = lbase + lc, nu = nu0 + j, mu = mu0 + col;
+      const bool ok = l < L && act[j] && mu <= l && nu <= l;
+      const int m = (sg & 1) ? -mu : mu;
+      const double2* src = ok ? a.flmn + bsel[j][sg >> 1] + (long long)l * l + l + m : a.flmn;
+      cp_async16(&S.H[lc][col][j][sg], src, ok);
+    }
+  };
+
+  if (nchunk > 0) {
+    stage(0, st[0]);
+    cp_commit();
+    for (int c = 0; c < nchunk; c++) {
+      if (c + 1 < nchunk) {
+        stage(c + 1, st[(c + 1) & 1]);
+        cp_commit();
+        cp_wait<1>();
+      } else {
+        cp_wait<0>();
       }
+      __syncthreads();
+      const Slab& S = st[c & 1];
+      const int lbase = lstart + c * kChunk;
+#pragma unroll
+      for (int lc = 0; lc < kChunk; lc++) {
+        const int l = lbase + lc;
+        const double cl = (2.0 * l + 1.0) * kInv8Pi2;
+        if (a.sym_n0)
+          mac_chunk<NSIGN, true>(S, lc, warp, lm, lu, cl, l & 1, mu_own, acc);
+        else
+          mac_chunk<NSIGN, false>(S, lc, warp, lm, lu, cl, l & 1, mu_own, acc);
+      }
+      __syncthreads();
     }
   }
+
+  const int mu = mu0 + 4 * warp + lu;
   if (mu >= L) return;
-  const int nplanes_sign = neg_n ? 2 : 1;
 #pragma unroll
   for (int i = 0; i < kPer; i++) {
-    const int mp = mp0 + i;
+    const int mp = mp0 + lm + 8 * i;
     if (mp >= L) continue;
     const double odd_mp = (mp & 1) ? -1.0 : 1.0;
 #pragma unroll
-    for (int s = 0; s < 4; s++) {
-      const int ms = (s & 1) ? -1 : 1, ns = (s & 2) ? -1 : 1;
-      if (ms < 0 && mu == 0) continue;
-      if (ns < 0 && nplanes_sign == 1) continue;
-      const int m = ms * mu, n = ns * nu;
-      double2 v = acc[i][s];
-      if (ms * ns < 0) v = make_double2(v.x * odd_mp, v.y * odd_mp);
-      v = ipow_mul(v, n - m + 4 * L);
-      a.W[(long long)(a.plane0 + n) * a.PS + (long long)mp * a.RS + (m + L - 1)] = v;
+    for (int j = 0; j < kNG; j++) {
+      const int nu = nu0 + j;
+      if (nu >= a.N) continue;
+#pragma unroll
+      for (int s = 0; s < NSIGN; s++) {
+        const int ms = (s & 1) ? -1 : 1, ns = (s & 2) ? -1 : 1;
+        if (ms < 0 && mu == 0) continue;
+        if (ns < 0 && nu == 0) continue;
+        const int m = ms * mu, n = ns * nu;
+        double2 v = acc[i][j][s];
+        if (ms * ns < 0) v = sc(v, odd_mp);
+        v = ipow_mul(v, n - m + 4 * L);
+        a.W[(long long)(a.plane0 + n) * a.PS + (long long)mp * a.RS + (m + L - 1)] = v;
+      }
     }
   }
 }
@@ -126,13 +231,20 @@ __global__ void __launch_bounds__(128) inverse_contract_kernel(InvArgs a) {
 int launch_inverse_contract(const Geometry& g, int n_mode, const double2* flmn, const long long* bases,
                             const double* dl, double2* W, int sym_n0, cudaStream_t s) {
   InvArgs a{flmn, bases, dl, W, g.L, g.N, g.L0, g.plane0, n_mode, g.real, sym_n0, g.RS, g.PS};
-  dim3 grid((g.L + 31) / 32, (g.L + kTile - 1) / kTile, g.N);
-  inverse_contract_kernel<<<grid, 128, 0, s>>>(a);
+  dim3 grid((g.N + kNG - 1) / kNG, (g.L + kRows - 1) / kRows, (g.L + kCols - 1) / kCols);
+  if (g.real) {
+    SO3G_CUDA(cudaFuncSetAttribute(inverse_contract_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));
+    inverse_contract_kernel<2><<<grid, kThreads, kSmem, s>>>(a);
+  } else {
+    SO3G_CUDA(cudaFuncSetAttribute(inverse_contract_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));
+    inverse_contract_kernel<4><<<grid, kThreads, kSmem, s>>>(a);
+  }
   SO3G_LAUNCHED();
   SO3G_CUDA(cudaGetLastError());
   return kOk;
 }
 
+// ------------------------------------------------------------------ forward
 struct FwdArgs {
   const double2* W;
   const long long* base;
@@ -142,76 +254,103 @@ struct FwdArgs {
   long long RS, PS;
 };
 
-__global__ void __launch_bounds__(128) forward_contract_kernel(FwdArgs a) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int mu = blockIdx.x * 32 + lane;
-  const int l0 = blockIdx.y * kTile + warp * kPer;
-  const int nu = blockIdx.z;
+template <int NSIGN>
+__global__ void __launch_bounds__(kThreads, 1) forward_contract_kernel(FwdArgs a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  Slab* st = reinterpret_cast<Slab*>(smraw);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, lm = lane & 7, lu = lane >> 3;
+  const int nu0 = blockIdx.x * kNG, l0 = blockIdx.y * kRows, mu0 = blockIdx.z * kCols;
   const int L = a.L;
-  const bool neg_n = !a.real && nu > 0;
-  if (plane_skipped(a.n_mode, a.N, nu)) return;  // caller-zeroed blocks stay untouched
+  bool act[kNG];
+#pragma unroll
+  for (int j = 0; j < kNG; j++) act[j] = (nu0 + j < a.N) && !plane_skipped(a.n_mode, a.N, nu0 + j);
+  if (!act[0] && !act[1]) return;  // caller-zeroed blocks stay untouched
 
-  double2 acc[kPer][4];
+  double2 acc[kPer][kNG][4];
 #pragma unroll
   for (int i = 0; i < kPer; i++)
 #pragma unroll
-    for (int s = 0; s < 4; s++) acc[i][s] = make_double2(0.0, 0.0);
+    for (int j = 0; j < kNG; j++)
+#pragma unroll
+      for (int s = 0; s < 4; s++) acc[i][j][s] = make_double2(0.0, 0.0);
 
-  const int ltop = min(L - 1, (int)(blockIdx.y * kTile) + kTile - 1);
-  const int lmin_needed = max(max(a.L0, nu), (int)(blockIdx.x * 32));
-  if (ltop >= lmin_needed) {
-    const double2* Gp = a.W + (long long)(a.plane0 + nu) * a.PS + (L - 1);
-    const double2* Gn = a.W + (long long)(a.plane0 - nu) * a.PS + (L - 1);
-    const bool mu_ok = mu < L;
-    for (int mp = 0; mp <= ltop; mp++) {
-      double2 g[4] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
-      if (mu_ok) {
-        const double sm = (mp & 1) ? -1.0 : 1.0;
-        const long long r = (long long)mp * a.RS;
-        double2 pp = __ldg(Gp + r + mu), mp_ = __ldg(Gp + r - mu);
-        g[0] = pp;
-        g[1] = make_double2(sm * mp_.x, sm * mp_.y);
-        if (neg_n) {
-          double2 pm = __ldg(Gn + r + mu), mm = __ldg(Gn + r - mu);
-          g[2] = make_double2(sm * pm.x, sm * pm.y);
-          g[3] = mm;
-        }
+  const int ltop = min(L - 1, l0 + kRows - 1);
+  const bool any = ltop >= max(max(a.L0, nu0), mu0);
+  const int nchunk = any ? (ltop + 1 + kChunk - 1) / kChunk : 0;
+
+  auto stage = [&](int c, Slab& S) {
+    const int mbase = c * kChunk;
+    for (int idx = tid; idx < kChunk * kRows * kCols; idx += kThreads) {
+      const int mc = idx / (kRows * kCols), rem = idx - mc * kRows * kCols, r = rem / kCols, col = rem - r * kCols;
+      const int mp = mbase + mc, l = l0 + r;
+      const bool ok = l < L && mp <= l && mu0 + col <= l;
+      const double* src = ok ? a.dl + dl_plane_offset(l) + (long long)mp * (l + 1) + mu0 + col : a.dl;
+      cp_async8(&S.B[mc][r][col], src, ok);
+    }
+    for (int idx = tid; idx < kChunk * kRows * kNG; idx += kThreads) {
+      const int mc = idx / (kRows * kNG), rem = idx - mc * kRows * kNG, r = rem / kNG, j = rem - r * kNG;
+      const int mp = mbase + mc, l = l0 + r, nu = nu0 + j;
+      const bool ok = l < L && act[j] && mp <= l && nu <= l;
+      const double* src = ok ? a.dl + dl_plane_offset(l) + (long long)mp * (l + 1) + nu : a.dl;
+      cp_async8(&S.A[mc][r][j], src, ok);
+    }
+    for (int idx = tid; idx < kChunk * kCols * kNG * NSIGN; idx += kThreads) {
+      const int mc = idx / (kCols * kNG * NSIGN), rem = idx - mc * kCols * kNG * NSIGN;
+      const int col = rem / (kNG * NSIGN), rem2 = rem - col * kNG * NSIGN, j = rem2 / NSIGN, sg = rem2 - j * NSIGN;
+      const int mp = mbase + mc, nu = nu0 + j, mu = mu0 + col;
+      const bool ok = mp < L && act[j] && mu < L;
+      const int n = (sg & 2) ? -nu : nu, m = (sg & 1) ? -mu : mu;
+      const double2* src =
+          ok ? a.W + (long long)(a.plane0 + n) * a.PS + (long long)mp * a.RS + (L - 1) + m : a.W;
+      cp_async16(&S.H[mc][col][j][sg], src, ok);
+    }
+  };
+
+  if (nchunk > 0) {
+    stage(0, st[0]);
+    cp_commit();
+    for (int c = 0; c < nchunk; c++) {
+      if (c + 1 < nchunk) {
+        stage(c + 1, st[(c + 1) & 1]);
+        cp_commit();
+        cp_wait<1>();
+      } else {
+        cp_wait<0>();
       }
+      __syncthreads();
+      const Slab& S = st[c & 1];
 #pragma unroll
-      for (int i = 0; i < kPer; i++) {
-        const int l = l0 + i;
-        if (l < L && mp <= l && mu <= l && l >= nu) {
-          const double* P = a.dl + dl_plane_offset(l) + (long long)mp * (l + 1);
-          const double w = __ldg(P + mu) * __ldg(P + nu);
-#pragma unroll
-          for (int s = 0; s < 4; s++) {
-            acc[i][s].x = fma(w, g[s].x, acc[i][s].x);
-            acc[i][s].y = fma(w, g[s].y, acc[i][s].y);
-          }
-        }
-      }
+      for (int mc = 0; mc < kChunk; mc++) mac_chunk<NSIGN, false>(S, mc, warp, lm, lu, 1.0, (c * kChunk + mc) & 1, 0, acc);
+      __syncthreads();
     }
   }
+
+  const int mu = mu0 + 4 * warp + lu;
   if (mu >= L) return;
 #pragma unroll
   for (int i = 0; i < kPer; i++) {
-    const int l = l0 + i;
+    const int l = l0 + lm + 8 * i;
     if (l >= L || mu > l) continue;
     const double odd_l = (l & 1) ? -1.0 : 1.0;
 #pragma unroll
-    for (int s = 0; s < 4; s++) {
-      const int ms = (s & 1) ? -1 : 1, ns = (s & 2) ? -1 : 1;
-      if (ms < 0 && mu == 0) continue;
-      if (ns < 0 && !neg_n) continue;
-      const int m = ms * mu, n = ns * nu;
+    for (int j = 0; j < kNG; j++) {
+      const int nu = nu0 + j;
+      if (!act[j]) continue;
       if (a.compact && l < nu) continue;  // not stored
-      double2 v = make_double2(0.0, 0.0);
-      if (l >= max(a.L0, nu)) {
-        v = acc[i][s];
-        if (ms * ns < 0) v = make_double2(v.x * odd_l, v.y * odd_l);
-        v = ipow_mul(v, m - n + 4 * L);
+#pragma unroll
+      for (int s = 0; s < NSIGN; s++) {
+        const int ms = (s & 1) ? -1 : 1, ns = (s & 2) ? -1 : 1;
+        if (ms < 0 && mu == 0) continue;
+        if (ns < 0 && nu == 0) continue;
+        const int m = ms * mu, n = ns * nu;
+        double2 v = make_double2(0.0, 0.0);
+        if (l >= max(a.L0, nu)) {
+          v = acc[i][j][s];
+          if (ms * ns < 0) v = sc(v, odd_l);
+          v = ipow_mul(v, m - n + 4 * L);
+        }
+        a.flmn[a.base[a.plane0 + n] + (long long)l * l + l + m] = v;
       }
-      a.flmn[a.base[a.plane0 + n] + (long long)l * l + l + m] = v;
     }
   }
 }
@@ -219,8 +358,14 @@ __global__ void __launch_bounds__(128) forward_contract_kernel(FwdArgs a) {
 int launch_forward_contract(const Geometry& g, int n_mode, const double2* W, const long long* bases,
                             const double* dl, double2* flmn, int storage_compact, cudaStream_t s) {
   FwdArgs a{W, bases, dl, flmn, g.L, g.N, g.L0, g.plane0, n_mode, g.real, storage_compact, g.RS, g.PS};
-  dim3 grid((g.L + 31) / 32, (g.L + kTile - 1) / kTile, g.N);
-  forward_contract_kernel<<<grid, 128, 0, s>>>(a);
+  dim3 grid((g.N + kNG - 1) / kNG, (g.L + kRows - 1) / kRows, (g.L + kCols - 1) / kCols);
+  if (g.real) {
+    SO3G_CUDA(cudaFuncSetAttribute(forward_contract_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));
+    forward_contract_kernel<2><<<grid, kThreads, kSmem, s>>>(a);
+  } else {
+    SO3G_CUDA(cudaFuncSetAttribute(forward_contract_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));
+    forward_contract_kernel<4><<<grid, kThreads, kSmem, s>>>(a);
+  }
   SO3G_LAUNCHED();
   SO3G_CUDA(cudaGetLastError());
   return kOk;

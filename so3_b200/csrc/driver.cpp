@@ -1,5 +1,7 @@
 // Transform drivers: stage order of the inverse and forward Wigner transforms
 // on device pointers.  Host code only; every kernel runs on stream s.
+#include <cstdlib>
+
 #include "so3gpu_internal.h"
 
 namespace so3g {

@@ -30,6 +30,14 @@ struct FftPlan {
   const double2* chirp;      // e^{-i pi k^2/n}, k < n     (Bluestein)
   const double2* kern;       // FFT_m(conj chirp) / m      (Bluestein)
   int ld() const { return blue ? m : n; }
+  // any radix above 8 (needs the large-radix kernel instances)
+  bool big() const {
+    for (int i = 0; i < npass; i++)
+      if (rad[i] > 8) return true;
+    for (int i = 0; i < mpass; i++)
+      if (mrad[i] > 8) return true;
+    return false;
+  }
 };
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
@@ -140,15 +148,9 @@ __device__ __forceinline__ void stockham_pass(const double2* __restrict__ src, d
   }
 }
 
-__device__ __forceinline__ void dispatch_pass(int R, const double2* src, double2* dst, int n, int Ns, int T,
-                                              int ld, const double2* roots) {
+static __device__ __noinline__ void dispatch_big(int R, const double2* src, double2* dst, int n, int Ns, int T, int ld,
+                                          const double2* roots) {
   switch (R) {
-    case 2: stockham_pass<2>(src, dst, n, Ns, T, ld, roots); break;
-    case 3: stockham_pass<3>(src, dst, n, Ns, T, ld, roots); break;
-    case 4: stockham_pass<4>(src, dst, n, Ns, T, ld, roots); break;
-    case 5: stockham_pass<5>(src, dst, n, Ns, T, ld, roots); break;
-    case 7: stockham_pass<7>(src, dst, n, Ns, T, ld, roots); break;
-    case 8: stockham_pass<8>(src, dst, n, Ns, T, ld, roots); break;
     case 11: stockham_pass<11>(src, dst, n, Ns, T, ld, roots); break;
     case 13: stockham_pass<13>(src, dst, n, Ns, T, ld, roots); break;
     case 17: stockham_pass<17>(src, dst, n, Ns, T, ld, roots); break;
@@ -160,12 +162,28 @@ __device__ __forceinline__ void dispatch_pass(int R, const double2* src, double2
   }
 }
 
+// BIG selects the radix set: false -> {2,3,4,5,7,8} only (low register use,
+// two CTAs per SM), true -> also the odd primes 11..31.
+template <bool BIG>
+__device__ __forceinline__ void dispatch_pass(int R, const double2* src, double2* dst, int n, int Ns, int T,
+                                              int ld, const double2* roots) {
+  switch (R) {
+    case 2: stockham_pass<2>(src, dst, n, Ns, T, ld, roots); break;
+    case 3: stockham_pass<3>(src, dst, n, Ns, T, ld, roots); break;
+    case 4: stockham_pass<4>(src, dst, n, Ns, T, ld, roots); break;
+    case 5: stockham_pass<5>(src, dst, n, Ns, T, ld, roots); break;
+    case 7: stockham_pass<7>(src, dst, n, Ns, T, ld, roots); break;
+    case 8: stockham_pass<8>(src, dst, n, Ns, T, ld, roots); break;
+    default: if constexpr (BIG) dispatch_big(R, src, dst, n, Ns, T, ld, roots); break;
+  }
+}
 // Runs the passes; data starts in a, returns the buffer holding the result.
+template <bool BIG>
 __device__ __forceinline__ double2* run_passes(double2* a, double2* b, int n, const int* rad, int npass, int T,
                                                int ld, const double2* roots) {
   int Ns = 1;
   for (int p = 0; p < npass; p++) {
-    dispatch_pass(rad[p], a, b, n, Ns, T, ld, roots);
+    dispatch_pass<BIG>(rad[p], a, b, n, Ns, T, ld, roots);
     __syncthreads();
     double2* t = a;
     a = b;
@@ -179,9 +197,10 @@ __device__ __forceinline__ double2* run_passes(double2* a, double2* b, int n, co
 // j < n; b is scratch of the same size.  Both buffers need ld >= plan.ld().
 // Caller must __syncthreads() after staging the input.  Returns the buffer
 // holding the n outputs of each sequence.
+template <bool BIG>
 __device__ __forceinline__ double2* fft_fwd_smem(double2* a, double2* b, int T, int ld, const FftPlan& P) {
   if (P.n == 1) return a;
-  if (!P.blue) return run_passes(a, b, P.n, P.rad, P.npass, T, ld, P.roots);
+  if (!P.blue) return run_passes<BIG>(a, b, P.n, P.rad, P.npass, T, ld, P.roots);
   const int n = P.n, m = P.m;
   for (int w = threadIdx.x; w < T * m; w += blockDim.x) {
     const int t = w / m, k = w - t * m;
@@ -189,7 +208,7 @@ __device__ __forceinline__ double2* fft_fwd_smem(double2* a, double2* b, int T, 
     s[k] = k < n ? cmul(s[k], __ldg(P.chirp + k)) : make_double2(0.0, 0.0);
   }
   __syncthreads();
-  double2* r = run_passes(a, b, m, P.mrad, P.mpass, T, ld, P.mroots);
+  double2* r = run_passes<BIG>(a, b, m, P.mrad, P.mpass, T, ld, P.mroots);
   for (int w = threadIdx.x; w < T * m; w += blockDim.x) {
     const int t = w / m, k = w - t * m;
     double2* s = r + t * ld;
@@ -197,7 +216,7 @@ __device__ __forceinline__ double2* fft_fwd_smem(double2* a, double2* b, int T, 
   }
   __syncthreads();
   double2* o = (r == a) ? b : a;
-  r = run_passes(r, o, m, P.mrad, P.mpass, T, ld, P.mroots);
+  r = run_passes<BIG>(r, o, m, P.mrad, P.mpass, T, ld, P.mroots);
   for (int w = threadIdx.x; w < T * n; w += blockDim.x) {
     const int t = w / n, k = w - t * n;
     double2* s = r + t * ld;

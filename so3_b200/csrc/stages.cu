@@ -30,10 +30,35 @@ int pick_T(int ld, int buffers_per_seq, int Tmax) {
   return T;
 }
 
+// Sequences per CTA and dynamic shared memory for a plan of engine length ld:
+// large-radix instances may use up to kSmemCap (one CTA per SM), the others
+// stay within half of an SM's shared memory (two CTAs per SM).
+struct Sizing {
+  int T;
+  size_t smem;
+};
+Sizing size_for(bool big, int ld, int Tmax) {
+  Sizing z;
+  const size_t cap = big ? kSmemCap : kSmemCap / 2 + 10 * 1024;
+  int T = Tmax;
+  while (T > 1 && 2 * (size_t)T * ld * sizeof(double2) > cap) T >>= 1;
+  z.T = T;
+  z.smem = 2 * (size_t)T * ld * sizeof(double2);
+  return z;
+}
+
 template <typename K>
 int set_smem(K kernel, size_t bytes) {
   SO3G_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
   return kOk;
+}
+
+// Instances for plans with a radix above 8 carry the large odd-radix
+// butterflies (high register use, one CTA per SM); the others stay below 128
+// registers and run two CTAs per SM.
+template <bool BIG>
+__device__ __forceinline__ double2* run_fft(double2* a, double2* b, int T, int ld, const FftPlan& P) {
+  return fft_fwd_smem<BIG>(a, b, T, ld, P);
 }
 
 __device__ __forceinline__ int wrapi(int k, int P) {
@@ -48,7 +73,8 @@ __device__ __forceinline__ double2 phase(int k, int den, double sign) {  // e^{s
 }  // namespace
 
 // ------------------------------------------------------------------ inverse
-__global__ void __launch_bounds__(kThreads) inv_beta_kernel(Geometry g, FftPlan P, double2* __restrict__ W,
+template <bool BIG>
+__global__ void __launch_bounds__(kThreads, BIG ? 1 : 2) inv_beta_kernel(Geometry g, FftPlan P, double2* __restrict__ W,
                                                              int T, int ld) {
   extern __shared__ double2 sm[];
   double2* a = sm;
@@ -73,14 +99,15 @@ __global__ void __launch_bounds__(kThreads) inv_beta_kernel(Geometry g, FftPlan 
     if (mp > 0) a[t * ld + Pn - mp] = cconj(xn);
   }
   __syncthreads();
-  double2* r = fft_fwd_smem(a, b, T, ld, P);
+  double2* r = run_fft<BIG>(a, b, T, ld, P);
   for (int idx = threadIdx.x; idx < g.nb * T; idx += blockDim.x) {
     const int t = idx % T, row = idx / T, c = c0 + t;
     if (c < ncols) base[(long long)row * g.RS + c] = cconj(r[t * ld + row]);
   }
 }
 
-__global__ void __launch_bounds__(kThreads) inv_alpha_kernel(Geometry g, FftPlan P, double2* __restrict__ W,
+template <bool BIG>
+__global__ void __launch_bounds__(kThreads, BIG ? 1 : 2) inv_alpha_kernel(Geometry g, FftPlan P, double2* __restrict__ W,
                                                               int T, int ld) {
   extern __shared__ double2 sm[];
   double2* a = sm;
@@ -100,7 +127,7 @@ __global__ void __launch_bounds__(kThreads) inv_alpha_kernel(Geometry g, FftPlan
     a[j * ld + k] = cconj(v);
   }
   __syncthreads();
-  double2* r = fft_fwd_smem(a, b, T, ld, P);
+  double2* r = run_fft<BIG>(a, b, T, ld, P);
   for (int idx = threadIdx.x; idx < T * g.na; idx += blockDim.x) {
     const int j = idx / g.na, k = idx - j * g.na, row = r0 + j;
     if (row < nrows) {
@@ -110,8 +137,8 @@ __global__ void __launch_bounds__(kThreads) inv_alpha_kernel(Geometry g, FftPlan
   }
 }
 
-template <bool REAL>
-__global__ void __launch_bounds__(kThreads) inv_gamma_kernel(Geometry g, FftPlan P, const double2* __restrict__ W,
+template <bool REAL, bool BIG>
+__global__ void __launch_bounds__(kThreads, BIG ? 1 : 2) inv_gamma_kernel(Geometry g, FftPlan P, const double2* __restrict__ W,
                                                               void* __restrict__ fout, int T, int ld) {
   extern __shared__ double2 sm[];
   double2* a = sm;
@@ -134,7 +161,7 @@ __global__ void __launch_bounds__(kThreads) inv_gamma_kernel(Geometry g, FftPlan
     }
   }
   __syncthreads();
-  double2* r = fft_fwd_smem(a, b, T, ld, P);
+  double2* r = run_fft<BIG>(a, b, T, ld, P);
   const long long plane_sz = (long long)g.nb * g.na;
   for (int idx = threadIdx.x; idx < ng * T; idx += blockDim.x) {
     const int t = idx % T, gi = idx / T, al = a0 + t;
@@ -149,8 +176,8 @@ __global__ void __launch_bounds__(kThreads) inv_gamma_kernel(Geometry g, FftPlan
 }
 
 // ------------------------------------------------------------------ forward
-template <bool REAL>
-__global__ void __launch_bounds__(kThreads) fwd_gamma_kernel(Geometry g, FftPlan P, const void* __restrict__ fin,
+template <bool REAL, bool BIG>
+__global__ void __launch_bounds__(kThreads, BIG ? 1 : 2) fwd_gamma_kernel(Geometry g, FftPlan P, const void* __restrict__ fin,
                                                               double2* __restrict__ W, int T, int ld) {
   extern __shared__ double2 sm[];
   double2* a = sm;
@@ -170,7 +197,7 @@ __global__ void __launch_bounds__(kThreads) fwd_gamma_kernel(Geometry g, FftPlan
     a[t * ld + gi] = v;
   }
   __syncthreads();
-  double2* r = fft_fwd_smem(a, b, T, ld, P);
+  double2* r = run_fft<BIG>(a, b, T, ld, P);
   const double scale = 2.0 * 3.141592653589793238462643383279502884 / ng;
   for (int idx = threadIdx.x; idx < g.nplanes * T; idx += blockDim.x) {
     const int t = idx % T, p = idx / T, al = a0 + t;
@@ -180,7 +207,8 @@ __global__ void __launch_bounds__(kThreads) fwd_gamma_kernel(Geometry g, FftPlan
   }
 }
 
-__global__ void __launch_bounds__(kThreads) fwd_alpha_kernel(Geometry g, FftPlan P, double2* __restrict__ W,
+template <bool BIG>
+__global__ void __launch_bounds__(kThreads, BIG ? 1 : 2) fwd_alpha_kernel(Geometry g, FftPlan P, double2* __restrict__ W,
                                                               int T, int ld) {
   extern __shared__ double2 sm[];
   double2* a = sm;
@@ -194,7 +222,7 @@ __global__ void __launch_bounds__(kThreads) fwd_alpha_kernel(Geometry g, FftPlan
     a[j * ld + k] = v;
   }
   __syncthreads();
-  double2* r = fft_fwd_smem(a, b, T, ld, P);
+  double2* r = run_fft<BIG>(a, b, T, ld, P);
   const double inv = 1.0 / Pn;
   for (int idx = threadIdx.x; idx < T * ncols; idx += blockDim.x) {
     const int j = idx / ncols, c = idx - j * ncols, row = r0 + j;
@@ -205,7 +233,8 @@ __global__ void __launch_bounds__(kThreads) fwd_alpha_kernel(Geometry g, FftPlan
   }
 }
 
-__global__ void __launch_bounds__(kThreads) fwd_beta_conv_kernel(Geometry g, FftPlan P, FftPlan Pc,
+template <bool BIG>
+__global__ void __launch_bounds__(kThreads, BIG ? 1 : 2) fwd_beta_conv_kernel(Geometry g, FftPlan P, FftPlan Pc,
                                                                   const double2* __restrict__ wr,
                                                                   double2* __restrict__ W, int T, int ld) {
   extern __shared__ double2 sm[];
@@ -227,14 +256,15 @@ __global__ void __launch_bounds__(kThreads) fwd_beta_conv_kernel(Geometry g, Fft
     a[t * ld + row] = cscale(a[t * ld + src], sg);
   }
   __syncthreads();
-  double2* r = fft_fwd_smem(a, b, T, ld, P);
+  double2* r = run_fft<BIG>(a, b, T, ld, P);
+  // conv input: F[m''] / P with the MW phase, at m'' mod Pc, zero elsewhere
+  const double invP = 1.0 / Pn;
   double2* o = (r == a) ? b : a;
   for (int idx = threadIdx.x; idx < T * pc; idx += blockDim.x) {
     const int t = idx / pc, k = idx - t * pc;
     o[t * ld + k] = make_double2(0.0, 0.0);
   }
   __syncthreads();
-  const double invP = 1.0 / Pn;
   for (int idx = threadIdx.x; idx < T * (2 * L - 1); idx += blockDim.x) {
     const int t = idx / (2 * L - 1), mpp = idx - t * (2 * L - 1) - (L - 1);
     double2 v = cscale(r[t * ld + wrapi(mpp, Pn)], invP);
@@ -243,14 +273,14 @@ __global__ void __launch_bounds__(kThreads) fwd_beta_conv_kernel(Geometry g, Fft
   }
   __syncthreads();
   double2* o2 = (o == a) ? b : a;
-  double2* q = fft_fwd_smem(o, o2, T, ld, Pc);  // conj of the inverse DFT
+  double2* q = run_fft<BIG>(o, o2, T, ld, Pc);  // conj of the inverse DFT
   for (int idx = threadIdx.x; idx < T * pc; idx += blockDim.x) {
     const int t = idx / pc, k = idx - t * pc;
     q[t * ld + k] = cmul(cconj(q[t * ld + k]), __ldg(wr + k));
   }
   __syncthreads();
   double2* q2 = (q == a) ? b : a;
-  double2* G = fft_fwd_smem(q, q2, T, ld, Pc);
+  double2* G = run_fft<BIG>(q, q2, T, ld, Pc);
   for (int idx = threadIdx.x; idx < L * T; idx += blockDim.x) {
     const int t = idx % T, mp = idx / T, c = c0 + t;
     if (c >= ncols) continue;
@@ -268,11 +298,17 @@ __global__ void __launch_bounds__(kThreads) fwd_beta_conv_kernel(Geometry g, Fft
 // ------------------------------------------------------------------ launchers
 int launch_inv_beta(const Geometry& g, const FftPlan& p, double2* W, cudaStream_t s) {
   const int ld = p.ld();
-  const int T = pick_T(ld, 2, 8);
-  const size_t sm = 2 * (size_t)T * ld * sizeof(double2);
-  if (int rc = set_smem(inv_beta_kernel, sm)) return rc;
+  const Sizing z = size_for(p.big(), ld, 16);
+  const int T = z.T;
+  const size_t sm = z.smem;
   dim3 grid((2 * g.L - 1 + T - 1) / T, g.nplanes);
-  inv_beta_kernel<<<grid, kThreads, sm, s>>>(g, p, W, T, ld);
+  if (p.big()) {
+    if (int rc = set_smem(inv_beta_kernel<true>, sm)) return rc;
+    inv_beta_kernel<true><<<grid, kThreads, sm, s>>>(g, p, W, T, ld);
+  } else {
+    if (int rc = set_smem(inv_beta_kernel<false>, sm)) return rc;
+    inv_beta_kernel<false><<<grid, kThreads, sm, s>>>(g, p, W, T, ld);
+  }
   SO3G_LAUNCHED();
   SO3G_CUDA(cudaGetLastError());
   return kOk;
@@ -280,11 +316,17 @@ int launch_inv_beta(const Geometry& g, const FftPlan& p, double2* W, cudaStream_
 
 int launch_inv_alpha(const Geometry& g, const FftPlan& p, double2* W, cudaStream_t s) {
   const int ld = p.ld();
-  const int T = pick_T(ld, 2, 8);
-  const size_t sm = 2 * (size_t)T * ld * sizeof(double2);
-  if (int rc = set_smem(inv_alpha_kernel, sm)) return rc;
+  const Sizing z = size_for(p.big(), ld, 16);
+  const int T = z.T;
+  const size_t sm = z.smem;
   const int nrows = g.nplanes * g.nb;
-  inv_alpha_kernel<<<(nrows + T - 1) / T, kThreads, sm, s>>>(g, p, W, T, ld);
+  if (p.big()) {
+    if (int rc = set_smem(inv_alpha_kernel<true>, sm)) return rc;
+    inv_alpha_kernel<true><<<(nrows + T - 1) / T, kThreads, sm, s>>>(g, p, W, T, ld);
+  } else {
+    if (int rc = set_smem(inv_alpha_kernel<false>, sm)) return rc;
+    inv_alpha_kernel<false><<<(nrows + T - 1) / T, kThreads, sm, s>>>(g, p, W, T, ld);
+  }
   SO3G_LAUNCHED();
   SO3G_CUDA(cudaGetLastError());
   return kOk;
@@ -292,16 +334,21 @@ int launch_inv_alpha(const Geometry& g, const FftPlan& p, double2* W, cudaStream
 
 int launch_inv_gamma(const Geometry& g, const FftPlan& p, const double2* W, void* f, cudaStream_t s) {
   const int ld = p.ld() > g.nplanes ? p.ld() : g.nplanes;
-  const int T = pick_T(ld, 2, 16);
-  const size_t sm = 2 * (size_t)T * ld * sizeof(double2);
+  const Sizing z = size_for(p.big(), ld, 16);
+  const int T = z.T;
+  const size_t sm = z.smem;
   dim3 grid((g.na + T - 1) / T, g.nb);
+#define SO3G_GAMMA_INV(R, B)                                                  \
+  do {                                                                        \
+    if (int rc = set_smem(inv_gamma_kernel<R, B>, sm)) return rc;             \
+    inv_gamma_kernel<R, B><<<grid, kThreads, sm, s>>>(g, p, W, f, T, ld);     \
+  } while (0)
   if (g.real) {
-    if (int rc = set_smem(inv_gamma_kernel<true>, sm)) return rc;
-    inv_gamma_kernel<true><<<grid, kThreads, sm, s>>>(g, p, W, f, T, ld);
+    if (p.big()) SO3G_GAMMA_INV(true, true); else SO3G_GAMMA_INV(true, false);
   } else {
-    if (int rc = set_smem(inv_gamma_kernel<false>, sm)) return rc;
-    inv_gamma_kernel<false><<<grid, kThreads, sm, s>>>(g, p, W, f, T, ld);
+    if (p.big()) SO3G_GAMMA_INV(false, true); else SO3G_GAMMA_INV(false, false);
   }
+#undef SO3G_GAMMA_INV
   SO3G_LAUNCHED();
   SO3G_CUDA(cudaGetLastError());
   return kOk;
@@ -309,16 +356,21 @@ int launch_inv_gamma(const Geometry& g, const FftPlan& p, const double2* W, void
 
 int launch_fwd_gamma(const Geometry& g, const FftPlan& p, const void* f, double2* W, cudaStream_t s) {
   const int ld = p.ld();
-  const int T = pick_T(ld, 2, 16);
-  const size_t sm = 2 * (size_t)T * ld * sizeof(double2);
+  const Sizing z = size_for(p.big(), ld, 16);
+  const int T = z.T;
+  const size_t sm = z.smem;
   dim3 grid((g.na + T - 1) / T, g.nb);
+#define SO3G_GAMMA_FWD(R, B)                                                  \
+  do {                                                                        \
+    if (int rc = set_smem(fwd_gamma_kernel<R, B>, sm)) return rc;             \
+    fwd_gamma_kernel<R, B><<<grid, kThreads, sm, s>>>(g, p, f, W, T, ld);     \
+  } while (0)
   if (g.real) {
-    if (int rc = set_smem(fwd_gamma_kernel<true>, sm)) return rc;
-    fwd_gamma_kernel<true><<<grid, kThreads, sm, s>>>(g, p, f, W, T, ld);
+    if (p.big()) SO3G_GAMMA_FWD(true, true); else SO3G_GAMMA_FWD(true, false);
   } else {
-    if (int rc = set_smem(fwd_gamma_kernel<false>, sm)) return rc;
-    fwd_gamma_kernel<false><<<grid, kThreads, sm, s>>>(g, p, f, W, T, ld);
+    if (p.big()) SO3G_GAMMA_FWD(false, true); else SO3G_GAMMA_FWD(false, false);
   }
+#undef SO3G_GAMMA_FWD
   SO3G_LAUNCHED();
   SO3G_CUDA(cudaGetLastError());
   return kOk;
@@ -326,11 +378,17 @@ int launch_fwd_gamma(const Geometry& g, const FftPlan& p, const void* f, double2
 
 int launch_fwd_alpha(const Geometry& g, const FftPlan& p, double2* W, cudaStream_t s) {
   const int ld = p.ld();
-  const int T = pick_T(ld, 2, 8);
-  const size_t sm = 2 * (size_t)T * ld * sizeof(double2);
-  if (int rc = set_smem(fwd_alpha_kernel, sm)) return rc;
+  const Sizing z = size_for(p.big(), ld, 16);
+  const int T = z.T;
+  const size_t sm = z.smem;
   const int nrows = g.nplanes * g.nb;
-  fwd_alpha_kernel<<<(nrows + T - 1) / T, kThreads, sm, s>>>(g, p, W, T, ld);
+  if (p.big()) {
+    if (int rc = set_smem(fwd_alpha_kernel<true>, sm)) return rc;
+    fwd_alpha_kernel<true><<<(nrows + T - 1) / T, kThreads, sm, s>>>(g, p, W, T, ld);
+  } else {
+    if (int rc = set_smem(fwd_alpha_kernel<false>, sm)) return rc;
+    fwd_alpha_kernel<false><<<(nrows + T - 1) / T, kThreads, sm, s>>>(g, p, W, T, ld);
+  }
   SO3G_LAUNCHED();
   SO3G_CUDA(cudaGetLastError());
   return kOk;
@@ -339,11 +397,17 @@ int launch_fwd_alpha(const Geometry& g, const FftPlan& p, double2* W, cudaStream
 int launch_fwd_beta_conv(const Geometry& g, const FftPlan& p, const FftPlan& pc, const double2* wr, double2* W,
                          cudaStream_t s) {
   int ld = p.ld() > pc.ld() ? p.ld() : pc.ld();
-  const int T = pick_T(ld, 2, 8);
-  const size_t sm = 2 * (size_t)T * ld * sizeof(double2);
-  if (int rc = set_smem(fwd_beta_conv_kernel, sm)) return rc;
+  const Sizing z = size_for(p.big() || pc.big(), ld, 8);
+  const int T = z.T;
+  const size_t sm = z.smem;
   dim3 grid((2 * g.L - 1 + T - 1) / T, g.nplanes);
-  fwd_beta_conv_kernel<<<grid, kThreads, sm, s>>>(g, p, pc, wr, W, T, ld);
+  if (p.big() || pc.big()) {
+    if (int rc = set_smem(fwd_beta_conv_kernel<true>, sm)) return rc;
+    fwd_beta_conv_kernel<true><<<grid, kThreads, sm, s>>>(g, p, pc, wr, W, T, ld);
+  } else {
+    if (int rc = set_smem(fwd_beta_conv_kernel<false>, sm)) return rc;
+    fwd_beta_conv_kernel<false><<<grid, kThreads, sm, s>>>(g, p, pc, wr, W, T, ld);
+  }
   SO3G_LAUNCHED();
   SO3G_CUDA(cudaGetLastError());
   return kOk;

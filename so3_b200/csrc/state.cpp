@@ -1,6 +1,7 @@
 // Per-device state of libso3gpu: error reporting, resident Wigner tables, FFT
 // plans, block-offset tables and grow-only scratch.  Host code only.
 #include <cmath>
+#include <cstdlib>
 #include <complex>
 #include <cstdio>
 #include <cstring>
@@ -262,7 +263,8 @@ static void fft_ld(std::vector<cld>& x, int sign) {
 }
 
 int ensure_fft(Device* D, int n, FftPlan* out) {
-  auto it = D->ffts.find(n);
+  const int key = n;
+  auto it = D->ffts.find(key);
   if (it != D->ffts.end()) {
     *out = it->second->plan;
     return kOk;
@@ -319,7 +321,7 @@ int ensure_fft(Device* D, int n, FftPlan* out) {
     P.kern = dp->mem + P.m + n;
   }
   *out = P;
-  D->ffts[n] = std::move(dp);
+  D->ffts[key] = std::move(dp);
   return kOk;
 }
 

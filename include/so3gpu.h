@@ -64,6 +64,19 @@ int so3gpu_stage_times(so3gpu_context *ctx, double *total_ms, long long *counts,
  * (2 flops per FMA), from a register-resident FMA chain kernel. */
 double so3gpu_measure_fp64_peak(int device);
 
+/* Complex inverse transform (same result as so3gpu_inverse) that allocates
+ * no device memory; no counterpart in the reference.  For callers that cannot
+ * call cudaMalloc (code running under a foreign allocator or memory cap, or
+ * loops that must not allocate after start-up).  f and flmn are device
+ * pointers; stream is a cudaStream_t (NULL: legacy default stream).  Its
+ * scratch, Wigner tables and FFT tables are file-scope device arrays (about
+ * 18 MB, held by every GPU that loads the library until exit); transforms
+ * needing more than 16 MiB of scratch, L > 64 or N > 64 return status 3.
+ * The first call on a device builds the tables and waits for them: make it
+ * before any stream capture.  Calls share the arrays, so calls whose GPU work
+ * overlaps race: serialise them. */
+int so3gpu_inverse_noalloc(void *f, const void *flmn, const so3_parameters_t *parameters, void *stream);
+
 /* Diagnostics. */
 int so3gpu_last_status(void);
 const char *so3gpu_last_error(void);

@@ -165,6 +165,8 @@ int require_mw(const so3_parameters_t* p) {
 
 }  // namespace
 
+void so3g_record_status(int rc) { t_status = rc; }
+
 struct so3gpu_context {
   int device = 0;
   cudaStream_t stream = nullptr;

@@ -177,3 +177,6 @@ const std::string& last_error();
 int validate(const so3_parameters_t& p, int real);
 
 }  // namespace so3g
+
+// Records the status of the calling thread's last call (so3gpu_last_status).
+void so3g_record_status(int rc);

@@ -215,19 +215,17 @@ def run_ours(a):
     import torch.distributed as dist
 
     import so3_b200 as so3
+    from so3_b200 import dist as sdist
     from so3_b200 import synth
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    info = sdist.rank_info()
+    world, rank, local = info.world, info.rank, info.local
     torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    sdist.init("nccl" if world > 1 else None, timeout_s=120)
 
     L, N = a.L, a.N
     p = so3.SO3Parameters(L=L, N=N, L0=0, sampling_scheme=0, n_order=1, storage=0, n_mode=0, dl_method=0)
-    fl_host = synth.gen_flmn(p, 1000 + rank, "uniform")
+    fl_host = synth.gen_flmn(p, sdist.signal_seed(1000, rank, 0), "uniform")
     stream = torch.cuda.current_stream()
     d_flmn = torch.from_numpy(fl_host).to(f"cuda:{local}")
     d_f = torch.empty(so3.f_size(p), dtype=torch.complex128, device=f"cuda:{local}")
@@ -244,7 +242,7 @@ def run_ours(a):
         step()
     torch.cuda.synchronize()
     if world > 1:
-        dist.barrier()
+        sdist.barrier()
     ctx.stage_timing(True)
     ctx.stage_times()
     evs = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps + 1)]
@@ -261,11 +259,8 @@ def run_ours(a):
     ctx.stage_timing(False)
     total_ms = evs[0].elapsed_time(evs[-1])
     lat = [evs[i].elapsed_time(evs[i + 1]) for i in range(a.steps)]
-    t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
-    value = world * a.steps / (total_ms / 1e3)
+    total_ms = sdist.max_over_ranks(total_ms, device=f"cuda:{local}")
+    value = sdist.job_throughput(world * a.steps, total_ms / 1e3)
     rt_err = float(((d_back - d_flmn).abs().max() / d_flmn.abs().max()).item())
 
     # ---- roofline of the dominant kernel
@@ -320,9 +315,7 @@ def run_ours(a):
                 "gpu_launches": int(launches), "roofline": roof, "e2e": e2e, "cpu_baseline": cpu,
                 "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    sdist.finalize()
 
 
 def run_e2e(so3, p, fl_host, steps, local, world, dist):
@@ -332,6 +325,8 @@ def run_e2e(so3, p, fl_host, steps, local, world, dist):
 
     import numpy as np
     import torch
+
+    from so3_b200 import dist as sdist
     lib = so3._lib.load()
     q = p.to_struct()
     fl_pin = torch.from_numpy(fl_host).pin_memory()
@@ -348,15 +343,12 @@ def run_e2e(so3, p, fl_host, steps, local, world, dist):
     step()  # warm-up (staging buffers)
     torch.cuda.synchronize()
     if world > 1:
-        dist.barrier()
+        sdist.barrier()
     t0 = time.perf_counter()
     for _ in range(steps):
         step()
     el = time.perf_counter() - t0
-    t = torch.tensor([el], dtype=torch.float64, device=f"cuda:{local}")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    el = float(t.item())
+    el = sdist.max_over_ranks(el, device=f"cuda:{local}")
     err = float(np.abs(back_pin.numpy() - fl_host).max() / np.abs(fl_host).max())
     nb_fl = fl_host.size * 16
     nb_f = so3.f_size(p) * 16

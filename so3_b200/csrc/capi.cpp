@@ -62,7 +62,9 @@ struct DropIn {
   std::mutex mu;
   Workspace wk;
   Staging io[4];
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;              // kernels
+  cudaStream_t cin = nullptr, cout = nullptr;  // host->device / device->host copies
+  cudaEvent_t ev[2 * so3g::kMaxChunks] = {};
 };
 
 std::mutex g_dropin_mu;
@@ -80,6 +82,9 @@ DropIn* dropin(int dev) {
   if (!slot) {
     slot = std::make_unique<DropIn>();
     cudaStreamCreateWithFlags(&slot->stream, cudaStreamNonBlocking);
+    cudaStreamCreateWithFlags(&slot->cin, cudaStreamNonBlocking);
+    cudaStreamCreateWithFlags(&slot->cout, cudaStreamNonBlocking);
+    for (cudaEvent_t& e : slot->ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   }
   return slot.get();
 }
@@ -123,6 +128,42 @@ size_t flmn_bytes(const so3_parameters_t* p, int real) {
   return (size_t)so3_sampling_flmn_size(&q) * sizeof(cd);
 }
 
+// Device buffer for one side of a staged call: the caller's own buffer when
+// the GPU can address it (no copies), else a staging buffer.
+int stage_side(DropIn* X, int slot, const void* user, size_t bytes, void** dev, bool* host) {
+  *host = !device_accessible(user);
+  if (!*host) {
+    *dev = const_cast<void*>(user);
+    return so3g::kOk;
+  }
+  return X->io[slot].get(bytes ? bytes : 16, dev);
+}
+
+// Waits for the copies and kernels of a staged call (also after a failure,
+// so nothing still reads or writes the caller's buffers on return).
+int drain(DropIn* X, int rc) {
+  const cudaError_t a = cudaStreamSynchronize(X->cin);
+  const cudaError_t b = cudaStreamSynchronize(X->stream);
+  const cudaError_t c = cudaStreamSynchronize(X->cout);
+  if (rc) return rc;
+  const cudaError_t e = a != cudaSuccess ? a : (b != cudaSuccess ? b : c);
+  if (e != cudaSuccess) return so3g::fail(so3g::kCudaError, std::string("staged transform: ") + cudaGetErrorString(e));
+  return so3g::kOk;
+}
+
+so3g::StagedIo staged_io(DropIn* X, const void* in_user, void* din, bool in_host, void* out_user, void* dout,
+                         bool out_host) {
+  so3g::StagedIo io;
+  io.host_in = in_host ? in_user : nullptr;
+  io.host_out = out_host ? out_user : nullptr;
+  io.dev_in = din;
+  io.dev_out = dout;
+  io.cin = X->cin;
+  io.cout = X->cout;
+  for (int i = 0; i < 2 * so3g::kMaxChunks; i++) io.ev[i] = X->ev[i];
+  return io;
+}
+
 int dropin_inverse(void* f, const void* flmn, const so3_parameters_t* p, int real) {
   if (!p) return so3g::fail(so3g::kInvalidParameter, "null parameters");
   if (int rc = so3g::validate(*p, real)) return rc;
@@ -131,11 +172,11 @@ int dropin_inverse(void* f, const void* flmn, const so3_parameters_t* p, int rea
   DropIn* X = dropin(dev);
   std::lock_guard<std::mutex> lk(X->mu);
   void *din, *dout;
-  bool sin_, sout;
-  if (int rc = device_view(X, 0, flmn, flmn_bytes(p, real), true, &din, &sin_)) return rc;
-  if (int rc = device_view(X, 1, f, f_bytes(p, real), false, &dout, &sout)) return rc;
-  if (int rc = so3g::run_inverse(so3g::device_state(dev), &X->wk, *p, din, dout, real, X->stream)) return rc;
-  return download(X, f, dout, f_bytes(p, real), sout);
+  bool hin, hout;
+  if (int rc = stage_side(X, 0, flmn, flmn_bytes(p, real), &din, &hin)) return rc;
+  if (int rc = stage_side(X, 1, f, f_bytes(p, real), &dout, &hout)) return rc;
+  const so3g::StagedIo io = staged_io(X, flmn, din, hin, f, dout, hout);
+  return drain(X, so3g::run_inverse_staged(so3g::device_state(dev), &X->wk, *p, real, io, X->stream));
 }
 
 int dropin_forward(void* flmn, const void* f, const so3_parameters_t* p, int real, bool zero_first) {
@@ -146,15 +187,14 @@ int dropin_forward(void* flmn, const void* f, const so3_parameters_t* p, int rea
   DropIn* X = dropin(dev);
   std::lock_guard<std::mutex> lk(X->mu);
   void *din, *dout;
-  bool sin_, sout;
-  const size_t nb = flmn_bytes(p, real);
-  // Skipped n-blocks keep the caller's contents (reference semantics).
-  const bool keep = !zero_first && p->n_mode != SO3_N_MODE_ALL && p->n_mode != SO3_N_MODE_L;
-  if (int rc = device_view(X, 0, f, f_bytes(p, real), true, &din, &sin_)) return rc;
-  if (int rc = device_view(X, 1, flmn, nb, keep, &dout, &sout)) return rc;
-  if (zero_first) SO3G_CUDA(cudaMemsetAsync(dout, 0, nb, X->stream));
-  if (int rc = so3g::run_forward(so3g::device_state(dev), &X->wk, *p, din, dout, real, X->stream)) return rc;
-  return download(X, flmn, dout, nb, sout);
+  bool hin, hout;
+  // Skipped n-blocks of a host output are never copied back, so they keep the
+  // caller's contents (reference semantics); a device output is written only
+  // where the transform computes.
+  if (int rc = stage_side(X, 0, f, f_bytes(p, real), &din, &hin)) return rc;
+  if (int rc = stage_side(X, 1, flmn, flmn_bytes(p, real), &dout, &hout)) return rc;
+  const so3g::StagedIo io = staged_io(X, f, din, hin, flmn, dout, hout);
+  return drain(X, so3g::run_forward_staged(so3g::device_state(dev), &X->wk, *p, real, zero_first, io, X->stream));
 }
 
 int require_mw(const so3_parameters_t* p) {

@@ -114,6 +114,7 @@ struct InvArgs {
   const double* dl;
   double2* W;
   int L, N, L0, plane0, n_mode, real, sym_n0;
+  int nu_lo, nu_hi;  // |n| range [nu_lo, nu_hi) of this launch
   long long RS, PS;
 };
 
@@ -123,11 +124,11 @@ __global__ void __launch_bounds__(kThreads, 1) inverse_contract_kernel(InvArgs a
   extern __shared__ __align__(16) unsigned char smraw[];
   Slab* st = reinterpret_cast<Slab*>(smraw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, lm = lane & 7, lu = lane >> 3;
-  const int nu0 = blockIdx.x * kNG, mp0 = blockIdx.y * kRows, mu0 = blockIdx.z * kCols;
+  const int nu0 = a.nu_lo + blockIdx.x * kNG, mp0 = blockIdx.y * kRows, mu0 = blockIdx.z * kCols;
   const int L = a.L;
   bool act[kNG];
 #pragma unroll
-  for (int j = 0; j < kNG; j++) act[j] = (nu0 + j < a.N) && !plane_skipped(a.n_mode, a.N, nu0 + j);
+  for (int j = 0; j < kNG; j++) act[j] = (nu0 + j < a.nu_hi) && !plane_skipped(a.n_mode, a.N, nu0 + j);
 
   double2 acc[kPer][kNG][4];
 #pragma unroll
@@ -212,7 +213,7 @@ __global__ void __launch_bounds__(kThreads, 1) inverse_contract_kernel(InvArgs a
 #pragma unroll
     for (int j = 0; j < kNG; j++) {
       const int nu = nu0 + j;
-      if (nu >= a.N) continue;
+      if (nu >= a.nu_hi) continue;
 #pragma unroll
       for (int s = 0; s < NSIGN; s++) {
         const int ms = (s & 1) ? -1 : 1, ns = (s & 2) ? -1 : 1;
@@ -229,9 +230,11 @@ __global__ void __launch_bounds__(kThreads, 1) inverse_contract_kernel(InvArgs a
 }
 
 int launch_inverse_contract(const Geometry& g, int n_mode, const double2* flmn, const long long* bases,
-                            const double* dl, double2* W, int sym_n0, cudaStream_t s) {
-  InvArgs a{flmn, bases, dl, W, g.L, g.N, g.L0, g.plane0, n_mode, g.real, sym_n0, g.RS, g.PS};
-  dim3 grid((g.N + kNG - 1) / kNG, (g.L + kRows - 1) / kRows, (g.L + kCols - 1) / kCols);
+                            const double* dl, double2* W, int sym_n0, cudaStream_t s, int nu_lo, int nu_hi) {
+  if (nu_hi < 0 || nu_hi > g.N) nu_hi = g.N;
+  if (nu_lo >= nu_hi) return kOk;
+  InvArgs a{flmn, bases, dl, W, g.L, g.N, g.L0, g.plane0, n_mode, g.real, sym_n0, nu_lo, nu_hi, g.RS, g.PS};
+  dim3 grid((nu_hi - nu_lo + kNG - 1) / kNG, (g.L + kRows - 1) / kRows, (g.L + kCols - 1) / kCols);
   if (g.real) {
     SO3G_CUDA(cudaFuncSetAttribute(inverse_contract_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));
     inverse_contract_kernel<2><<<grid, kThreads, kSmem, s>>>(a);
@@ -251,6 +254,7 @@ struct FwdArgs {
   const double* dl;
   double2* flmn;
   int L, N, L0, plane0, n_mode, real, compact;
+  int nu_lo, nu_hi;  // |n| range [nu_lo, nu_hi) of this launch
   long long RS, PS;
 };
 
@@ -259,11 +263,11 @@ __global__ void __launch_bounds__(kThreads, 1) forward_contract_kernel(FwdArgs a
   extern __shared__ __align__(16) unsigned char smraw[];
   Slab* st = reinterpret_cast<Slab*>(smraw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, lm = lane & 7, lu = lane >> 3;
-  const int nu0 = blockIdx.x * kNG, l0 = blockIdx.y * kRows, mu0 = blockIdx.z * kCols;
+  const int nu0 = a.nu_lo + blockIdx.x * kNG, l0 = blockIdx.y * kRows, mu0 = blockIdx.z * kCols;
   const int L = a.L;
   bool act[kNG];
 #pragma unroll
-  for (int j = 0; j < kNG; j++) act[j] = (nu0 + j < a.N) && !plane_skipped(a.n_mode, a.N, nu0 + j);
+  for (int j = 0; j < kNG; j++) act[j] = (nu0 + j < a.nu_hi) && !plane_skipped(a.n_mode, a.N, nu0 + j);
   if (!act[0] && !act[1]) return;  // caller-zeroed blocks stay untouched
 
   double2 acc[kPer][kNG][4];
@@ -356,9 +360,12 @@ __global__ void __launch_bounds__(kThreads, 1) forward_contract_kernel(FwdArgs a
 }
 
 int launch_forward_contract(const Geometry& g, int n_mode, const double2* W, const long long* bases,
-                            const double* dl, double2* flmn, int storage_compact, cudaStream_t s) {
-  FwdArgs a{W, bases, dl, flmn, g.L, g.N, g.L0, g.plane0, n_mode, g.real, storage_compact, g.RS, g.PS};
-  dim3 grid((g.N + kNG - 1) / kNG, (g.L + kRows - 1) / kRows, (g.L + kCols - 1) / kCols);
+                            const double* dl, double2* flmn, int storage_compact, cudaStream_t s, int nu_lo,
+                            int nu_hi) {
+  if (nu_hi < 0 || nu_hi > g.N) nu_hi = g.N;
+  if (nu_lo >= nu_hi) return kOk;
+  FwdArgs a{W, bases, dl, flmn, g.L, g.N, g.L0, g.plane0, n_mode, g.real, storage_compact, nu_lo, nu_hi, g.RS, g.PS};
+  dim3 grid((nu_hi - nu_lo + kNG - 1) / kNG, (g.L + kRows - 1) / kRows, (g.L + kCols - 1) / kCols);
   if (g.real) {
     SO3G_CUDA(cudaFuncSetAttribute(forward_contract_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));
     forward_contract_kernel<2><<<grid, kThreads, kSmem, s>>>(a);

@@ -1,6 +1,9 @@
 // Transform drivers: stage order of the inverse and forward Wigner transforms
 // on device pointers.  Host code only; every kernel runs on stream s.
+#include <algorithm>
 #include <cstdlib>
+#include <utility>
+#include <vector>
 
 #include "so3gpu_internal.h"
 
@@ -85,6 +88,190 @@ int run_forward(Device* D, Workspace* wk, const so3_parameters_t& p, const void*
                                p.storage == SO3_STORAGE_COMPACT, s);
   if (rc) return rc;
   timer_end(T, s, kStFwdContract, ev);
+  return kOk;
+}
+
+// ------------------------------------------------------------ staged drop-in
+namespace {
+
+typedef std::vector<std::pair<long long, long long>> Ranges;
+
+// Element ranges [begin, end) of the coefficient blocks of the planes with |n|
+// in [nu_lo, nu_hi), merged where adjacent.  Block n holds l >= |n| (compact)
+// or l >= 0 (padded) up to L-1, element (l, m) at base[n] + l*l + l + m.
+Ranges block_ranges(const std::vector<long long>& base, const Geometry& g, int compact, int n_mode, int nu_lo,
+                    int nu_hi, bool skip_inactive) {
+  Ranges r;
+  const long long L2 = (long long)g.L * g.L;
+  for (int nu = nu_lo; nu < nu_hi; nu++)
+    for (int neg = 0; neg < (g.real ? 1 : 2); neg++) {
+      if (neg && nu == 0) continue;
+      const int n = neg ? -nu : nu;
+      if (skip_inactive && plane_skipped(n_mode, g.N, n)) continue;
+      const long long b = base[g.plane0 + n];
+      r.push_back({b + (compact ? (long long)nu * nu : 0), b + L2});
+    }
+  std::sort(r.begin(), r.end());
+  Ranges m;
+  for (const auto& x : r) {
+    if (!m.empty() && m.back().second == x.first)
+      m.back().second = x.second;
+    else
+      m.push_back(x);
+  }
+  return m;
+}
+
+// Size from which a staged side is split into chunks (64 MiB; the
+// environment variable SO3GPU_STAGE_CHUNK_BYTES overrides it, which the tests
+// use to exercise the chunked path at small sizes).
+size_t chunk_threshold() {
+  const char* e = getenv("SO3GPU_STAGE_CHUNK_BYTES");
+  if (e && *e) return (size_t)strtoull(e, nullptr, 10);
+  return size_t(64) << 20;
+}
+
+// Chunk boundaries b[0] = 0 < ... < b[k] = total, interior ones multiples of
+// align; returns k (1 when the data are too small for overlap to pay).
+int split(int total, size_t bytes, int align, int* b) {
+  int k = bytes > 0 && bytes >= chunk_threshold() ? kMaxChunks : 1;
+  int nb = 0;
+  b[nb++] = 0;
+  for (int i = 1; i < k; i++) {
+    int v = (int)((long long)total * i / k);
+    v -= v % align;
+    if (v > b[nb - 1] && v < total) b[nb++] = v;
+  }
+  b[nb] = total;
+  return nb;
+}
+
+int copy_blocks(void* dst, const void* src, const Ranges& r, cudaMemcpyKind kind, cudaStream_t s) {
+  for (const auto& x : r)
+    SO3G_CUDA(cudaMemcpyAsync(static_cast<char*>(dst) + x.first * 16, static_cast<const char*>(src) + x.first * 16,
+                              (size_t)(x.second - x.first) * 16, kind, s));
+  return kOk;
+}
+
+// beta rows [r0, r1) of every gamma plane of a sample array f[g][b][a]
+int copy_rows(void* dst, const void* src, const Geometry& g, int r0, int r1, cudaMemcpyKind kind, cudaStream_t s) {
+  const size_t es = g.real ? sizeof(double) : sizeof(double2);
+  const size_t pitch = (size_t)g.nb * g.na * es, off = (size_t)r0 * g.na * es;
+  SO3G_CUDA(cudaMemcpy2DAsync(static_cast<char*>(dst) + off, pitch, static_cast<const char*>(src) + off, pitch,
+                              (size_t)(r1 - r0) * g.na * es, g.ng, kind, s));
+  return kOk;
+}
+
+}  // namespace
+
+int run_inverse_staged(Device* D, Workspace* wk, const so3_parameters_t& p, int real, const StagedIo& io,
+                       cudaStream_t s) {
+  Resources r;
+  if (int rc = acquire(D, p, real, s, &r, false)) return rc;
+  void* ws = nullptr;
+  if (int rc = ensure_ws(wk, workspace_bytes(p, real), &ws)) return rc;
+  double2* W = static_cast<double2*>(ws);
+  const Geometry& g = r.g;
+  const int sym_n0 = real && p.N == 1;
+  const int compact = p.storage == SO3_STORAGE_COMPACT;
+  const std::vector<long long> base = block_bases(p, real);
+  StageTimer* T = &wk->timer;
+  cudaEvent_t ev;
+  int rc;
+  int nb[kMaxChunks + 1], rb[kMaxChunks + 1];
+  const size_t in_bytes = (size_t)g.nplanes * g.L * g.L * 16;
+  const int kn = split(g.N, io.host_in ? in_bytes : 0, 2, nb);
+  timer_begin(T, s, &ev);
+  for (int k = 0; k < kn; k++) {
+    if (io.host_in) {
+      const Ranges cr = block_ranges(base, g, compact, p.n_mode, nb[k], nb[k + 1], true);
+      if ((rc = copy_blocks(const_cast<void*>(io.dev_in), io.host_in, cr, cudaMemcpyHostToDevice, io.cin))) return rc;
+      SO3G_CUDA(cudaEventRecord(io.ev[k], io.cin));
+      SO3G_CUDA(cudaStreamWaitEvent(s, io.ev[k], 0));
+    }
+    rc = launch_inverse_contract(g, p.n_mode, static_cast<const double2*>(io.dev_in), r.bases, r.dl, W, sym_n0, s,
+                                 nb[k], nb[k + 1]);
+    if (rc) return rc;
+  }
+  timer_end(T, s, kStInvContract, ev);
+  timer_begin(T, s, &ev);
+  if ((rc = launch_inv_beta(g, r.pP, W, s))) return rc;
+  timer_end(T, s, kStInvBeta, ev);
+  timer_begin(T, s, &ev);
+  if ((rc = launch_inv_alpha(g, r.pP, W, s))) return rc;
+  timer_end(T, s, kStInvAlpha, ev);
+  const size_t out_bytes = (size_t)g.ng * g.nb * g.na * (g.real ? 8 : 16);
+  const int kr = split(g.nb, io.host_out ? out_bytes : 0, 1, rb);
+  timer_begin(T, s, &ev);
+  for (int k = 0; k < kr; k++) {
+    if ((rc = launch_inv_gamma(g, r.pg, W, io.dev_out, s, rb[k], rb[k + 1]))) return rc;
+    if (io.host_out) SO3G_CUDA(cudaEventRecord(io.ev[kMaxChunks + k], s));
+  }
+  timer_end(T, s, kStInvGamma, ev);
+  if (io.host_out)
+    for (int k = 0; k < kr; k++) {
+      SO3G_CUDA(cudaStreamWaitEvent(io.cout, io.ev[kMaxChunks + k], 0));
+      if ((rc = copy_rows(io.host_out, io.dev_out, g, rb[k], rb[k + 1], cudaMemcpyDeviceToHost, io.cout))) return rc;
+    }
+  return kOk;
+}
+
+int run_forward_staged(Device* D, Workspace* wk, const so3_parameters_t& p, int real, bool zero_first,
+                       const StagedIo& io, cudaStream_t s) {
+  Resources r;
+  if (int rc = acquire(D, p, real, s, &r, true)) return rc;
+  void* ws = nullptr;
+  if (int rc = ensure_ws(wk, workspace_bytes(p, real), &ws)) return rc;
+  double2* W = static_cast<double2*>(ws);
+  const Geometry& g = r.g;
+  const int compact = p.storage == SO3_STORAGE_COMPACT;
+  const std::vector<long long> base = block_bases(p, real);
+  StageTimer* T = &wk->timer;
+  cudaEvent_t ev;
+  int rc;
+  int nb[kMaxChunks + 1], rb[kMaxChunks + 1];
+  const size_t in_bytes = (size_t)g.ng * g.nb * g.na * (g.real ? 8 : 16);
+  const int kr = split(g.nb, io.host_in ? in_bytes : 0, 1, rb);
+  timer_begin(T, s, &ev);
+  for (int k = 0; k < kr; k++) {
+    if (io.host_in) {
+      if ((rc = copy_rows(const_cast<void*>(io.dev_in), io.host_in, g, rb[k], rb[k + 1], cudaMemcpyHostToDevice,
+                          io.cin)))
+        return rc;
+      SO3G_CUDA(cudaEventRecord(io.ev[k], io.cin));
+      SO3G_CUDA(cudaStreamWaitEvent(s, io.ev[k], 0));
+    }
+    if ((rc = launch_fwd_gamma(g, r.pg, io.dev_in, W, s, rb[k], rb[k + 1]))) return rc;
+  }
+  timer_end(T, s, kStFwdGamma, ev);
+  timer_begin(T, s, &ev);
+  if ((rc = launch_fwd_alpha(g, r.pP, W, s))) return rc;
+  timer_end(T, s, kStFwdAlpha, ev);
+  timer_begin(T, s, &ev);
+  if ((rc = launch_fwd_beta_conv(g, r.pP, r.pc, r.wr, W, s))) return rc;
+  timer_end(T, s, kStFwdBetaConv, ev);
+  if (zero_first) {
+    const Ranges all = block_ranges(base, g, compact, p.n_mode, 0, g.N, false);
+    long long hi = 0;
+    for (const auto& x : all) hi = std::max(hi, x.second);
+    SO3G_CUDA(cudaMemsetAsync(io.dev_out, 0, (size_t)hi * 16, s));
+  }
+  const size_t out_bytes = (size_t)g.nplanes * g.L * g.L * 16;
+  const int kn = split(g.N, io.host_out ? out_bytes : 0, 2, nb);
+  timer_begin(T, s, &ev);
+  for (int k = 0; k < kn; k++) {
+    rc = launch_forward_contract(g, p.n_mode, W, r.bases, r.dl, static_cast<double2*>(io.dev_out), compact, s,
+                                 nb[k], nb[k + 1]);
+    if (rc) return rc;
+    if (io.host_out) SO3G_CUDA(cudaEventRecord(io.ev[kMaxChunks + k], s));
+  }
+  timer_end(T, s, kStFwdContract, ev);
+  if (io.host_out)
+    for (int k = 0; k < kn; k++) {
+      SO3G_CUDA(cudaStreamWaitEvent(io.cout, io.ev[kMaxChunks + k], 0));
+      const Ranges cr = block_ranges(base, g, compact, p.n_mode, nb[k], nb[k + 1], !zero_first);
+      if ((rc = copy_blocks(io.host_out, io.dev_out, cr, cudaMemcpyDeviceToHost, io.cout))) return rc;
+    }
   return kOk;
 }
 

@@ -1,0 +1,231 @@
+// Compile-time DFT plans for the lengths that dominate the transform stages.
+//
+// Same self-sorting (Stockham, decimation in time) passes as fft_core.cuh,
+// but with the length, the radix order, the number of sequences per CTA (T),
+// their shared-memory pitch (LD) and the CTA size (NT) fixed at compile time:
+// every index division becomes a multiply-shift, loop bounds are constants,
+// and the odd-radix butterfly constants come from a constant-memory table
+// (fft_trig.h) at compile-time offsets, i.e. as constant-bank operands
+// instead of registers.  Large odd
+// radices run as NG "units" per butterfly, each streaming over the R inputs
+// and accumulating one group of output pairs (q, R-q); that keeps register
+// use low enough for several CTAs per SM.  Twiddles e^{-2 pi i k/n} come
+// from the plan's root table (long double on the host, read through L1).
+#pragma once
+#include "fft_core.cuh"
+#include "fft_trig.h"
+
+namespace so3g {
+namespace fx {
+
+// Odd prime radix, whole butterfly in registers.
+template <int R>
+__device__ __forceinline__ void bfly_odd(double2* v) {
+  constexpr int H = (R - 1) / 2;
+  double2 s[H + 1], d[H + 1];
+  double2 tot = v[0];
+#pragma unroll
+  for (int r = 1; r <= H; r++) {
+    s[r] = cadd(v[r], v[R - r]);
+    d[r] = csub(v[r], v[R - r]);
+    tot = cadd(tot, s[r]);
+  }
+  const double2 v0 = v[0];
+  v[0] = tot;
+#pragma unroll
+  for (int q = 1; q <= H; q++) {
+    double ar = v0.x, ai = v0.y, br = 0.0, bi = 0.0;
+#pragma unroll
+    for (int r = 1; r <= H; r++) {
+      const int k = (r * q) % R;
+      const double c = k <= H ? kTrigCos[TrigOff<R>::v + k] : kTrigCos[TrigOff<R>::v + R - k];
+      const double sn = k <= H ? kTrigSin[TrigOff<R>::v + k] : -kTrigSin[TrigOff<R>::v + R - k];
+      ar = fma(c, s[r].x, ar);
+      ai = fma(c, s[r].y, ai);
+      br = fma(sn, d[r].x, br);
+      bi = fma(sn, d[r].y, bi);
+    }
+    v[q] = make_double2(ar + bi, ai - br);
+    v[R - q] = make_double2(ar - bi, ai + br);
+  }
+}
+
+template <int R>
+__device__ __forceinline__ void bfly_any(double2* v) {
+  if constexpr (R == 2 || R == 4 || R == 8)
+    bfly<R>(v, nullptr);
+  else
+    bfly_odd<R>(v);
+}
+
+// One output group of an odd-radix butterfly: pairs q = QA..QB (and q = 0
+// when ZERO), streaming over the inputs x_r = in[r * M] (times tw^r when
+// TW).  d receives output q at d[q * NS].
+template <int R, int QA, int QB, bool ZERO, int M, int NS, bool TW>
+__device__ __forceinline__ void odd_group(const double2* __restrict__ in, double2* __restrict__ d,
+                                          const double2* __restrict__ roots, int tw_step) {
+  constexpr int H = (R - 1) / 2;
+  constexpr int G = QB - QA + 1;
+  double2 a[G], b[G];
+#pragma unroll
+  for (int i = 0; i < G; i++) a[i] = b[i] = make_double2(0.0, 0.0);
+  const double2 v0 = in[0];
+  double2 tot = v0;
+#pragma unroll
+  for (int r = 1; r <= H; r++) {
+    double2 xp = in[r * M], xn = in[(R - r) * M];
+    if constexpr (TW) {
+      xp = cmul(xp, __ldg(roots + r * tw_step));
+      xn = cmul(xn, __ldg(roots + (R - r) * tw_step));
+    }
+    const double2 s = cadd(xp, xn), dd = csub(xp, xn);
+    if constexpr (ZERO) tot = cadd(tot, s);
+#pragma unroll
+    for (int i = 0; i < G; i++) {
+      const int q = QA + i;
+      const int k = (r * q) % R;
+      const double c = k <= H ? kTrigCos[TrigOff<R>::v + k] : kTrigCos[TrigOff<R>::v + R - k];
+      const double sn = k <= H ? kTrigSin[TrigOff<R>::v + k] : -kTrigSin[TrigOff<R>::v + R - k];
+      a[i].x = fma(c, s.x, a[i].x);
+      a[i].y = fma(c, s.y, a[i].y);
+      b[i].x = fma(sn, dd.x, b[i].x);
+      b[i].y = fma(sn, dd.y, b[i].y);
+    }
+  }
+  if constexpr (ZERO) d[0] = tot;
+#pragma unroll
+  for (int i = 0; i < G; i++) {
+    const int q = QA + i;
+    const double ar = v0.x + a[i].x, ai = v0.y + a[i].y;
+    d[q * NS] = make_double2(ar + b[i].y, ai - b[i].x);
+    d[(R - q) * NS] = make_double2(ar - b[i].y, ai + b[i].x);
+  }
+}
+
+// One Stockham pass of radix R at stride NS over T sequences of length N
+// (sequence t at src[t * LD]).  NG > 1 splits each butterfly into NG output
+// groups handled by different threads (odd R only).
+template <int N, int R, int NS, int T, int LD, int NT, int NG>
+__device__ __forceinline__ void pass(const double2* __restrict__ src, double2* __restrict__ dst,
+                                     const double2* __restrict__ roots) {
+  constexpr int M = N / R;
+  constexpr int TSTEP = N / (NS * R);
+  constexpr int UNITS = M * NG;
+  constexpr bool TW = NS > 1;
+  for (int u = threadIdx.x; u < T * UNITS; u += NT) {
+    const int t = u / UNITS;
+    const int rem = u - t * UNITS;
+    const int g = NG == 1 ? 0 : rem / M;
+    const int j = NG == 1 ? rem : rem - g * M;
+    const int k = j % NS;
+    const double2* s = src + t * LD + j;
+    double2* d = dst + t * LD + (j / NS) * NS * R + k;
+    if constexpr (NG == 1) {
+      double2 v[R];
+      v[0] = s[0];
+#pragma unroll
+      for (int r = 1; r < R; r++) {
+        double2 x = s[r * M];
+        if constexpr (TW) x = cmul(x, __ldg(roots + r * k * TSTEP));
+        v[r] = x;
+      }
+      bfly_any<R>(v);
+#pragma unroll
+      for (int q = 0; q < R; q++) d[q * NS] = v[q];
+    } else {
+      static_assert(R % 2 == 1 && NG <= 3, "output groups need an odd radix");
+      constexpr int H = (R - 1) / 2;
+      constexpr int QS = (H + NG - 1) / NG;
+      const int tws = k * TSTEP;
+      if (g == 0) {
+        odd_group<R, 1, QS, true, M, NS, TW>(s, d, roots, tws);
+      } else if (NG == 2 || g == 1) {
+        constexpr int B = NG == 2 ? H : 2 * QS;
+        odd_group<R, QS + 1, B, false, M, NS, TW>(s, d, roots, tws);
+      } else {
+        odd_group<R, 2 * QS + 1, H, false, M, NS, TW>(s, d, roots, tws);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- plans
+// Each plan: static constexpr n (length), ld (buffer extent per sequence),
+// and run(a, b, P) -> buffer holding the result (a and b: T * LD entries).
+
+// 1023 = 31 * 11 * 3 (the MW alpha / extended-beta length at L = 512).
+template <int T, int LD, int NT>
+struct P1023 {
+  static constexpr int n = 1023, ld = 1023;
+  static __device__ __forceinline__ double2* run(double2* a, double2* b, const FftPlan& P) {
+    pass<1023, 31, 1, T, LD, NT, 3>(a, b, P.roots);
+    __syncthreads();
+    pass<1023, 11, 31, T, LD, NT, 1>(b, a, P.roots);
+    __syncthreads();
+    pass<1023, 3, 341, T, LD, NT, 1>(a, b, P.roots);
+    __syncthreads();
+    return b;
+  }
+};
+
+// 2048 = 8 * 8 * 8 * 4 (the quadrature-weight convolution length at L = 512).
+template <int T, int LD, int NT>
+struct P2048 {
+  static constexpr int n = 2048, ld = 2048;
+  static __device__ __forceinline__ double2* run(double2* a, double2* b, const FftPlan& P) {
+    pass<2048, 8, 1, T, LD, NT, 1>(a, b, P.roots);
+    __syncthreads();
+    pass<2048, 8, 8, T, LD, NT, 1>(b, a, P.roots);
+    __syncthreads();
+    pass<2048, 8, 64, T, LD, NT, 1>(a, b, P.roots);
+    __syncthreads();
+    pass<2048, 4, 512, T, LD, NT, 1>(b, a, P.roots);
+    __syncthreads();
+    return a;
+  }
+};
+
+// 256 = 8 * 8 * 4 with an explicit root table (Bluestein inner length).
+template <int T, int LD, int NT>
+__device__ __forceinline__ double2* fft256(double2* a, double2* b, const double2* roots) {
+  pass<256, 8, 1, T, LD, NT, 1>(a, b, roots);
+  __syncthreads();
+  pass<256, 8, 8, T, LD, NT, 1>(b, a, roots);
+  __syncthreads();
+  pass<256, 4, 64, T, LD, NT, 1>(a, b, roots);
+  __syncthreads();
+  return b;
+}
+
+// 127 (prime; the gamma length at N = 64) by Bluestein's algorithm over 256.
+template <int T, int LD, int NT>
+struct P127 {
+  static constexpr int n = 127, ld = 256;
+  static __device__ __forceinline__ double2* run(double2* a, double2* b, const FftPlan& P) {
+    for (int w = threadIdx.x; w < T * 256; w += NT) {
+      const int t = w >> 8, k = w & 255;
+      double2* s = a + t * LD;
+      s[k] = k < 127 ? cmul(s[k], __ldg(P.chirp + k)) : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    double2* r = fft256<T, LD, NT>(a, b, P.mroots);
+    for (int w = threadIdx.x; w < T * 256; w += NT) {
+      const int t = w >> 8, k = w & 255;
+      double2* s = r + t * LD;
+      s[k] = cconj(cmul(s[k], __ldg(P.kern + k)));
+    }
+    __syncthreads();
+    double2* o = r == a ? b : a;
+    r = fft256<T, LD, NT>(r, o, P.mroots);
+    for (int w = threadIdx.x; w < T * 127; w += NT) {
+      const int t = w / 127, k = w - t * 127;
+      double2* s = r + t * LD;
+      s[k] = cmul(__ldg(P.chirp + k), cconj(s[k]));
+    }
+    __syncthreads();
+    return r;
+  }
+};
+
+}  // namespace fx
+}  // namespace so3g

@@ -143,15 +143,23 @@ __host__ __device__ inline bool plane_skipped(int mode, int N, int n) {
   return false;
 }
 
+// nu_lo/nu_hi restrict a launch to the planes with |n| in [nu_lo, nu_hi)
+// (nu_hi < 0: up to N); ranges split at even |n| so CTAs never straddle.
 int launch_inverse_contract(const Geometry& g, int n_mode, const double2* flmn, const long long* bases,
-                            const double* dl, double2* W, int sym_n0, cudaStream_t s);
+                            const double* dl, double2* W, int sym_n0, cudaStream_t s, int nu_lo = 0,
+                            int nu_hi = -1);
 int launch_forward_contract(const Geometry& g, int n_mode, const double2* W, const long long* bases,
-                            const double* dl, double2* flmn, int storage_compact, cudaStream_t s);
+                            const double* dl, double2* flmn, int storage_compact, cudaStream_t s, int nu_lo = 0,
+                            int nu_hi = -1);
 
 int launch_inv_beta(const Geometry& g, const FftPlan& pP, double2* W, cudaStream_t s);
 int launch_inv_alpha(const Geometry& g, const FftPlan& pP, double2* W, cudaStream_t s);
-int launch_inv_gamma(const Geometry& g, const FftPlan& pg, const double2* W, void* f, cudaStream_t s);
-int launch_fwd_gamma(const Geometry& g, const FftPlan& pg, const void* f, double2* W, cudaStream_t s);
+// row_lo/row_hi restrict the gamma stages to the beta rows [row_lo, row_hi)
+// (row_hi < 0: up to nb).
+int launch_inv_gamma(const Geometry& g, const FftPlan& pg, const double2* W, void* f, cudaStream_t s,
+                     int row_lo = 0, int row_hi = -1);
+int launch_fwd_gamma(const Geometry& g, const FftPlan& pg, const void* f, double2* W, cudaStream_t s,
+                     int row_lo = 0, int row_hi = -1);
 int launch_fwd_alpha(const Geometry& g, const FftPlan& pP, double2* W, cudaStream_t s);
 int launch_fwd_beta_conv(const Geometry& g, const FftPlan& pP, const FftPlan& pc, const double2* wr,
                          double2* W, cudaStream_t s);
@@ -173,6 +181,31 @@ int run_inverse(Device* D, Workspace* wk, const so3_parameters_t& p, const void*
                 cudaStream_t s);
 int run_forward(Device* D, Workspace* wk, const so3_parameters_t& p, const void* f_d, void* flmn_d, int real,
                 cudaStream_t s);
+
+// Drop-in calls on caller buffers that may live in host memory: the
+// transform runs in chunks (|n| ranges for the contractions, beta-row ranges
+// for the gamma stages) so that the host<->device copies of one chunk overlap
+// the kernels of the others.  host_in / host_out are the caller's host
+// buffers (nullptr when that side is already device memory); dev_in / dev_out
+// are the device buffers the kernels use.  Copies run on cin / cout, ordered
+// against the compute stream s by events; the caller synchronises cout and s.
+constexpr int kMaxChunks = 8;
+struct StagedIo {
+  const void* host_in = nullptr;
+  void* host_out = nullptr;
+  const void* dev_in = nullptr;
+  void* dev_out = nullptr;
+  cudaStream_t cin = nullptr, cout = nullptr;
+  cudaEvent_t ev[2 * kMaxChunks] = {};
+};
+int run_inverse_staged(Device* D, Workspace* wk, const so3_parameters_t& p, int real, const StagedIo& io,
+                       cudaStream_t s);
+// zero_first: clear the whole coefficient array first (skipped n-blocks read
+// back as zero); otherwise skipped blocks of a host output keep the caller's
+// contents, as in the reference.
+int run_forward_staged(Device* D, Workspace* wk, const so3_parameters_t& p, int real, bool zero_first,
+                       const StagedIo& io, cudaStream_t s);
+
 const std::string& last_error();
 int validate(const so3_parameters_t& p, int real);
 

@@ -16,6 +16,7 @@
 //          phase e^{-i m'' pi/(2L-1)} (MW), convolve with the quadrature
 //          weights through a power-of-two oversampled product, and fold
 //          G[m'] + (-1)^{m+n} G[-m'] onto m' >= 0.
+#include "fft_fixed.cuh"
 #include "so3gpu_internal.h"
 
 namespace so3g {
@@ -53,13 +54,47 @@ int set_smem(K kernel, size_t bytes) {
   return kOk;
 }
 
-// Instances for plans with a radix above 8 carry the large odd-radix
-// butterflies (high register use, one CTA per SM); the others stay below 128
-// registers and run two CTAs per SM.
+// DFT engines the stage kernels are instantiated with.  Gen<BIG> runs any
+// plan from its runtime description (fft_core.cuh): instances for plans with
+// a radix above 8 carry the large odd-radix butterflies (high register use,
+// one CTA per SM), the others stay below 128 registers and run two CTAs per
+// SM.  Fix<...> runs a compile-time plan (fft_fixed.cuh) with T sequences of
+// pitch LD per CTA of NT threads; T and LD of the kernel arguments are then
+// ignored.  runP / runC are the two DFT lengths of the forward beta kernel
+// (extended beta circle, weight convolution); single-length stages use runP.
 template <bool BIG>
-__device__ __forceinline__ double2* run_fft(double2* a, double2* b, int T, int ld, const FftPlan& P) {
-  return fft_fwd_smem<BIG>(a, b, T, ld, P);
-}
+struct Gen {
+  static constexpr bool fixed = false;
+  static constexpr int NT = kThreads, MINB = BIG ? 1 : 2, T = 0, LD = 0;
+  static __device__ __forceinline__ double2* runP(double2* a, double2* b, int T_, int ld, const FftPlan& P) {
+    return fft_fwd_smem<BIG>(a, b, T_, ld, P);
+  }
+  static __device__ __forceinline__ double2* runC(double2* a, double2* b, int T_, int ld, const FftPlan& P) {
+    return fft_fwd_smem<BIG>(a, b, T_, ld, P);
+  }
+};
+
+template <template <int, int, int> class PP, template <int, int, int> class PC, int T_, int NT_, int MINB_>
+struct Fix {
+  static constexpr bool fixed = true;
+  static constexpr int NT = NT_, MINB = MINB_, T = T_;
+  static constexpr int ldP = PP<1, 1, 1>::ld, ldC = PC<1, 1, 1>::ld;
+  static constexpr int ldmax = ldP > ldC ? ldP : ldC;
+  static constexpr int LD = T_ > 1 ? ldmax + 1 : ldmax;  // odd pitch: no bank conflicts across sequences
+  static __device__ __forceinline__ double2* runP(double2* a, double2* b, int, int, const FftPlan& P) {
+    return PP<T_, LD, NT_>::run(a, b, P);
+  }
+  static __device__ __forceinline__ double2* runC(double2* a, double2* b, int, int, const FftPlan& P) {
+    return PC<T_, LD, NT_>::run(a, b, P);
+  }
+  static constexpr size_t smem() { return 2 * (size_t)T_ * LD * sizeof(double2); }
+};
+
+// alpha / extended-beta length 1023 (L = 512), gamma length 127 (N = 64), and
+// the forward beta pair 1023 / 2048.
+using E1023 = Fix<fx::P1023, fx::P1023, 1, 128, 4>;
+using E127 = Fix<fx::P127, fx::P127, 4, 128, 4>;
+using EConv1023 = Fix<fx::P1023, fx::P2048, 1, 128, 3>;
 
 __device__ __forceinline__ int wrapi(int k, int P) {
   k %= P;
@@ -73,18 +108,19 @@ __device__ __forceinline__ double2 phase(int k, int den, double sign) {  // e^{s
 }  // namespace
 
 // ------------------------------------------------------------------ inverse
-template <bool BIG>
-__global__ void __launch_bounds__(kThreads, BIG ? 1 : 2) inv_beta_kernel(Geometry g, FftPlan P, double2* __restrict__ W,
-                                                             int T, int ld) {
+template <class E>
+__global__ void __launch_bounds__(E::NT, E::MINB) inv_beta_kernel(Geometry g, FftPlan P, double2* __restrict__ W,
+                                                             int T_, int ld_) {
   extern __shared__ double2 sm[];
+  const int T = E::fixed ? E::T : T_, ld = E::fixed ? E::LD : ld_;
   double2* a = sm;
   double2* b = sm + (size_t)T * ld;
   const int plane = blockIdx.y, n = plane - g.plane0;
   const int c0 = blockIdx.x * T, ncols = 2 * g.L - 1, L = g.L, Pn = g.P;
   double2* base = W + (long long)plane * g.PS;
   if (!g.mw)
-    for (int t = threadIdx.x; t < T; t += blockDim.x) a[t * ld + L] = make_double2(0.0, 0.0);
-  for (int idx = threadIdx.x; idx < L * T; idx += blockDim.x) {
+    for (int t = threadIdx.x; t < T; t += E::NT) a[t * ld + L] = make_double2(0.0, 0.0);
+  for (int idx = threadIdx.x; idx < L * T; idx += E::NT) {
     const int t = idx % T, mp = idx / T, c = c0 + t;
     double2 v = c < ncols ? base[(long long)mp * g.RS + c] : make_double2(0.0, 0.0);
     const int m = c - (L - 1);
@@ -99,22 +135,23 @@ __global__ void __launch_bounds__(kThreads, BIG ? 1 : 2) inv_beta_kernel(Geometr
     if (mp > 0) a[t * ld + Pn - mp] = cconj(xn);
   }
   __syncthreads();
-  double2* r = run_fft<BIG>(a, b, T, ld, P);
-  for (int idx = threadIdx.x; idx < g.nb * T; idx += blockDim.x) {
+  double2* r = E::runP(a, b, T, ld, P);
+  for (int idx = threadIdx.x; idx < g.nb * T; idx += E::NT) {
     const int t = idx % T, row = idx / T, c = c0 + t;
     if (c < ncols) base[(long long)row * g.RS + c] = cconj(r[t * ld + row]);
   }
 }
 
-template <bool BIG>
-__global__ void __launch_bounds__(kThreads, BIG ? 1 : 2) inv_alpha_kernel(Geometry g, FftPlan P, double2* __restrict__ W,
-                                                              int T, int ld) {
+template <class E>
+__global__ void __launch_bounds__(E::NT, E::MINB) inv_alpha_kernel(Geometry g, FftPlan P, double2* __restrict__ W,
+                                                              int T_, int ld_) {
   extern __shared__ double2 sm[];
+  const int T = E::fixed ? E::T : T_, ld = E::fixed ? E::LD : ld_;
   double2* a = sm;
   double2* b = sm + (size_t)T * ld;
   const int L = g.L, Pn = g.P, nrows = g.nplanes * g.nb;
   const int r0 = blockIdx.x * T;
-  for (int idx = threadIdx.x; idx < T * Pn; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < T * Pn; idx += E::NT) {
     const int j = idx / Pn, k = idx - j * Pn, row = r0 + j;
     double2 v = make_double2(0.0, 0.0);
     if (row < nrows) {
@@ -127,8 +164,8 @@ __global__ void __launch_bounds__(kThreads, BIG ? 1 : 2) inv_alpha_kernel(Geomet
     a[j * ld + k] = cconj(v);
   }
   __syncthreads();
-  double2* r = run_fft<BIG>(a, b, T, ld, P);
-  for (int idx = threadIdx.x; idx < T * g.na; idx += blockDim.x) {
+  double2* r = E::runP(a, b, T, ld, P);
+  for (int idx = threadIdx.x; idx < T * g.na; idx += E::NT) {
     const int j = idx / g.na, k = idx - j * g.na, row = r0 + j;
     if (row < nrows) {
       const long long off = (long long)(row / g.nb) * g.PS + (long long)(row % g.nb) * g.RS;
@@ -137,14 +174,15 @@ __global__ void __launch_bounds__(kThreads, BIG ? 1 : 2) inv_alpha_kernel(Geomet
   }
 }
 
-template <bool REAL, bool BIG>
-__global__ void __launch_bounds__(kThreads, BIG ? 1 : 2) inv_gamma_kernel(Geometry g, FftPlan P, const double2* __restrict__ W,
-                                                              void* __restrict__ fout, int T, int ld) {
+template <bool REAL, class E>
+__global__ void __launch_bounds__(E::NT, E::MINB) inv_gamma_kernel(Geometry g, FftPlan P, const double2* __restrict__ W,
+                                                              void* __restrict__ fout, int T_, int ld_, int row0) {
   extern __shared__ double2 sm[];
+  const int T = E::fixed ? E::T : T_, ld = E::fixed ? E::LD : ld_;
   double2* a = sm;
   double2* b = sm + (size_t)T * ld;
-  const int row = blockIdx.y, a0 = blockIdx.x * T, ng = g.ng;
-  for (int idx = threadIdx.x; idx < g.nplanes * T; idx += blockDim.x) {
+  const int row = row0 + blockIdx.y, a0 = blockIdx.x * T, ng = g.ng;
+  for (int idx = threadIdx.x; idx < g.nplanes * T; idx += E::NT) {
     const int t = idx % T, p = idx / T, al = a0 + t;
     double2 v = al < g.na ? W[(long long)p * g.PS + (long long)row * g.RS + al] : make_double2(0.0, 0.0);
     if (!REAL) {
@@ -161,9 +199,9 @@ __global__ void __launch_bounds__(kThreads, BIG ? 1 : 2) inv_gamma_kernel(Geomet
     }
   }
   __syncthreads();
-  double2* r = run_fft<BIG>(a, b, T, ld, P);
+  double2* r = E::runP(a, b, T, ld, P);
   const long long plane_sz = (long long)g.nb * g.na;
-  for (int idx = threadIdx.x; idx < ng * T; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < ng * T; idx += E::NT) {
     const int t = idx % T, gi = idx / T, al = a0 + t;
     if (al >= g.na) continue;
     const long long o = (long long)gi * plane_sz + (long long)row * g.na + al;
@@ -176,15 +214,16 @@ __global__ void __launch_bounds__(kThreads, BIG ? 1 : 2) inv_gamma_kernel(Geomet
 }
 
 // ------------------------------------------------------------------ forward
-template <bool REAL, bool BIG>
-__global__ void __launch_bounds__(kThreads, BIG ? 1 : 2) fwd_gamma_kernel(Geometry g, FftPlan P, const void* __restrict__ fin,
-                                                              double2* __restrict__ W, int T, int ld) {
+template <bool REAL, class E>
+__global__ void __launch_bounds__(E::NT, E::MINB) fwd_gamma_kernel(Geometry g, FftPlan P, const void* __restrict__ fin,
+                                                              double2* __restrict__ W, int T_, int ld_, int row0) {
   extern __shared__ double2 sm[];
+  const int T = E::fixed ? E::T : T_, ld = E::fixed ? E::LD : ld_;
   double2* a = sm;
   double2* b = sm + (size_t)T * ld;
-  const int row = blockIdx.y, a0 = blockIdx.x * T, ng = g.ng;
+  const int row = row0 + blockIdx.y, a0 = blockIdx.x * T, ng = g.ng;
   const long long plane_sz = (long long)g.nb * g.na;
-  for (int idx = threadIdx.x; idx < ng * T; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < ng * T; idx += E::NT) {
     const int t = idx % T, gi = idx / T, al = a0 + t;
     double2 v = make_double2(0.0, 0.0);
     if (al < g.na) {
@@ -197,9 +236,9 @@ __global__ void __launch_bounds__(kThreads, BIG ? 1 : 2) fwd_gamma_kernel(Geomet
     a[t * ld + gi] = v;
   }
   __syncthreads();
-  double2* r = run_fft<BIG>(a, b, T, ld, P);
+  double2* r = E::runP(a, b, T, ld, P);
   const double scale = 2.0 * 3.141592653589793238462643383279502884 / ng;
-  for (int idx = threadIdx.x; idx < g.nplanes * T; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < g.nplanes * T; idx += E::NT) {
     const int t = idx % T, p = idx / T, al = a0 + t;
     if (al >= g.na) continue;
     const int k = REAL ? p : wrapi(p - g.plane0, ng);
@@ -207,24 +246,25 @@ __global__ void __launch_bounds__(kThreads, BIG ? 1 : 2) fwd_gamma_kernel(Geomet
   }
 }
 
-template <bool BIG>
-__global__ void __launch_bounds__(kThreads, BIG ? 1 : 2) fwd_alpha_kernel(Geometry g, FftPlan P, double2* __restrict__ W,
-                                                              int T, int ld) {
+template <class E>
+__global__ void __launch_bounds__(E::NT, E::MINB) fwd_alpha_kernel(Geometry g, FftPlan P, double2* __restrict__ W,
+                                                              int T_, int ld_) {
   extern __shared__ double2 sm[];
+  const int T = E::fixed ? E::T : T_, ld = E::fixed ? E::LD : ld_;
   double2* a = sm;
   double2* b = sm + (size_t)T * ld;
   const int L = g.L, Pn = g.P, nrows = g.nplanes * g.nb, ncols = 2 * L - 1;
   const int r0 = blockIdx.x * T;
-  for (int idx = threadIdx.x; idx < T * Pn; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < T * Pn; idx += E::NT) {
     const int j = idx / Pn, k = idx - j * Pn, row = r0 + j;
     double2 v = make_double2(0.0, 0.0);
     if (row < nrows) v = W[(long long)(row / g.nb) * g.PS + (long long)(row % g.nb) * g.RS + k];
     a[j * ld + k] = v;
   }
   __syncthreads();
-  double2* r = run_fft<BIG>(a, b, T, ld, P);
+  double2* r = E::runP(a, b, T, ld, P);
   const double inv = 1.0 / Pn;
-  for (int idx = threadIdx.x; idx < T * ncols; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < T * ncols; idx += E::NT) {
     const int j = idx / ncols, c = idx - j * ncols, row = r0 + j;
     if (row < nrows) {
       const int k = wrapi(c - (L - 1), Pn);
@@ -233,22 +273,23 @@ __global__ void __launch_bounds__(kThreads, BIG ? 1 : 2) fwd_alpha_kernel(Geomet
   }
 }
 
-template <bool BIG>
-__global__ void __launch_bounds__(kThreads, BIG ? 1 : 2) fwd_beta_conv_kernel(Geometry g, FftPlan P, FftPlan Pc,
+template <class E>
+__global__ void __launch_bounds__(E::NT, E::MINB) fwd_beta_conv_kernel(Geometry g, FftPlan P, FftPlan Pc,
                                                                   const double2* __restrict__ wr,
-                                                                  double2* __restrict__ W, int T, int ld) {
+                                                                  double2* __restrict__ W, int T_, int ld_) {
   extern __shared__ double2 sm[];
+  const int T = E::fixed ? E::T : T_, ld = E::fixed ? E::LD : ld_;
   double2* a = sm;
   double2* b = sm + (size_t)T * ld;
   const int plane = blockIdx.y, n = plane - g.plane0;
   const int c0 = blockIdx.x * T, L = g.L, ncols = 2 * L - 1, Pn = g.P, pc = g.Pc;
   double2* base = W + (long long)plane * g.PS;
-  for (int idx = threadIdx.x; idx < g.nb * T; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < g.nb * T; idx += E::NT) {
     const int t = idx % T, row = idx / T, c = c0 + t;
     a[t * ld + row] = c < ncols ? base[(long long)row * g.RS + c] : make_double2(0.0, 0.0);
   }
   __syncthreads();
-  for (int idx = threadIdx.x; idx < (Pn - g.nb) * T; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < (Pn - g.nb) * T; idx += E::NT) {
     const int t = idx % T, row = g.nb + idx / T, c = c0 + t;
     const int m = c - (L - 1);
     const double sg = ((m + n) & 1) ? -1.0 : 1.0;
@@ -256,16 +297,16 @@ __global__ void __launch_bounds__(kThreads, BIG ? 1 : 2) fwd_beta_conv_kernel(Ge
     a[t * ld + row] = cscale(a[t * ld + src], sg);
   }
   __syncthreads();
-  double2* r = run_fft<BIG>(a, b, T, ld, P);
+  double2* r = E::runP(a, b, T, ld, P);
   // conv input: F[m''] / P with the MW phase, at m'' mod Pc, zero elsewhere
   const double invP = 1.0 / Pn;
   double2* o = (r == a) ? b : a;
-  for (int idx = threadIdx.x; idx < T * pc; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < T * pc; idx += E::NT) {
     const int t = idx / pc, k = idx - t * pc;
     o[t * ld + k] = make_double2(0.0, 0.0);
   }
   __syncthreads();
-  for (int idx = threadIdx.x; idx < T * (2 * L - 1); idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < T * (2 * L - 1); idx += E::NT) {
     const int t = idx / (2 * L - 1), mpp = idx - t * (2 * L - 1) - (L - 1);
     double2 v = cscale(r[t * ld + wrapi(mpp, Pn)], invP);
     if (g.mw) v = cmul(v, phase(mpp, 2 * L - 1, -1.0));
@@ -273,15 +314,15 @@ __global__ void __launch_bounds__(kThreads, BIG ? 1 : 2) fwd_beta_conv_kernel(Ge
   }
   __syncthreads();
   double2* o2 = (o == a) ? b : a;
-  double2* q = run_fft<BIG>(o, o2, T, ld, Pc);  // conj of the inverse DFT
-  for (int idx = threadIdx.x; idx < T * pc; idx += blockDim.x) {
+  double2* q = E::runC(o, o2, T, ld, Pc);  // conj of the inverse DFT
+  for (int idx = threadIdx.x; idx < T * pc; idx += E::NT) {
     const int t = idx / pc, k = idx - t * pc;
     q[t * ld + k] = cmul(cconj(q[t * ld + k]), __ldg(wr + k));
   }
   __syncthreads();
   double2* q2 = (q == a) ? b : a;
-  double2* G = run_fft<BIG>(q, q2, T, ld, Pc);
-  for (int idx = threadIdx.x; idx < L * T; idx += blockDim.x) {
+  double2* G = E::runC(q, q2, T, ld, Pc);
+  for (int idx = threadIdx.x; idx < L * T; idx += E::NT) {
     const int t = idx % T, mp = idx / T, c = c0 + t;
     if (c >= ncols) continue;
     const int m = c - (L - 1);
@@ -296,121 +337,163 @@ __global__ void __launch_bounds__(kThreads, BIG ? 1 : 2) fwd_beta_conv_kernel(Ge
 }
 
 // ------------------------------------------------------------------ launchers
-int launch_inv_beta(const Geometry& g, const FftPlan& p, double2* W, cudaStream_t s) {
-  const int ld = p.ld();
-  const Sizing z = size_for(p.big(), ld, 16);
-  const int T = z.T;
-  const size_t sm = z.smem;
-  dim3 grid((2 * g.L - 1 + T - 1) / T, g.nplanes);
-  if (p.big()) {
-    if (int rc = set_smem(inv_beta_kernel<true>, sm)) return rc;
-    inv_beta_kernel<true><<<grid, kThreads, sm, s>>>(g, p, W, T, ld);
-  } else {
-    if (int rc = set_smem(inv_beta_kernel<false>, sm)) return rc;
-    inv_beta_kernel<false><<<grid, kThreads, sm, s>>>(g, p, W, T, ld);
-  }
+namespace {
+
+enum class Eng { kGenSmall, kGenBig, k1023, k127 };
+Eng pick(const FftPlan& p) {
+  if (!p.blue && p.n == 1023) return Eng::k1023;
+  if (p.blue && p.n == 127 && p.m == 256) return Eng::k127;
+  return p.big() ? Eng::kGenBig : Eng::kGenSmall;
+}
+
+// Launch geometry of one engine: sequences per CTA and shared memory.
+template <class E>
+Sizing sizing(int ld, int Tmax) {
+  if constexpr (E::fixed) return Sizing{E::T, E::smem()};
+  return size_for(E::MINB == 1, ld, Tmax);
+}
+
+template <class E>
+int inv_beta(const Geometry& g, const FftPlan& p, double2* W, cudaStream_t s) {
+  const Sizing z = sizing<E>(p.ld(), 16);
+  dim3 grid((2 * g.L - 1 + z.T - 1) / z.T, g.nplanes);
+  if (int rc = set_smem(inv_beta_kernel<E>, z.smem)) return rc;
+  inv_beta_kernel<E><<<grid, E::NT, z.smem, s>>>(g, p, W, z.T, p.ld());
+  return kOk;
+}
+template <class E>
+int inv_alpha(const Geometry& g, const FftPlan& p, double2* W, cudaStream_t s) {
+  const Sizing z = sizing<E>(p.ld(), 16);
+  const int nrows = g.nplanes * g.nb;
+  if (int rc = set_smem(inv_alpha_kernel<E>, z.smem)) return rc;
+  inv_alpha_kernel<E><<<(nrows + z.T - 1) / z.T, E::NT, z.smem, s>>>(g, p, W, z.T, p.ld());
+  return kOk;
+}
+template <bool REAL, class E>
+int inv_gamma(const Geometry& g, const FftPlan& p, const double2* W, void* f, cudaStream_t s, int row_lo,
+              int row_hi) {
+  const int ld = p.ld() > g.nplanes ? p.ld() : g.nplanes;
+  const Sizing z = sizing<E>(ld, 16);
+  dim3 grid((g.na + z.T - 1) / z.T, row_hi - row_lo);
+  if (int rc = set_smem(inv_gamma_kernel<REAL, E>, z.smem)) return rc;
+  inv_gamma_kernel<REAL, E><<<grid, E::NT, z.smem, s>>>(g, p, W, f, z.T, ld, row_lo);
+  return kOk;
+}
+template <bool REAL, class E>
+int fwd_gamma(const Geometry& g, const FftPlan& p, const void* f, double2* W, cudaStream_t s, int row_lo,
+              int row_hi) {
+  const Sizing z = sizing<E>(p.ld(), 16);
+  dim3 grid((g.na + z.T - 1) / z.T, row_hi - row_lo);
+  if (int rc = set_smem(fwd_gamma_kernel<REAL, E>, z.smem)) return rc;
+  fwd_gamma_kernel<REAL, E><<<grid, E::NT, z.smem, s>>>(g, p, f, W, z.T, p.ld(), row_lo);
+  return kOk;
+}
+template <class E>
+int fwd_alpha(const Geometry& g, const FftPlan& p, double2* W, cudaStream_t s) {
+  const Sizing z = sizing<E>(p.ld(), 16);
+  const int nrows = g.nplanes * g.nb;
+  if (int rc = set_smem(fwd_alpha_kernel<E>, z.smem)) return rc;
+  fwd_alpha_kernel<E><<<(nrows + z.T - 1) / z.T, E::NT, z.smem, s>>>(g, p, W, z.T, p.ld());
+  return kOk;
+}
+template <class E>
+int fwd_beta_conv(const Geometry& g, const FftPlan& p, const FftPlan& pc, const double2* wr, double2* W,
+                  cudaStream_t s) {
+  const int ld = p.ld() > pc.ld() ? p.ld() : pc.ld();
+  const Sizing z = sizing<E>(ld, 8);
+  dim3 grid((2 * g.L - 1 + z.T - 1) / z.T, g.nplanes);
+  if (int rc = set_smem(fwd_beta_conv_kernel<E>, z.smem)) return rc;
+  fwd_beta_conv_kernel<E><<<grid, E::NT, z.smem, s>>>(g, p, pc, wr, W, z.T, ld);
+  return kOk;
+}
+
+int launched() {
   SO3G_LAUNCHED();
   SO3G_CUDA(cudaGetLastError());
   return kOk;
+}
+
+}  // namespace
+
+int launch_inv_beta(const Geometry& g, const FftPlan& p, double2* W, cudaStream_t s) {
+  int rc;
+  switch (pick(p)) {
+    case Eng::k1023: rc = inv_beta<E1023>(g, p, W, s); break;
+    case Eng::k127: rc = inv_beta<E127>(g, p, W, s); break;
+    case Eng::kGenBig: rc = inv_beta<Gen<true>>(g, p, W, s); break;
+    default: rc = inv_beta<Gen<false>>(g, p, W, s); break;
+  }
+  return rc ? rc : launched();
 }
 
 int launch_inv_alpha(const Geometry& g, const FftPlan& p, double2* W, cudaStream_t s) {
-  const int ld = p.ld();
-  const Sizing z = size_for(p.big(), ld, 16);
-  const int T = z.T;
-  const size_t sm = z.smem;
-  const int nrows = g.nplanes * g.nb;
-  if (p.big()) {
-    if (int rc = set_smem(inv_alpha_kernel<true>, sm)) return rc;
-    inv_alpha_kernel<true><<<(nrows + T - 1) / T, kThreads, sm, s>>>(g, p, W, T, ld);
-  } else {
-    if (int rc = set_smem(inv_alpha_kernel<false>, sm)) return rc;
-    inv_alpha_kernel<false><<<(nrows + T - 1) / T, kThreads, sm, s>>>(g, p, W, T, ld);
+  int rc;
+  switch (pick(p)) {
+    case Eng::k1023: rc = inv_alpha<E1023>(g, p, W, s); break;
+    case Eng::k127: rc = inv_alpha<E127>(g, p, W, s); break;
+    case Eng::kGenBig: rc = inv_alpha<Gen<true>>(g, p, W, s); break;
+    default: rc = inv_alpha<Gen<false>>(g, p, W, s); break;
   }
-  SO3G_LAUNCHED();
-  SO3G_CUDA(cudaGetLastError());
-  return kOk;
+  return rc ? rc : launched();
 }
 
-int launch_inv_gamma(const Geometry& g, const FftPlan& p, const double2* W, void* f, cudaStream_t s) {
-  const int ld = p.ld() > g.nplanes ? p.ld() : g.nplanes;
-  const Sizing z = size_for(p.big(), ld, 16);
-  const int T = z.T;
-  const size_t sm = z.smem;
-  dim3 grid((g.na + T - 1) / T, g.nb);
-#define SO3G_GAMMA_INV(R, B)                                                  \
-  do {                                                                        \
-    if (int rc = set_smem(inv_gamma_kernel<R, B>, sm)) return rc;             \
-    inv_gamma_kernel<R, B><<<grid, kThreads, sm, s>>>(g, p, W, f, T, ld);     \
-  } while (0)
+int launch_inv_gamma(const Geometry& g, const FftPlan& p, const double2* W, void* f, cudaStream_t s, int row_lo,
+                     int row_hi) {
+  if (row_hi < 0 || row_hi > g.nb) row_hi = g.nb;
+  if (row_lo >= row_hi) return kOk;
+  int rc;
+  const Eng e = pick(p);
   if (g.real) {
-    if (p.big()) SO3G_GAMMA_INV(true, true); else SO3G_GAMMA_INV(true, false);
+    rc = e == Eng::kGenBig ? inv_gamma<true, Gen<true>>(g, p, W, f, s, row_lo, row_hi)
+                           : inv_gamma<true, Gen<false>>(g, p, W, f, s, row_lo, row_hi);
+  } else if (e == Eng::k127) {
+    rc = inv_gamma<false, E127>(g, p, W, f, s, row_lo, row_hi);
   } else {
-    if (p.big()) SO3G_GAMMA_INV(false, true); else SO3G_GAMMA_INV(false, false);
+    rc = e == Eng::kGenBig ? inv_gamma<false, Gen<true>>(g, p, W, f, s, row_lo, row_hi)
+                           : inv_gamma<false, Gen<false>>(g, p, W, f, s, row_lo, row_hi);
   }
-#undef SO3G_GAMMA_INV
-  SO3G_LAUNCHED();
-  SO3G_CUDA(cudaGetLastError());
-  return kOk;
+  return rc ? rc : launched();
 }
 
-int launch_fwd_gamma(const Geometry& g, const FftPlan& p, const void* f, double2* W, cudaStream_t s) {
-  const int ld = p.ld();
-  const Sizing z = size_for(p.big(), ld, 16);
-  const int T = z.T;
-  const size_t sm = z.smem;
-  dim3 grid((g.na + T - 1) / T, g.nb);
-#define SO3G_GAMMA_FWD(R, B)                                                  \
-  do {                                                                        \
-    if (int rc = set_smem(fwd_gamma_kernel<R, B>, sm)) return rc;             \
-    fwd_gamma_kernel<R, B><<<grid, kThreads, sm, s>>>(g, p, f, W, T, ld);     \
-  } while (0)
+int launch_fwd_gamma(const Geometry& g, const FftPlan& p, const void* f, double2* W, cudaStream_t s, int row_lo,
+                     int row_hi) {
+  if (row_hi < 0 || row_hi > g.nb) row_hi = g.nb;
+  if (row_lo >= row_hi) return kOk;
+  int rc;
+  const Eng e = pick(p);
   if (g.real) {
-    if (p.big()) SO3G_GAMMA_FWD(true, true); else SO3G_GAMMA_FWD(true, false);
+    rc = e == Eng::kGenBig ? fwd_gamma<true, Gen<true>>(g, p, f, W, s, row_lo, row_hi)
+                           : fwd_gamma<true, Gen<false>>(g, p, f, W, s, row_lo, row_hi);
+  } else if (e == Eng::k127) {
+    rc = fwd_gamma<false, E127>(g, p, f, W, s, row_lo, row_hi);
   } else {
-    if (p.big()) SO3G_GAMMA_FWD(false, true); else SO3G_GAMMA_FWD(false, false);
+    rc = e == Eng::kGenBig ? fwd_gamma<false, Gen<true>>(g, p, f, W, s, row_lo, row_hi)
+                           : fwd_gamma<false, Gen<false>>(g, p, f, W, s, row_lo, row_hi);
   }
-#undef SO3G_GAMMA_FWD
-  SO3G_LAUNCHED();
-  SO3G_CUDA(cudaGetLastError());
-  return kOk;
+  return rc ? rc : launched();
 }
 
 int launch_fwd_alpha(const Geometry& g, const FftPlan& p, double2* W, cudaStream_t s) {
-  const int ld = p.ld();
-  const Sizing z = size_for(p.big(), ld, 16);
-  const int T = z.T;
-  const size_t sm = z.smem;
-  const int nrows = g.nplanes * g.nb;
-  if (p.big()) {
-    if (int rc = set_smem(fwd_alpha_kernel<true>, sm)) return rc;
-    fwd_alpha_kernel<true><<<(nrows + T - 1) / T, kThreads, sm, s>>>(g, p, W, T, ld);
-  } else {
-    if (int rc = set_smem(fwd_alpha_kernel<false>, sm)) return rc;
-    fwd_alpha_kernel<false><<<(nrows + T - 1) / T, kThreads, sm, s>>>(g, p, W, T, ld);
+  int rc;
+  switch (pick(p)) {
+    case Eng::k1023: rc = fwd_alpha<E1023>(g, p, W, s); break;
+    case Eng::k127: rc = fwd_alpha<E127>(g, p, W, s); break;
+    case Eng::kGenBig: rc = fwd_alpha<Gen<true>>(g, p, W, s); break;
+    default: rc = fwd_alpha<Gen<false>>(g, p, W, s); break;
   }
-  SO3G_LAUNCHED();
-  SO3G_CUDA(cudaGetLastError());
-  return kOk;
+  return rc ? rc : launched();
 }
 
 int launch_fwd_beta_conv(const Geometry& g, const FftPlan& p, const FftPlan& pc, const double2* wr, double2* W,
                          cudaStream_t s) {
-  int ld = p.ld() > pc.ld() ? p.ld() : pc.ld();
-  const Sizing z = size_for(p.big() || pc.big(), ld, 8);
-  const int T = z.T;
-  const size_t sm = z.smem;
-  dim3 grid((2 * g.L - 1 + T - 1) / T, g.nplanes);
-  if (p.big() || pc.big()) {
-    if (int rc = set_smem(fwd_beta_conv_kernel<true>, sm)) return rc;
-    fwd_beta_conv_kernel<true><<<grid, kThreads, sm, s>>>(g, p, pc, wr, W, T, ld);
-  } else {
-    if (int rc = set_smem(fwd_beta_conv_kernel<false>, sm)) return rc;
-    fwd_beta_conv_kernel<false><<<grid, kThreads, sm, s>>>(g, p, pc, wr, W, T, ld);
-  }
-  SO3G_LAUNCHED();
-  SO3G_CUDA(cudaGetLastError());
-  return kOk;
+  int rc;
+  if (pick(p) == Eng::k1023 && !pc.blue && pc.n == 2048)
+    rc = fwd_beta_conv<EConv1023>(g, p, pc, wr, W, s);
+  else if (p.big() || pc.big())
+    rc = fwd_beta_conv<Gen<true>>(g, p, pc, wr, W, s);
+  else
+    rc = fwd_beta_conv<Gen<false>>(g, p, pc, wr, W, s);
+  return rc ? rc : launched();
 }
 
 }  // namespace so3g

@@ -62,6 +62,18 @@ def test_edge_sizes(O, L, N, L0, real, sampling):
     assert rel_err(fl_g, O.forward(f_ref, op)) < TOL
 
 
+@pytest.mark.parametrize("N", [1, 2])
+def test_metric_lengths_L512_against_oracle(O, N):
+    """L=512 runs the compile-time DFT plans (1023 = 31*11*3 over alpha and the
+    extended beta circle, 2048 for the weight convolution); compared with the
+    oracle on a few n-planes, inverse and forward (forward on the oracle's
+    samples)."""
+    p = params(512, N)
+    fl, op, f_gpu, f_ref = _both(O, p, seed=512 + N)
+    assert rel_err(f_gpu, f_ref) < TOL
+    assert rel_err(so3.forward(f_ref, p), O.forward(f_ref, op)) < TOL
+
+
 def test_config_complex_L64_N64_risbo(O):
     """Plain complex round trip, MW, L=64, N=64, padded, all n, Risbo, U(-1,1)."""
     p = params(64, 64)

@@ -64,6 +64,15 @@ int so3gpu_stage_times(so3gpu_context *ctx, double *total_ms, long long *counts,
  * (2 flops per FMA), from a register-resident FMA chain kernel. */
 double so3gpu_measure_fp64_peak(int device);
 
+/* Kernel variants of the DFT stages for the geometry of p (L, N, sampling,
+ * reality) on a device: 8 entries indexed like so3gpu_stage_times (only the
+ * FFT stages have more than one variant).  The autotuner fills them on the
+ * first transform of a geometry (or in so3gpu_prepare); setting them pins a
+ * choice and skips tuning.  get returns 1 if the geometry has been tuned or
+ * pinned, 0 if not (var untouched). */
+int so3gpu_get_stage_variants(int device, const so3_parameters_t *p, int *var);
+int so3gpu_set_stage_variants(int device, const so3_parameters_t *p, const int *var);
+
 /* Complex inverse transform (same result as so3gpu_inverse) that allocates
  * no device memory; no counterpart in the reference.  For callers that cannot
  * call cudaMalloc (code running under a foreign allocator or memory cap, or

@@ -411,11 +411,7 @@ int so3gpu_prepare(so3gpu_context* c, const so3_parameters_t* p) {
   if (!c || !p) return t_status = so3g::fail(so3g::kInvalidParameter, "null argument");
   DeviceScope ds(c->device);
   std::lock_guard<std::mutex> lk(c->mu);
-  int rc = so3g::prepare(so3g::device_state(c->device), *p, p->reality != 0, c->stream);
-  if (!rc) {
-    void* ws;
-    rc = so3g::ensure_ws(&c->wk, so3g::workspace_bytes(*p, p->reality != 0), &ws);
-  }
+  int rc = so3g::prepare(so3g::device_state(c->device), *p, p->reality != 0, c->stream, &c->wk);
   if (!rc && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = so3g::fail(so3g::kCudaError, "prepare sync");
   return t_status = rc;
 }
@@ -506,6 +502,17 @@ double so3gpu_measure_fp64_peak(int device) {
   }
   t_status = 0;
   return tf;
+}
+
+int so3gpu_get_stage_variants(int device, const so3_parameters_t* p, int* var) {
+  if (!p || !var) return t_status = so3g::fail(so3g::kInvalidParameter, "null argument"), 0;
+  t_status = 0;
+  return so3g::get_stage_variants(so3g::device_state(device), *p, p->reality != 0, var);
+}
+
+int so3gpu_set_stage_variants(int device, const so3_parameters_t* p, const int* var) {
+  if (!p || !var) return t_status = so3g::fail(so3g::kInvalidParameter, "null argument");
+  return t_status = so3g::set_stage_variants(so3g::device_state(device), *p, p->reality != 0, var);
 }
 
 int so3gpu_last_status(void) { return t_status; }

@@ -2,6 +2,7 @@
 // on device pointers.  Host code only; every kernel runs on stream s.
 #include <algorithm>
 #include <cstdlib>
+#include <string>
 #include <utility>
 #include <vector>
 
@@ -32,9 +33,71 @@ static int acquire(Device* D, const so3_parameters_t& p, int real, cudaStream_t 
   return kOk;
 }
 
-int prepare(Device* D, const so3_parameters_t& p, int real, cudaStream_t s) {
+static std::string tune_key(const so3_parameters_t& p, int real) {
+  return std::to_string(p.L) + "/" + std::to_string(p.N) + "/" + std::to_string((int)p.sampling_scheme) + "/" +
+         std::to_string(real);
+}
+
+// Stage variants for this geometry: cached per device, else measured on the
+// workspace (skipped while s is being captured, and when the environment sets
+// SO3GPU_AUTOTUNE=0; defaults are used then).
+static int ensure_tuned(Device* D, const so3_parameters_t& p, int real, Resources* r, double2* W, cudaStream_t s) {
+  const std::string key = tune_key(p, real);
+  {
+    std::lock_guard<std::mutex> lk(D->mu);
+    auto it = D->tuned.find(key);
+    if (it != D->tuned.end()) {
+      for (int i = 0; i < 8; i++) r->g.var[i] = it->second[i];
+      return kOk;
+    }
+  }
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  SO3G_CUDA(cudaStreamIsCapturing(s, &cs));
+  if (cs != cudaStreamCaptureStatusNone) return kOk;
+  const char* env = getenv("SO3GPU_AUTOTUNE");
+  Geometry g = r->g;
+  if (!(env && env[0] == '0')) {
+    FftPlan pc{};
+    const double2* wr = nullptr;
+    {
+      std::lock_guard<std::mutex> lk(D->mu);
+      if (int rc = ensure_fft(D, g.Pc, &pc)) return rc;
+      if (int rc = ensure_conv_kernel(D, g, &wr)) return rc;
+    }
+    if (int rc = autotune_stages(&g, r->pP, r->pg, pc, wr, W, s, 3)) return rc;
+  }
+  std::lock_guard<std::mutex> lk(D->mu);
+  D->tuned[key] = std::vector<signed char>(g.var, g.var + 8);
+  for (int i = 0; i < 8; i++) r->g.var[i] = g.var[i];
+  return kOk;
+}
+
+int get_stage_variants(Device* D, const so3_parameters_t& p, int real, int* var) {
+  std::lock_guard<std::mutex> lk(D->mu);
+  auto it = D->tuned.find(tune_key(p, real));
+  if (it == D->tuned.end()) return 0;
+  for (int i = 0; i < 8; i++) var[i] = it->second[i];
+  return 1;
+}
+
+int set_stage_variants(Device* D, const so3_parameters_t& p, int real, const int* var) {
+  std::vector<signed char> v(8);
+  for (int i = 0; i < 8; i++) {
+    if (var[i] < 0 || var[i] > 7) return fail(kInvalidParameter, "stage variant out of range");
+    v[i] = (signed char)var[i];
+  }
+  std::lock_guard<std::mutex> lk(D->mu);
+  D->tuned[tune_key(p, real)] = v;
+  return kOk;
+}
+
+int prepare(Device* D, const so3_parameters_t& p, int real, cudaStream_t s, Workspace* wk) {
   Resources r;
-  return acquire(D, p, real, s, &r, true);
+  if (int rc = acquire(D, p, real, s, &r, true)) return rc;
+  if (!wk) return kOk;
+  void* ws = nullptr;
+  if (int rc = ensure_ws(wk, workspace_bytes(p, real), &ws)) return rc;
+  return ensure_tuned(D, p, real, &r, static_cast<double2*>(ws), s);
 }
 
 int run_inverse(Device* D, Workspace* wk, const so3_parameters_t& p, const void* flmn_d, void* f_d, int real,
@@ -44,6 +107,7 @@ int run_inverse(Device* D, Workspace* wk, const so3_parameters_t& p, const void*
   void* ws = nullptr;
   if (int rc = ensure_ws(wk, workspace_bytes(p, real), &ws)) return rc;
   double2* W = static_cast<double2*>(ws);
+  if (int rc = ensure_tuned(D, p, real, &r, W, s)) return rc;
   const int sym_n0 = real && p.N == 1;
   StageTimer* T = &wk->timer;
   cudaEvent_t ev;
@@ -71,6 +135,7 @@ int run_forward(Device* D, Workspace* wk, const so3_parameters_t& p, const void*
   void* ws = nullptr;
   if (int rc = ensure_ws(wk, workspace_bytes(p, real), &ws)) return rc;
   double2* W = static_cast<double2*>(ws);
+  if (int rc = ensure_tuned(D, p, real, &r, W, s)) return rc;
   StageTimer* T = &wk->timer;
   cudaEvent_t ev;
   int rc;
@@ -171,6 +236,7 @@ int run_inverse_staged(Device* D, Workspace* wk, const so3_parameters_t& p, int 
   void* ws = nullptr;
   if (int rc = ensure_ws(wk, workspace_bytes(p, real), &ws)) return rc;
   double2* W = static_cast<double2*>(ws);
+  if (int rc = ensure_tuned(D, p, real, &r, W, s)) return rc;
   const Geometry& g = r.g;
   const int sym_n0 = real && p.N == 1;
   const int compact = p.storage == SO3_STORAGE_COMPACT;
@@ -223,6 +289,7 @@ int run_forward_staged(Device* D, Workspace* wk, const so3_parameters_t& p, int 
   void* ws = nullptr;
   if (int rc = ensure_ws(wk, workspace_bytes(p, real), &ws)) return rc;
   double2* W = static_cast<double2*>(ws);
+  if (int rc = ensure_tuned(D, p, real, &r, W, s)) return rc;
   const Geometry& g = r.g;
   const int compact = p.storage == SO3_STORAGE_COMPACT;
   const std::vector<long long> base = block_bases(p, real);

@@ -18,6 +18,15 @@
 namespace so3g {
 namespace fx {
 
+// Shared-memory position of element i of a sequence.  Plans with a first
+// radix-8 pass (SK = true) leave one pad slot after every 8 elements, so that
+// its stride-8 stores (and the T-interleaved staging loops) fall into
+// distinct banks; odd-radix plans store densely (SK = false).
+template <bool SK>
+__host__ __device__ constexpr int phys(int i) { return SK ? i + (i >> 3) : i; }
+template <bool SK>
+__host__ __device__ constexpr int extent(int n) { return phys<SK>(n - 1) + 1; }
+
 // Odd prime radix, whole butterfly in registers.
 template <int R>
 __device__ __forceinline__ void bfly_odd(double2* v) {
@@ -59,21 +68,21 @@ __device__ __forceinline__ void bfly_any(double2* v) {
 }
 
 // One output group of an odd-radix butterfly: pairs q = QA..QB (and q = 0
-// when ZERO), streaming over the inputs x_r = in[r * M] (times tw^r when
-// TW).  d receives output q at d[q * NS].
-template <int R, int QA, int QB, bool ZERO, int M, int NS, bool TW>
-__device__ __forceinline__ void odd_group(const double2* __restrict__ in, double2* __restrict__ d,
+// when ZERO), streaming over the inputs x_r = in[phys<SK>(j + r * M)] (times
+// tw^r when TW).  Output q goes to d[phys<SK>(o + q * NS)].
+template <int R, int QA, int QB, bool ZERO, int M, int NS, bool TW, bool SK>
+__device__ __forceinline__ void odd_group(const double2* __restrict__ in, int j, double2* __restrict__ d, int o,
                                           const double2* __restrict__ roots, int tw_step) {
   constexpr int H = (R - 1) / 2;
   constexpr int G = QB - QA + 1;
   double2 a[G], b[G];
 #pragma unroll
   for (int i = 0; i < G; i++) a[i] = b[i] = make_double2(0.0, 0.0);
-  const double2 v0 = in[0];
+  const double2 v0 = in[phys<SK>(j)];
   double2 tot = v0;
 #pragma unroll
   for (int r = 1; r <= H; r++) {
-    double2 xp = in[r * M], xn = in[(R - r) * M];
+    double2 xp = in[phys<SK>(j + r * M)], xn = in[phys<SK>(j + (R - r) * M)];
     if constexpr (TW) {
       xp = cmul(xp, __ldg(roots + r * tw_step));
       xn = cmul(xn, __ldg(roots + (R - r) * tw_step));
@@ -92,20 +101,20 @@ __device__ __forceinline__ void odd_group(const double2* __restrict__ in, double
       b[i].y = fma(sn, dd.y, b[i].y);
     }
   }
-  if constexpr (ZERO) d[0] = tot;
+  if constexpr (ZERO) d[phys<SK>(o)] = tot;
 #pragma unroll
   for (int i = 0; i < G; i++) {
     const int q = QA + i;
     const double ar = v0.x + a[i].x, ai = v0.y + a[i].y;
-    d[q * NS] = make_double2(ar + b[i].y, ai - b[i].x);
-    d[(R - q) * NS] = make_double2(ar - b[i].y, ai + b[i].x);
+    d[phys<SK>(o + q * NS)] = make_double2(ar + b[i].y, ai - b[i].x);
+    d[phys<SK>(o + (R - q) * NS)] = make_double2(ar - b[i].y, ai + b[i].x);
   }
 }
 
 // One Stockham pass of radix R at stride NS over T sequences of length N
 // (sequence t at src[t * LD]).  NG > 1 splits each butterfly into NG output
 // groups handled by different threads (odd R only).
-template <int N, int R, int NS, int T, int LD, int NT, int NG>
+template <int N, int R, int NS, int T, int LD, int NT, int NG, bool SK>
 __device__ __forceinline__ void pass(const double2* __restrict__ src, double2* __restrict__ dst,
                                      const double2* __restrict__ roots) {
   constexpr int M = N / R;
@@ -118,51 +127,54 @@ __device__ __forceinline__ void pass(const double2* __restrict__ src, double2* _
     const int g = NG == 1 ? 0 : rem / M;
     const int j = NG == 1 ? rem : rem - g * M;
     const int k = j % NS;
-    const double2* s = src + t * LD + j;
-    double2* d = dst + t * LD + (j / NS) * NS * R + k;
+    const double2* s = src + t * LD;
+    double2* d = dst + t * LD;
+    const int o = (j / NS) * NS * R + k;
     if constexpr (NG == 1) {
       double2 v[R];
-      v[0] = s[0];
+      v[0] = s[phys<SK>(j)];
 #pragma unroll
       for (int r = 1; r < R; r++) {
-        double2 x = s[r * M];
+        double2 x = s[phys<SK>(j + r * M)];
         if constexpr (TW) x = cmul(x, __ldg(roots + r * k * TSTEP));
         v[r] = x;
       }
       bfly_any<R>(v);
 #pragma unroll
-      for (int q = 0; q < R; q++) d[q * NS] = v[q];
+      for (int q = 0; q < R; q++) d[phys<SK>(o + q * NS)] = v[q];
     } else {
       static_assert(R % 2 == 1 && NG <= 3, "output groups need an odd radix");
       constexpr int H = (R - 1) / 2;
       constexpr int QS = (H + NG - 1) / NG;
       const int tws = k * TSTEP;
       if (g == 0) {
-        odd_group<R, 1, QS, true, M, NS, TW>(s, d, roots, tws);
+        odd_group<R, 1, QS, true, M, NS, TW, SK>(s, j, d, o, roots, tws);
       } else if (NG == 2 || g == 1) {
         constexpr int B = NG == 2 ? H : 2 * QS;
-        odd_group<R, QS + 1, B, false, M, NS, TW>(s, d, roots, tws);
+        odd_group<R, QS + 1, B, false, M, NS, TW, SK>(s, j, d, o, roots, tws);
       } else {
-        odd_group<R, 2 * QS + 1, H, false, M, NS, TW>(s, d, roots, tws);
+        odd_group<R, 2 * QS + 1, H, false, M, NS, TW, SK>(s, j, d, o, roots, tws);
       }
     }
   }
 }
 
 // ---------------------------------------------------------------- plans
-// Each plan: static constexpr n (length), ld (buffer extent per sequence),
-// and run(a, b, P) -> buffer holding the result (a and b: T * LD entries).
+// Each plan: static constexpr n (length), ld (buffer extent per sequence,
+// padded by phys), and run(a, b, P) -> buffer holding the result (a and b:
+// T * LD entries; element i of sequence t at t * LD + phys<sk>(i)).
 
 // 1023 = 31 * 11 * 3 (the MW alpha / extended-beta length at L = 512).
 template <int T, int LD, int NT>
 struct P1023 {
-  static constexpr int n = 1023, ld = 1023;
+  static constexpr bool sk = false;
+  static constexpr int n = 1023, ld = extent<sk>(1023);
   static __device__ __forceinline__ double2* run(double2* a, double2* b, const FftPlan& P) {
-    pass<1023, 31, 1, T, LD, NT, 3>(a, b, P.roots);
+    pass<1023, 31, 1, T, LD, NT, 3, sk>(a, b, P.roots);
     __syncthreads();
-    pass<1023, 11, 31, T, LD, NT, 1>(b, a, P.roots);
+    pass<1023, 11, 31, T, LD, NT, 1, sk>(b, a, P.roots);
     __syncthreads();
-    pass<1023, 3, 341, T, LD, NT, 1>(a, b, P.roots);
+    pass<1023, 3, 341, T, LD, NT, 1, sk>(a, b, P.roots);
     __syncthreads();
     return b;
   }
@@ -171,15 +183,16 @@ struct P1023 {
 // 2048 = 8 * 8 * 8 * 4 (the quadrature-weight convolution length at L = 512).
 template <int T, int LD, int NT>
 struct P2048 {
-  static constexpr int n = 2048, ld = 2048;
+  static constexpr bool sk = true;
+  static constexpr int n = 2048, ld = extent<sk>(2048);
   static __device__ __forceinline__ double2* run(double2* a, double2* b, const FftPlan& P) {
-    pass<2048, 8, 1, T, LD, NT, 1>(a, b, P.roots);
+    pass<2048, 8, 1, T, LD, NT, 1, sk>(a, b, P.roots);
     __syncthreads();
-    pass<2048, 8, 8, T, LD, NT, 1>(b, a, P.roots);
+    pass<2048, 8, 8, T, LD, NT, 1, sk>(b, a, P.roots);
     __syncthreads();
-    pass<2048, 8, 64, T, LD, NT, 1>(a, b, P.roots);
+    pass<2048, 8, 64, T, LD, NT, 1, sk>(a, b, P.roots);
     __syncthreads();
-    pass<2048, 4, 512, T, LD, NT, 1>(b, a, P.roots);
+    pass<2048, 4, 512, T, LD, NT, 1, sk>(b, a, P.roots);
     __syncthreads();
     return a;
   }
@@ -188,11 +201,11 @@ struct P2048 {
 // 256 = 8 * 8 * 4 with an explicit root table (Bluestein inner length).
 template <int T, int LD, int NT>
 __device__ __forceinline__ double2* fft256(double2* a, double2* b, const double2* roots) {
-  pass<256, 8, 1, T, LD, NT, 1>(a, b, roots);
+  pass<256, 8, 1, T, LD, NT, 1, true>(a, b, roots);
   __syncthreads();
-  pass<256, 8, 8, T, LD, NT, 1>(b, a, roots);
+  pass<256, 8, 8, T, LD, NT, 1, true>(b, a, roots);
   __syncthreads();
-  pass<256, 4, 64, T, LD, NT, 1>(a, b, roots);
+  pass<256, 4, 64, T, LD, NT, 1, true>(a, b, roots);
   __syncthreads();
   return b;
 }
@@ -200,19 +213,20 @@ __device__ __forceinline__ double2* fft256(double2* a, double2* b, const double2
 // 127 (prime; the gamma length at N = 64) by Bluestein's algorithm over 256.
 template <int T, int LD, int NT>
 struct P127 {
-  static constexpr int n = 127, ld = 256;
+  static constexpr bool sk = true;
+  static constexpr int n = 127, ld = extent<sk>(256);
   static __device__ __forceinline__ double2* run(double2* a, double2* b, const FftPlan& P) {
     for (int w = threadIdx.x; w < T * 256; w += NT) {
       const int t = w >> 8, k = w & 255;
       double2* s = a + t * LD;
-      s[k] = k < 127 ? cmul(s[k], __ldg(P.chirp + k)) : make_double2(0.0, 0.0);
+      s[phys<true>(k)] = k < 127 ? cmul(s[phys<true>(k)], __ldg(P.chirp + k)) : make_double2(0.0, 0.0);
     }
     __syncthreads();
     double2* r = fft256<T, LD, NT>(a, b, P.mroots);
     for (int w = threadIdx.x; w < T * 256; w += NT) {
       const int t = w >> 8, k = w & 255;
       double2* s = r + t * LD;
-      s[k] = cconj(cmul(s[k], __ldg(P.kern + k)));
+      s[phys<true>(k)] = cconj(cmul(s[phys<true>(k)], __ldg(P.kern + k)));
     }
     __syncthreads();
     double2* o = r == a ? b : a;
@@ -220,7 +234,7 @@ struct P127 {
     for (int w = threadIdx.x; w < T * 127; w += NT) {
       const int t = w / 127, k = w - t * 127;
       double2* s = r + t * LD;
-      s[k] = cmul(__ldg(P.chirp + k), cconj(s[k]));
+      s[phys<true>(k)] = cmul(__ldg(P.chirp + k), cconj(s[phys<true>(k)]));
     }
     __syncthreads();
     return r;

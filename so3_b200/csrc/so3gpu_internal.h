@@ -54,6 +54,9 @@ struct Geometry {
   int plane0;
   long RS, PS;
   int Pc;       // weight-convolution length (power of two >= 4L-3)
+  // Kernel variant of each DFT stage (index = Stage below; 0 = default),
+  // chosen by the autotuner for this geometry.
+  signed char var[8];
 };
 Geometry make_geometry(const so3_parameters_t& p, int real);
 
@@ -82,6 +85,7 @@ struct DevPlan {
 struct Device {
   int device = 0;
   std::mutex mu;
+  std::map<std::string, std::vector<signed char>> tuned;  // stage variants by geometry key
   DlTable dl[2];                                 // per dl_method
   std::map<int, std::unique_ptr<DevPlan>> ffts;  // by length
   std::map<int, double2*> conv_kernels;          // weight kernel by L (MW/MWSS identical)
@@ -171,12 +175,27 @@ int launch_harmonic_convolution(const so3_parameters_t& hp, const so3_parameters
                                 const long long* gb, const double2* flmn, const double2* glmn, double2* hlmn,
                                 cudaStream_t s);
 int launch_zero(void* p, size_t bytes, cudaStream_t s);
+
+// Autotuner of the DFT stages: times every kernel variant of each stage on
+// the workspace W (its contents are scratch; results are discarded) and
+// writes the fastest into g->var.  Synchronises stream s: never call it while
+// s is being captured.  reps timed launches per variant after one warm-up.
+int autotune_stages(Geometry* g, const FftPlan& pP, const FftPlan& pg, const FftPlan& pc, const double2* wr,
+                    double2* W, cudaStream_t s, int reps);
+// Number of kernel variants the tuner can choose from for a stage.
+int stage_variants(const Geometry& g, const FftPlan& pP, const FftPlan& pg, const FftPlan& pc, int stage);
 int measure_fp64_fma_rate(double* tflops);
 
 // ---------------------------------------------------------------- drivers
 // Lock-protected creation of the per-device read-only resources a transform
 // with parameters p needs; safe to call before stream capture.
-int prepare(Device* D, const so3_parameters_t& p, int real, cudaStream_t s);
+// Tuned / pinned stage variants of a geometry (get: 1 if known, else 0).
+// Variants beyond a stage's count fall back to its default kernel.
+int get_stage_variants(Device* D, const so3_parameters_t& p, int real, int* var);
+int set_stage_variants(Device* D, const so3_parameters_t& p, int real, const int* var);
+// With a workspace it also sizes the workspace and tunes the stage kernels
+// for this geometry (both synchronise s, so prepare before stream capture).
+int prepare(Device* D, const so3_parameters_t& p, int real, cudaStream_t s, Workspace* wk = nullptr);
 int run_inverse(Device* D, Workspace* wk, const so3_parameters_t& p, const void* flmn_d, void* f_d, int real,
                 cudaStream_t s);
 int run_forward(Device* D, Workspace* wk, const so3_parameters_t& p, const void* f_d, void* flmn_d, int real,

@@ -66,6 +66,8 @@ template <bool BIG>
 struct Gen {
   static constexpr bool fixed = false;
   static constexpr int NT = kThreads, MINB = BIG ? 1 : 2, T = 0, LD = 0;
+  static __device__ __forceinline__ int at(int k) { return k; }
+  static __device__ __forceinline__ int atC(int k) { return k; }
   static __device__ __forceinline__ double2* runP(double2* a, double2* b, int T_, int ld, const FftPlan& P) {
     return fft_fwd_smem<BIG>(a, b, T_, ld, P);
   }
@@ -80,7 +82,11 @@ struct Fix {
   static constexpr int NT = NT_, MINB = MINB_, T = T_;
   static constexpr int ldP = PP<1, 1, 1>::ld, ldC = PC<1, 1, 1>::ld;
   static constexpr int ldmax = ldP > ldC ? ldP : ldC;
-  static constexpr int LD = T_ > 1 ? ldmax + 1 : ldmax;  // odd pitch: no bank conflicts across sequences
+  // pitch = 2 (mod 8) slots: T-interleaved staging loops hit distinct banks
+  static constexpr int LD = T_ > 1 ? ldmax + ((10 - ldmax % 8) % 8) : ldmax;
+  // element k of a sequence in the buffers of the runP / runC lengths
+  static __device__ __forceinline__ int at(int k) { return fx::phys<PP<1, 1, 1>::sk>(k); }
+  static __device__ __forceinline__ int atC(int k) { return fx::phys<PC<1, 1, 1>::sk>(k); }
   static __device__ __forceinline__ double2* runP(double2* a, double2* b, int, int, const FftPlan& P) {
     return PP<T_, LD, NT_>::run(a, b, P);
   }
@@ -90,11 +96,17 @@ struct Fix {
   static constexpr size_t smem() { return 2 * (size_t)T_ * LD * sizeof(double2); }
 };
 
-// alpha / extended-beta length 1023 (L = 512), gamma length 127 (N = 64), and
-// the forward beta pair 1023 / 2048.
-using E1023 = Fix<fx::P1023, fx::P1023, 1, 128, 4>;
-using E127 = Fix<fx::P127, fx::P127, 4, 128, 4>;
-using EConv1023 = Fix<fx::P1023, fx::P2048, 1, 128, 3>;
+// Variants the autotuner chooses from (sequences per CTA, CTA size, minimum
+// CTAs per SM): alpha / extended-beta length 1023 (L = 512), gamma length 127
+// (N = 64), and the forward beta pair 1023 / 2048.  Variant 0 is the default.
+using E1023a = Fix<fx::P1023, fx::P1023, 1, 128, 4>;
+using E1023b = Fix<fx::P1023, fx::P1023, 1, 64, 8>;
+using E1023c = Fix<fx::P1023, fx::P1023, 2, 128, 3>;
+using E127a = Fix<fx::P127, fx::P127, 4, 128, 4>;
+using E127b = Fix<fx::P127, fx::P127, 8, 128, 3>;
+using E127c = Fix<fx::P127, fx::P127, 2, 64, 8>;
+using EConv1023a = Fix<fx::P1023, fx::P2048, 1, 128, 3>;
+using EConv1023b = Fix<fx::P1023, fx::P2048, 1, 256, 2>;
 
 __device__ __forceinline__ int wrapi(int k, int P) {
   k %= P;
@@ -119,7 +131,7 @@ __global__ void __launch_bounds__(E::NT, E::MINB) inv_beta_kernel(Geometry g, Ff
   const int c0 = blockIdx.x * T, ncols = 2 * g.L - 1, L = g.L, Pn = g.P;
   double2* base = W + (long long)plane * g.PS;
   if (!g.mw)
-    for (int t = threadIdx.x; t < T; t += E::NT) a[t * ld + L] = make_double2(0.0, 0.0);
+    for (int t = threadIdx.x; t < T; t += E::NT) a[t * ld + E::at(L)] = make_double2(0.0, 0.0);
   for (int idx = threadIdx.x; idx < L * T; idx += E::NT) {
     const int t = idx % T, mp = idx / T, c = c0 + t;
     double2 v = c < ncols ? base[(long long)mp * g.RS + c] : make_double2(0.0, 0.0);
@@ -131,14 +143,14 @@ __global__ void __launch_bounds__(E::NT, E::MINB) inv_beta_kernel(Geometry g, Ff
       xp = cmul(xp, e);
       xn = cmul(xn, cconj(e));
     }
-    a[t * ld + mp] = cconj(xp);
-    if (mp > 0) a[t * ld + Pn - mp] = cconj(xn);
+    a[t * ld + E::at(mp)] = cconj(xp);
+    if (mp > 0) a[t * ld + E::at(Pn - mp)] = cconj(xn);
   }
   __syncthreads();
   double2* r = E::runP(a, b, T, ld, P);
   for (int idx = threadIdx.x; idx < g.nb * T; idx += E::NT) {
     const int t = idx % T, row = idx / T, c = c0 + t;
-    if (c < ncols) base[(long long)row * g.RS + c] = cconj(r[t * ld + row]);
+    if (c < ncols) base[(long long)row * g.RS + c] = cconj(r[t * ld + E::at(row)]);
   }
 }
 
@@ -161,7 +173,7 @@ __global__ void __launch_bounds__(E::NT, E::MINB) inv_alpha_kernel(Geometry g, F
         v = W[off + m + L - 1];
       }
     }
-    a[j * ld + k] = cconj(v);
+    a[j * ld + E::at(k)] = cconj(v);
   }
   __syncthreads();
   double2* r = E::runP(a, b, T, ld, P);
@@ -169,7 +181,7 @@ __global__ void __launch_bounds__(E::NT, E::MINB) inv_alpha_kernel(Geometry g, F
     const int j = idx / g.na, k = idx - j * g.na, row = r0 + j;
     if (row < nrows) {
       const long long off = (long long)(row / g.nb) * g.PS + (long long)(row % g.nb) * g.RS;
-      W[off + k] = cconj(r[j * ld + k]);
+      W[off + k] = cconj(r[j * ld + E::at(k)]);
     }
   }
 }
@@ -187,14 +199,14 @@ __global__ void __launch_bounds__(E::NT, E::MINB) inv_gamma_kernel(Geometry g, F
     double2 v = al < g.na ? W[(long long)p * g.PS + (long long)row * g.RS + al] : make_double2(0.0, 0.0);
     if (!REAL) {
       const int k = wrapi(p - g.plane0, ng);
-      a[t * ld + k] = cconj(v);
+      a[t * ld + E::at(k)] = cconj(v);
     } else {
       // Hermitian completion of planes n = 0..N-1, Im of n = 0 ignored
       if (p == 0) {
         a[t * ld] = make_double2(v.x, 0.0);
       } else {
-        a[t * ld + p] = cconj(v);
-        a[t * ld + ng - p] = v;
+        a[t * ld + E::at(p)] = cconj(v);
+        a[t * ld + E::at(ng - p)] = v;
       }
     }
   }
@@ -205,7 +217,7 @@ __global__ void __launch_bounds__(E::NT, E::MINB) inv_gamma_kernel(Geometry g, F
     const int t = idx % T, gi = idx / T, al = a0 + t;
     if (al >= g.na) continue;
     const long long o = (long long)gi * plane_sz + (long long)row * g.na + al;
-    const double2 y = r[t * ld + gi];
+    const double2 y = r[t * ld + E::at(gi)];
     if (REAL)
       static_cast<double*>(fout)[o] = y.x;
     else
@@ -233,7 +245,7 @@ __global__ void __launch_bounds__(E::NT, E::MINB) fwd_gamma_kernel(Geometry g, F
       else
         v = static_cast<const double2*>(fin)[o];
     }
-    a[t * ld + gi] = v;
+    a[t * ld + E::at(gi)] = v;
   }
   __syncthreads();
   double2* r = E::runP(a, b, T, ld, P);
@@ -242,7 +254,7 @@ __global__ void __launch_bounds__(E::NT, E::MINB) fwd_gamma_kernel(Geometry g, F
     const int t = idx % T, p = idx / T, al = a0 + t;
     if (al >= g.na) continue;
     const int k = REAL ? p : wrapi(p - g.plane0, ng);
-    W[(long long)p * g.PS + (long long)row * g.RS + al] = cscale(r[t * ld + k], scale);
+    W[(long long)p * g.PS + (long long)row * g.RS + al] = cscale(r[t * ld + E::at(k)], scale);
   }
 }
 
@@ -259,7 +271,7 @@ __global__ void __launch_bounds__(E::NT, E::MINB) fwd_alpha_kernel(Geometry g, F
     const int j = idx / Pn, k = idx - j * Pn, row = r0 + j;
     double2 v = make_double2(0.0, 0.0);
     if (row < nrows) v = W[(long long)(row / g.nb) * g.PS + (long long)(row % g.nb) * g.RS + k];
-    a[j * ld + k] = v;
+    a[j * ld + E::at(k)] = v;
   }
   __syncthreads();
   double2* r = E::runP(a, b, T, ld, P);
@@ -268,7 +280,7 @@ __global__ void __launch_bounds__(E::NT, E::MINB) fwd_alpha_kernel(Geometry g, F
     const int j = idx / ncols, c = idx - j * ncols, row = r0 + j;
     if (row < nrows) {
       const int k = wrapi(c - (L - 1), Pn);
-      W[(long long)(row / g.nb) * g.PS + (long long)(row % g.nb) * g.RS + c] = cscale(r[j * ld + k], inv);
+      W[(long long)(row / g.nb) * g.PS + (long long)(row % g.nb) * g.RS + c] = cscale(r[j * ld + E::at(k)], inv);
     }
   }
 }
@@ -286,7 +298,7 @@ __global__ void __launch_bounds__(E::NT, E::MINB) fwd_beta_conv_kernel(Geometry 
   double2* base = W + (long long)plane * g.PS;
   for (int idx = threadIdx.x; idx < g.nb * T; idx += E::NT) {
     const int t = idx % T, row = idx / T, c = c0 + t;
-    a[t * ld + row] = c < ncols ? base[(long long)row * g.RS + c] : make_double2(0.0, 0.0);
+    a[t * ld + E::at(row)] = c < ncols ? base[(long long)row * g.RS + c] : make_double2(0.0, 0.0);
   }
   __syncthreads();
   for (int idx = threadIdx.x; idx < (Pn - g.nb) * T; idx += E::NT) {
@@ -294,7 +306,7 @@ __global__ void __launch_bounds__(E::NT, E::MINB) fwd_beta_conv_kernel(Geometry 
     const int m = c - (L - 1);
     const double sg = ((m + n) & 1) ? -1.0 : 1.0;
     const int src = g.mw ? 2 * L - 2 - row : 2 * L - row;
-    a[t * ld + row] = cscale(a[t * ld + src], sg);
+    a[t * ld + E::at(row)] = cscale(a[t * ld + E::at(src)], sg);
   }
   __syncthreads();
   double2* r = E::runP(a, b, T, ld, P);
@@ -303,21 +315,21 @@ __global__ void __launch_bounds__(E::NT, E::MINB) fwd_beta_conv_kernel(Geometry 
   double2* o = (r == a) ? b : a;
   for (int idx = threadIdx.x; idx < T * pc; idx += E::NT) {
     const int t = idx / pc, k = idx - t * pc;
-    o[t * ld + k] = make_double2(0.0, 0.0);
+    o[t * ld + E::atC(k)] = make_double2(0.0, 0.0);
   }
   __syncthreads();
   for (int idx = threadIdx.x; idx < T * (2 * L - 1); idx += E::NT) {
     const int t = idx / (2 * L - 1), mpp = idx - t * (2 * L - 1) - (L - 1);
-    double2 v = cscale(r[t * ld + wrapi(mpp, Pn)], invP);
+    double2 v = cscale(r[t * ld + E::at(wrapi(mpp, Pn))], invP);
     if (g.mw) v = cmul(v, phase(mpp, 2 * L - 1, -1.0));
-    o[t * ld + wrapi(mpp, pc)] = cconj(v);
+    o[t * ld + E::atC(wrapi(mpp, pc))] = cconj(v);
   }
   __syncthreads();
   double2* o2 = (o == a) ? b : a;
   double2* q = E::runC(o, o2, T, ld, Pc);  // conj of the inverse DFT
   for (int idx = threadIdx.x; idx < T * pc; idx += E::NT) {
     const int t = idx / pc, k = idx - t * pc;
-    q[t * ld + k] = cmul(cconj(q[t * ld + k]), __ldg(wr + k));
+    q[t * ld + E::atC(k)] = cmul(cconj(q[t * ld + E::atC(k)]), __ldg(wr + k));
   }
   __syncthreads();
   double2* q2 = (q == a) ? b : a;
@@ -327,9 +339,9 @@ __global__ void __launch_bounds__(E::NT, E::MINB) fwd_beta_conv_kernel(Geometry 
     if (c >= ncols) continue;
     const int m = c - (L - 1);
     const double sg = ((m + n) & 1) ? -1.0 : 1.0;
-    double2 v = G[t * ld + mp];
+    double2 v = G[t * ld + E::atC(mp)];
     if (mp > 0) {
-      const double2 u = G[t * ld + pc - mp];
+      const double2 u = G[t * ld + E::atC(pc - mp)];
       v = make_double2(v.x + sg * u.x, v.y + sg * u.y);
     }
     base[(long long)mp * g.RS + c] = v;
@@ -417,9 +429,14 @@ int launched() {
 
 int launch_inv_beta(const Geometry& g, const FftPlan& p, double2* W, cudaStream_t s) {
   int rc;
+  const int v = g.var[kStInvBeta];
   switch (pick(p)) {
-    case Eng::k1023: rc = inv_beta<E1023>(g, p, W, s); break;
-    case Eng::k127: rc = inv_beta<E127>(g, p, W, s); break;
+    case Eng::k1023:
+      rc = v == 1 ? inv_beta<E1023b>(g, p, W, s) : v == 2 ? inv_beta<E1023c>(g, p, W, s) : inv_beta<E1023a>(g, p, W, s);
+      break;
+    case Eng::k127:
+      rc = v == 1 ? inv_beta<E127b>(g, p, W, s) : v == 2 ? inv_beta<E127c>(g, p, W, s) : inv_beta<E127a>(g, p, W, s);
+      break;
     case Eng::kGenBig: rc = inv_beta<Gen<true>>(g, p, W, s); break;
     default: rc = inv_beta<Gen<false>>(g, p, W, s); break;
   }
@@ -428,9 +445,15 @@ int launch_inv_beta(const Geometry& g, const FftPlan& p, double2* W, cudaStream_
 
 int launch_inv_alpha(const Geometry& g, const FftPlan& p, double2* W, cudaStream_t s) {
   int rc;
+  const int v = g.var[kStInvAlpha];
   switch (pick(p)) {
-    case Eng::k1023: rc = inv_alpha<E1023>(g, p, W, s); break;
-    case Eng::k127: rc = inv_alpha<E127>(g, p, W, s); break;
+    case Eng::k1023:
+      rc = v == 1 ? inv_alpha<E1023b>(g, p, W, s) : v == 2 ? inv_alpha<E1023c>(g, p, W, s)
+                                                           : inv_alpha<E1023a>(g, p, W, s);
+      break;
+    case Eng::k127:
+      rc = v == 1 ? inv_alpha<E127b>(g, p, W, s) : v == 2 ? inv_alpha<E127c>(g, p, W, s) : inv_alpha<E127a>(g, p, W, s);
+      break;
     case Eng::kGenBig: rc = inv_alpha<Gen<true>>(g, p, W, s); break;
     default: rc = inv_alpha<Gen<false>>(g, p, W, s); break;
   }
@@ -443,11 +466,14 @@ int launch_inv_gamma(const Geometry& g, const FftPlan& p, const double2* W, void
   if (row_lo >= row_hi) return kOk;
   int rc;
   const Eng e = pick(p);
+  const int v = g.var[kStInvGamma];
   if (g.real) {
     rc = e == Eng::kGenBig ? inv_gamma<true, Gen<true>>(g, p, W, f, s, row_lo, row_hi)
                            : inv_gamma<true, Gen<false>>(g, p, W, f, s, row_lo, row_hi);
   } else if (e == Eng::k127) {
-    rc = inv_gamma<false, E127>(g, p, W, f, s, row_lo, row_hi);
+    rc = v == 1   ? inv_gamma<false, E127b>(g, p, W, f, s, row_lo, row_hi)
+         : v == 2 ? inv_gamma<false, E127c>(g, p, W, f, s, row_lo, row_hi)
+                  : inv_gamma<false, E127a>(g, p, W, f, s, row_lo, row_hi);
   } else {
     rc = e == Eng::kGenBig ? inv_gamma<false, Gen<true>>(g, p, W, f, s, row_lo, row_hi)
                            : inv_gamma<false, Gen<false>>(g, p, W, f, s, row_lo, row_hi);
@@ -461,11 +487,14 @@ int launch_fwd_gamma(const Geometry& g, const FftPlan& p, const void* f, double2
   if (row_lo >= row_hi) return kOk;
   int rc;
   const Eng e = pick(p);
+  const int v = g.var[kStFwdGamma];
   if (g.real) {
     rc = e == Eng::kGenBig ? fwd_gamma<true, Gen<true>>(g, p, f, W, s, row_lo, row_hi)
                            : fwd_gamma<true, Gen<false>>(g, p, f, W, s, row_lo, row_hi);
   } else if (e == Eng::k127) {
-    rc = fwd_gamma<false, E127>(g, p, f, W, s, row_lo, row_hi);
+    rc = v == 1   ? fwd_gamma<false, E127b>(g, p, f, W, s, row_lo, row_hi)
+         : v == 2 ? fwd_gamma<false, E127c>(g, p, f, W, s, row_lo, row_hi)
+                  : fwd_gamma<false, E127a>(g, p, f, W, s, row_lo, row_hi);
   } else {
     rc = e == Eng::kGenBig ? fwd_gamma<false, Gen<true>>(g, p, f, W, s, row_lo, row_hi)
                            : fwd_gamma<false, Gen<false>>(g, p, f, W, s, row_lo, row_hi);
@@ -475,25 +504,96 @@ int launch_fwd_gamma(const Geometry& g, const FftPlan& p, const void* f, double2
 
 int launch_fwd_alpha(const Geometry& g, const FftPlan& p, double2* W, cudaStream_t s) {
   int rc;
+  const int v = g.var[kStFwdAlpha];
   switch (pick(p)) {
-    case Eng::k1023: rc = fwd_alpha<E1023>(g, p, W, s); break;
-    case Eng::k127: rc = fwd_alpha<E127>(g, p, W, s); break;
+    case Eng::k1023:
+      rc = v == 1 ? fwd_alpha<E1023b>(g, p, W, s) : v == 2 ? fwd_alpha<E1023c>(g, p, W, s)
+                                                           : fwd_alpha<E1023a>(g, p, W, s);
+      break;
+    case Eng::k127:
+      rc = v == 1 ? fwd_alpha<E127b>(g, p, W, s) : v == 2 ? fwd_alpha<E127c>(g, p, W, s) : fwd_alpha<E127a>(g, p, W, s);
+      break;
     case Eng::kGenBig: rc = fwd_alpha<Gen<true>>(g, p, W, s); break;
     default: rc = fwd_alpha<Gen<false>>(g, p, W, s); break;
   }
   return rc ? rc : launched();
 }
 
+namespace {
+bool conv_fixed(const FftPlan& p, const FftPlan& pc) { return pick(p) == Eng::k1023 && !pc.blue && pc.n == 2048; }
+}  // namespace
+
 int launch_fwd_beta_conv(const Geometry& g, const FftPlan& p, const FftPlan& pc, const double2* wr, double2* W,
                          cudaStream_t s) {
   int rc;
-  if (pick(p) == Eng::k1023 && !pc.blue && pc.n == 2048)
-    rc = fwd_beta_conv<EConv1023>(g, p, pc, wr, W, s);
+  if (conv_fixed(p, pc))
+    rc = g.var[kStFwdBetaConv] == 1 ? fwd_beta_conv<EConv1023b>(g, p, pc, wr, W, s)
+                                    : fwd_beta_conv<EConv1023a>(g, p, pc, wr, W, s);
   else if (p.big() || pc.big())
     rc = fwd_beta_conv<Gen<true>>(g, p, pc, wr, W, s);
   else
     rc = fwd_beta_conv<Gen<false>>(g, p, pc, wr, W, s);
   return rc ? rc : launched();
+}
+
+// ------------------------------------------------------------------ autotuner
+int stage_variants(const Geometry& g, const FftPlan& pP, const FftPlan& pg, const FftPlan& pc, int stage) {
+  switch (stage) {
+    case kStInvBeta:
+    case kStInvAlpha:
+    case kStFwdAlpha: return (pick(pP) == Eng::k1023 || pick(pP) == Eng::k127) ? 3 : 1;
+    case kStInvGamma:
+    case kStFwdGamma: return (!g.real && pick(pg) == Eng::k127) ? 3 : 1;
+    case kStFwdBetaConv: return conv_fixed(pP, pc) ? 2 : 1;
+    default: return 1;
+  }
+}
+
+int autotune_stages(Geometry* g, const FftPlan& pP, const FftPlan& pg, const FftPlan& pc, const double2* wr,
+                    double2* W, cudaStream_t s, int reps) {
+  const int stages[] = {kStInvBeta, kStInvAlpha, kStInvGamma, kStFwdGamma, kStFwdAlpha, kStFwdBetaConv};
+  cudaEvent_t e0, e1;
+  SO3G_CUDA(cudaEventCreate(&e0));
+  SO3G_CUDA(cudaEventCreate(&e1));
+  int rc = kOk;
+  for (int st : stages) {
+    const int nv = stage_variants(*g, pP, pg, pc, st);
+    if (nv <= 1) {
+      g->var[st] = 0;
+      continue;
+    }
+    float best = 1e30f;
+    int best_v = 0;
+    for (int v = 0; v < nv && rc == kOk; v++) {
+      g->var[st] = (signed char)v;
+      auto run = [&]() -> int {
+        switch (st) {
+          case kStInvBeta: return launch_inv_beta(*g, pP, W, s);
+          case kStInvAlpha: return launch_inv_alpha(*g, pP, W, s);
+          case kStInvGamma: return launch_inv_gamma(*g, pg, W, W, s);  // samples written over the scratch
+          case kStFwdGamma: return launch_fwd_gamma(*g, pg, W, W, s);
+          case kStFwdAlpha: return launch_fwd_alpha(*g, pP, W, s);
+          default: return launch_fwd_beta_conv(*g, pP, pc, wr, W, s);
+        }
+      };
+      if ((rc = run())) break;
+      if (cudaEventRecord(e0, s) != cudaSuccess) rc = fail(kCudaError, "autotune event");
+      for (int i = 0; i < reps && rc == kOk; i++) rc = run();
+      if (rc == kOk && cudaEventRecord(e1, s) != cudaSuccess) rc = fail(kCudaError, "autotune event");
+      if (rc == kOk && cudaEventSynchronize(e1) != cudaSuccess) rc = fail(kCudaError, "autotune sync");
+      float ms = 0.f;
+      if (rc == kOk) cudaEventElapsedTime(&ms, e0, e1);
+      if (rc == kOk && ms < best) {
+        best = ms;
+        best_v = v;
+      }
+    }
+    g->var[st] = (signed char)best_v;
+    if (rc) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
 }
 
 }  // namespace so3g

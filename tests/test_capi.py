@@ -83,3 +83,19 @@ def test_reference_exit_semantics_in_default_mode(tmp_path):
     r = subprocess.run(["python", "-c", code], cwd=ROOT, capture_output=True, text=True)
     assert r.returncode == 1
     assert "ERROR: Invalid sampling scheme." in r.stdout
+
+
+def test_stage_variant_pinning_round_trip(lib):
+    """Pinned DFT-stage variants are stored per device and geometry (host
+    state only; no GPU needed)."""
+    import ctypes
+    from tests.helpers import params
+    p = params(40, 3, sampling=1).to_struct()
+    got = (ctypes.c_int * 8)()
+    assert lib.so3gpu_get_stage_variants(5, ctypes.byref(p), got) == 0
+    want = (ctypes.c_int * 8)(0, 1, 2, 0, 0, 1, 1, 0)
+    assert lib.so3gpu_set_stage_variants(5, ctypes.byref(p), want) == 0
+    assert lib.so3gpu_get_stage_variants(5, ctypes.byref(p), got) == 1
+    assert list(got) == list(want)
+    bad = (ctypes.c_int * 8)(0, 9, 0, 0, 0, 0, 0, 0)
+    assert lib.so3gpu_set_stage_variants(5, ctypes.byref(p), bad) == 1

@@ -1,15 +1,21 @@
 #!/usr/bin/env python
 """Benchmark of the SO(3) Wigner transform path on B200.
 
-One step = one complex inverse transform plus one forward transform
-(so3_core_inverse_via_ssht then so3_core_forward_via_ssht semantics) of one
-signal at L=512, N=64, MW sampling, L0=0, padded storage, negative-first
-n-order, all n, Risbo recursion, with flmn real and imaginary parts iid
-U(-1, 1) (seeded, per rank).  The metric is transforms per second (one
-inverse + one forward = one transform unit); ranks run independent signals
-(weak scaling, no collective on the data path).
+Workload: complex signals at L=512, N=64, MW sampling, L0=0, padded storage,
+negative-first n-order, all n, Risbo recursion, flmn real and imaginary
+parts iid U(-1, 1) (seeded, per rank).  One transform unit = one inverse plus
+one forward transform; the metric is units per second, split precision
+against FP64.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  * headline step: inverse_batch + forward_batch of --batch signals (default
+    8) with the int8 tensor-core (Ozaki split) contractions, FP64 everywhere
+    else; its error against the FP64 path is measured on the same inputs;
+  * "fp64": one FP64 inverse + forward per step (reference-exact path);
+  * "e2e": the FP64 drop-in so3_core_{inverse,forward}_via_ssht on pinned host
+    buffers, copies included.
+Ranks run independent signals (weak scaling, no collective on the data path).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl ours|reference]
 
 Prints one JSON line on rank 0.
 """
@@ -41,6 +47,8 @@ def args_():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--L", type=int, default=512)
     ap.add_argument("--N", type=int, default=64)
+    ap.add_argument("--batch", type=int, default=8,
+                    help="signals per split-precision step (0: time the FP64 path only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
@@ -210,9 +218,80 @@ def run_reference(a):
 
 
 # --------------------------------------------------------------------- our arm
+def fft_flops(n):
+    """Nominal FFT flop count 5 n log2 n (the usual convention)."""
+    return 5.0 * n * math.log2(n) if n > 1 else 0.0
+
+
+def stage_work(L, N):
+    """Algorithmic work per launch of every stage at (L, N), complex MW:
+    (kind, amount, unit description)."""
+    P, nb, ng, Pc = 2 * L - 1, L, 2 * N - 1, 1 << math.ceil(math.log2(4 * L - 3))
+    planes = 2 * N - 1
+    macs = contraction_macs(L, N)
+    return {
+        "inv_contract": ("fp64", 4.0 * macs, f"4 flops x {macs:.4g} complex-by-real MACs"),
+        "fwd_contract": ("fp64", 4.0 * macs, f"4 flops x {macs:.4g} complex-by-real MACs"),
+        "inv_beta": ("fp64", planes * P * fft_flops(P), f"{planes * P} DFTs of {P} at 5 n log2 n"),
+        "inv_alpha": ("fp64", planes * nb * fft_flops(P), f"{planes * nb} DFTs of {P} at 5 n log2 n"),
+        "fwd_alpha": ("fp64", planes * nb * fft_flops(P), f"{planes * nb} DFTs of {P} at 5 n log2 n"),
+        "inv_gamma": ("fp64", nb * P * fft_flops(ng), f"{nb * P} DFTs of {ng} at 5 n log2 n"),
+        "fwd_gamma": ("fp64", nb * P * fft_flops(ng), f"{nb * P} DFTs of {ng} at 5 n log2 n"),
+        "fwd_beta_conv": ("fp64", planes * P * (fft_flops(P) + 2 * fft_flops(Pc)),
+                          f"{planes * P} x (DFT {P} + 2 DFTs {Pc}) at 5 n log2 n"),
+    }
+
+
+def mixed_mma_count(L, N):
+    """mma.sync m16n8k32 instructions one split-precision contraction issues
+    per group of 8 signals (both directions issue the same number): 56 per warp
+    and 32-step of the reduction, 8 warps per CTA."""
+    import numpy as np
+    T = 32
+    MT = (L + T - 1) // T
+    mu = np.arange(L)[:, None, None]
+    nu = np.arange(N)[None, :, None]
+    t = np.arange(MT)[None, None, :]
+    lmin = np.maximum(mu, nu)
+    kfirst = (np.maximum(lmin, t * T) // T) * T
+    nk_inv = np.where(kfirst < L, (L - kfirst + T - 1) // T, 0)
+    return int(nk_inv.sum()) * 8 * 56
+
+
+def timed_steps(step, steps, warmup, stream, ctx, so3, sdist, local, world):
+    import torch
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        sdist.barrier()
+    ctx.stage_timing(True)
+    ctx.stage_times()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    launches0 = so3.launch_count()
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        evs[0].record(stream)
+        for i in range(steps):
+            step()
+            evs[i + 1].record(stream)
+        torch.cuda.synchronize()
+    launches = so3.launch_count() - launches0
+    stages = ctx.stage_times()
+    ctx.stage_timing(False)
+    total_ms = evs[0].elapsed_time(evs[-1])
+    lat = [evs[i].elapsed_time(evs[i + 1]) for i in range(steps)]
+    total_ms = sdist.max_over_ranks(total_ms, device=f"cuda:{local}")
+    return {"total_ms": total_ms, "lat": lat, "launches": launches, "stages": stages, "clocks": clk.summary()}
+
+
+def pct(lat, q):
+    s = sorted(lat)
+    return s[min(len(s) - 1, max(0, math.ceil(q * len(s)) - 1))]
+
+
 def run_ours(a):
     import torch
-    import torch.distributed as dist
 
     import so3_b200 as so3
     from so3_b200 import dist as sdist
@@ -222,72 +301,98 @@ def run_ours(a):
     world, rank, local = info.world, info.rank, info.local
     torch.cuda.set_device(local)
     sdist.init("nccl" if world > 1 else None, timeout_s=120)
+    dev = f"cuda:{local}"
 
-    L, N = a.L, a.N
+    L, N, B = a.L, a.N, a.batch
     p = so3.SO3Parameters(L=L, N=N, L0=0, sampling_scheme=0, n_order=1, storage=0, n_mode=0, dl_method=0)
-    fl_host = synth.gen_flmn(p, sdist.signal_seed(1000, rank, 0), "uniform")
     stream = torch.cuda.current_stream()
-    d_flmn = torch.from_numpy(fl_host).to(f"cuda:{local}")
-    d_f = torch.empty(so3.f_size(p), dtype=torch.complex128, device=f"cuda:{local}")
-    d_back = torch.empty(so3.flmn_size(p), dtype=torch.complex128, device=f"cuda:{local}")
     ctx = so3.Context(local, stream=stream)
     ctx.prepare(p)
     fp64_peak = so3.measure_fp64_peak(local)
+    int8_peak = so3.measure_int8_mma_peak(local)
 
-    def step():
+    # ---- plain FP64 path, one signal per step
+    fl_host = synth.gen_flmn(p, sdist.signal_seed(1000, rank, 0), "uniform")
+    d_flmn = torch.from_numpy(fl_host).to(dev)
+    d_f = torch.empty(so3.f_size(p), dtype=torch.complex128, device=dev)
+    d_back = torch.empty(so3.flmn_size(p), dtype=torch.complex128, device=dev)
+
+    def step64():
         ctx.inverse(d_flmn, p, out=d_f)
         ctx.forward(d_f, p, out=d_back)
 
-    for _ in range(a.warmup):
-        step()
-    torch.cuda.synchronize()
-    if world > 1:
-        sdist.barrier()
-    ctx.stage_timing(True)
-    ctx.stage_times()
-    evs = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps + 1)]
-    launches0 = so3.launch_count()
-    with ClockSampler(local) as clk:
-        torch.cuda.synchronize()
-        evs[0].record(stream)
-        for i in range(a.steps):
-            step()
-            evs[i + 1].record(stream)
-        torch.cuda.synchronize()
-    launches = so3.launch_count() - launches0
-    stages = ctx.stage_times()
-    ctx.stage_timing(False)
-    total_ms = evs[0].elapsed_time(evs[-1])
-    lat = [evs[i].elapsed_time(evs[i + 1]) for i in range(a.steps)]
-    total_ms = sdist.max_over_ranks(total_ms, device=f"cuda:{local}")
-    value = sdist.job_throughput(world * a.steps, total_ms / 1e3)
+    r64 = timed_steps(step64, a.steps, a.warmup, stream, ctx, so3, sdist, local, world)
+    fp64_value = sdist.job_throughput(world * a.steps, r64["total_ms"] / 1e3)
     rt_err = float(((d_back - d_flmn).abs().max() / d_flmn.abs().max()).item())
+    del d_back
 
-    # ---- roofline of the dominant kernel
-    per = {k: v[0] / v[1] for k, v in stages.items()}
-    dom = max(per, key=per.get)
-    macs = contraction_macs(L, N)
-    f_bytes = (2 * N - 1) * L * (2 * L - 1) * 16
-    if "contract" in dom:
-        achieved = 4.0 * macs / (per[dom] / 1e3) / 1e12
+    # ---- split-precision batch path: B signals per step
+    mixed = None
+    headline = {"value": fp64_value, "run": r64, "units_per_step": 1, "precision": "fp64"}
+    if B > 0:
+        fls = [d_flmn] + [torch.from_numpy(synth.gen_flmn(p, sdist.signal_seed(1000, rank, i), "uniform")).to(dev)
+                          for i in range(1, B)]
+        fs = [torch.empty(so3.f_size(p), dtype=torch.complex128, device=dev) for _ in range(B)]
+        backs = [torch.zeros(so3.flmn_size(p), dtype=torch.complex128, device=dev) for _ in range(B)]
+
+        def stepmx():
+            ctx.inverse_batch(fls, p, "mixed", outs=fs)
+            ctx.forward_batch(fs, p, "mixed", outs=backs)
+
+        rmx = timed_steps(stepmx, a.steps, a.warmup, stream, ctx, so3, sdist, local, world)
+        mixed_value = sdist.job_throughput(world * a.steps * B, rmx["total_ms"] / 1e3)
+        # error of the split path against the FP64 path on the same inputs
+        err_f = err_fl = err_rt = 0.0
+        for i in range(B):
+            ctx.inverse(fls[i], p, out=d_f)
+            torch.cuda.synchronize()
+            err_f = max(err_f, float(((fs[i] - d_f).abs().max() / d_f.abs().max()).item()))
+            ref = ctx.forward(fs[i], p)
+            torch.cuda.synchronize()
+            err_fl = max(err_fl, float(((backs[i] - ref).abs().max() / ref.abs().max()).item()))
+            err_rt = max(err_rt, float(((backs[i] - fls[i]).abs().max() / fls[i].abs().max()).item()))
+            del ref
+        mixed = {"value": mixed_value, "unit": UNIT, "batch": B, "ms_per_step": rmx["total_ms"] / a.steps,
+                 "over_fp64": mixed_value / fp64_value,
+                 "rel_err_vs_fp64": {"samples": err_f, "coefficients": err_fl, "max": max(err_f, err_fl)},
+                 "roundtrip_rel_err": err_rt}
+        headline = {"value": mixed_value, "run": rmx, "units_per_step": B, "precision": "mixed"}
+
+    run = headline["run"]
+    ups = headline["units_per_step"]
+    stages = run["stages"]
+    per_signal = {k: v[0] / (a.steps * ups) for k, v in stages.items()}  # ms per transform unit
+    per_launch = {k: v[0] / v[1] for k, v in stages.items()}
+
+    # ---- roofline of the dominant kernel of the headline step
+    work = stage_work(L, N)
+    dom = max(per_signal, key=per_signal.get)
+    t_launch = per_launch[dom] / 1e3
+    if dom.startswith("mixed"):
+        mmas = mixed_mma_count(L, N) * ((B + 7) // 8)
+        ops = mmas * 2.0 * 16 * 8 * 32
+        achieved = ops / t_launch / 1e12
+        roof = {"kernel": dom, "bound": "tensor", "achieved": achieved, "peak": int8_peak, "unit": "TOP/s",
+                "frac": achieved / int8_peak,
+                "peak_source": "int8 mma.sync m16n8k32 chain microbenchmark on this GPU "
+                               "(so3gpu_measure_int8_mma_peak); nominal tcgen05 int8 dense peak 4500 TOP/s",
+                "algorithmic": f"{mmas} mma.sync m16n8k32 s8 per launch (28 slice products, batch {B})"}
+    else:
+        kind, amount, desc = work[dom]
+        achieved = amount / t_launch / 1e12
         roof = {"kernel": dom, "bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                 "frac": achieved / fp64_peak,
                 "peak_source": "FP64 FMA-chain microbenchmark on this GPU (so3gpu_measure_fp64_peak); the "
-                               "measured-peaks file has no FP64 figure",
-                "algorithmic": f"4 flops x {macs:.4g} complex-by-real MACs per launch"}
-    else:
-        peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"] \
-            if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
-        achieved = 2.0 * f_bytes / (per[dom] / 1e3) / 1e9
-        roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "algorithmic": f"read+write of the sample array, 2 x {f_bytes} B"}
+                               "measured-peaks file has no FP64 figure", "algorithmic": desc + " per launch"}
     roof["traffic"] = traffic_from_profiles(dom, L, N)
-    roof["avg_ms"] = per[dom]
+    roof["avg_ms"] = per_launch[dom]
 
     # ---- end to end through the drop-in C ABI with host buffers
     e2e = None
     if not a.no_e2e:
-        e2e = run_e2e(so3, p, fl_host, a.steps, local, world, dist)
+        del fls, fs, backs
+        torch.cuda.empty_cache()
+        e2e = run_e2e(so3, p, fl_host, a.steps, local, world, None)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -304,16 +409,23 @@ def run_ours(a):
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {ex}"}
 
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
-                "warmup": a.warmup, "ms_per_step": total_ms / a.steps, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload(L, N),
-                "precision": "plain FP64 path (the split-precision path is not part of this line)",
-                "roundtrip_rel_err": rt_err,
-                "latency_ms": {"p50": statistics.median(lat), "p99": sorted(lat)[min(len(lat) - 1,
-                                                                                 math.ceil(0.99 * len(lat)) - 1)]},
-                "stage_ms": {k: round(v, 4) for k, v in per.items()},
-                "gpu_launches": int(launches), "roofline": roof, "e2e": e2e, "cpu_baseline": cpu,
-                "clocks": clk.summary()}
+        lat = run["lat"]
+        line = {"metric": METRIC, "value": headline["value"], "unit": UNIT, "n_gpus": world, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": run["total_ms"] / a.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": dict(workload(L, N), batch=B if mixed else 1,
+                               step=f"inverse_batch + forward_batch of {B} signals, split-precision contractions"
+                               if mixed else "one inverse + one forward, FP64"),
+                "precision": headline["precision"],
+                "mixed": mixed,
+                "fp64": {"value": fp64_value, "unit": UNIT, "ms_per_step": r64["total_ms"] / a.steps,
+                         "roundtrip_rel_err": rt_err,
+                         "stage_ms": {k: round(v[0] / v[1], 4) for k, v in r64["stages"].items()},
+                         "latency_ms": {"p50": statistics.median(r64["lat"]), "p99": pct(r64["lat"], 0.99)}},
+                "latency_ms": {"p50": statistics.median(lat), "p99": pct(lat, 0.99)},
+                "stage_ms_per_transform": {k: round(v, 4) for k, v in per_signal.items()},
+                "gpu_launches": int(run["launches"]), "roofline": roof, "e2e": e2e, "cpu_baseline": cpu,
+                "clocks": run["clocks"]}
         print(json.dumps(line), flush=True)
     sdist.finalize()
 

@@ -45,6 +45,24 @@ int so3gpu_inverse_real(so3gpu_context *ctx, double *f, const void *flmn,
 int so3gpu_forward_real(so3gpu_context *ctx, void *flmn, const double *f,
                         const so3_parameters_t *parameters);
 
+/* Batches of `count` signals sharing one parameter set (no counterpart in the
+ * reference).  f and flmn are host arrays of `count` device pointers.
+ * precision SO3GPU_PRECISION_FP64: the FP64 path signal by signal (results
+ * identical to so3gpu_inverse / so3gpu_forward).  SO3GPU_PRECISION_MIXED_INT8:
+ * the Wigner contractions of all signals run as int8 tensor-core products
+ * (7-slice Ozaki split, exact int32 accumulation, FP64 recombination) while
+ * Delta, the quadrature weights and every DFT stay FP64; normwise relative
+ * error against the FP64 path below 1e-10 (about 1e-12 measured).  Real
+ * signals (parameters->reality) always use the FP64 path.  The batch
+ * workspace holds `count` scratch plane sets plus the sliced operands
+ * (about 0.9 GB per group of 8 signals at L = 512, N = 64). */
+#define SO3GPU_PRECISION_FP64 0
+#define SO3GPU_PRECISION_MIXED_INT8 1
+int so3gpu_inverse_batch(so3gpu_context *ctx, void *const *f, const void *const *flmn, int count,
+                         const so3_parameters_t *parameters, int precision);
+int so3gpu_forward_batch(so3gpu_context *ctx, void *const *flmn, const void *const *f, int count,
+                         const so3_parameters_t *parameters, int precision);
+
 /* Same as so3_conv_s2toso3_harmonic_convolution / so3_conv_harmonic_convolution. */
 int so3gpu_s2toso3_harmonic_convolution(so3gpu_context *ctx, void *hlmn, const so3_parameters_t *h_parameters,
                                         const void *flm, const void *glm);
@@ -57,12 +75,16 @@ int so3gpu_harmonic_convolution(so3gpu_context *ctx, void *hlmn, const so3_param
  * accumulated milliseconds and launch counts per stage since the previous
  * call (stages: 0 inverse contraction, 1 inverse beta, 2 inverse alpha,
  * 3 inverse gamma, 4 forward gamma, 5 forward alpha, 6 forward beta and
- * quadrature convolution, 7 forward contraction) and resets them. */
+ * quadrature convolution, 7 forward contraction, 8 / 9 split-precision
+ * inverse / forward contraction of a batch) and resets them. */
 int so3gpu_stage_timing(so3gpu_context *ctx, int enable);
 int so3gpu_stage_times(so3gpu_context *ctx, double *total_ms, long long *counts, int n);
 /* Measured FP64 fused multiply-add throughput of the device in TFLOP/s
  * (2 flops per FMA), from a register-resident FMA chain kernel. */
 double so3gpu_measure_fp64_peak(int device);
+/* Measured int8 tensor-core throughput in TOP/s (2 ops per multiply-add) of
+ * mma.sync m16n8k32, the instruction of the split-precision contractions. */
+double so3gpu_measure_int8_mma_peak(int device);
 
 /* Kernel variants of the DFT stages for the geometry of p (L, N, sampling,
  * reality) on a device: 8 entries indexed like so3gpu_stage_times (only the

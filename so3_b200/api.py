@@ -297,6 +297,33 @@ class Context:
             _lib.check("so3gpu_forward")
         return out
 
+    def _batch(self, fn, ins, outs, q, precision, name):
+        if precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
+        n = len(ins)
+        pin = (ctypes.c_void_p * n)(*[t.data_ptr() for t in ins])
+        pout = (ctypes.c_void_p * n)(*[t.data_ptr() for t in outs])
+        if fn(self._c, pout, pin, n, ctypes.byref(q), PRECISIONS[precision]):
+            _lib.check(name)
+        return outs
+
+    def inverse_batch(self, flmns, p, precision="fp64", outs=None):
+        """Inverse transforms of a list of coefficient tensors with one
+        parameter set; precision "fp64" or "mixed" (int8 split contractions)."""
+        import torch
+        q = _s(p)
+        if outs is None:
+            dt = torch.float64 if q.reality else torch.complex128
+            outs = [torch.empty(f_size(q), dtype=dt, device=x.device) for x in flmns]
+        return self._batch(self._lib.so3gpu_inverse_batch, flmns, outs, q, precision, "so3gpu_inverse_batch")
+
+    def forward_batch(self, fs, p, precision="fp64", outs=None):
+        import torch
+        q = _s(p)
+        if outs is None:
+            outs = [torch.zeros(flmn_size(q), dtype=torch.complex128, device=x.device) for x in fs]
+        return self._batch(self._lib.so3gpu_forward_batch, fs, outs, q, precision, "so3gpu_forward_batch")
+
     def s2toso3(self, hp, flm, glm, out=None):
         import torch
         q = _s(hp)
@@ -321,13 +348,22 @@ class Context:
 
 
 STAGES = ["inv_contract", "inv_beta", "inv_alpha", "inv_gamma", "fwd_gamma", "fwd_alpha", "fwd_beta_conv",
-          "fwd_contract"]
+          "fwd_contract", "mixed_inv_contract", "mixed_fwd_contract"]
+
+PRECISIONS = {"fp64": 0, "mixed": 1}
 
 
 def measure_fp64_peak(device: int = 0) -> float:
     """Measured FP64 FMA throughput (TFLOP/s) of the device."""
     v = _lib.load().so3gpu_measure_fp64_peak(device)
     _lib.check("measure_fp64_peak")
+    return v
+
+
+def measure_int8_mma_peak(device: int = 0) -> float:
+    """Measured int8 mma.sync (m16n8k32) throughput in TOP/s."""
+    v = _lib.load().so3gpu_measure_int8_mma_peak(device)
+    _lib.check("measure_int8_mma_peak")
     return v
 
 

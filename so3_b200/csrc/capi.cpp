@@ -440,6 +440,29 @@ int so3gpu_forward_real(so3gpu_context* c, void* flmn, const double* f, const so
   return ctx_transform(c, flmn, f, p, 1, false);
 }
 
+static int ctx_batch(so3gpu_context* c, void* const* out, const void* const* in, int count, const so3_parameters_t* p,
+                     int precision, bool inverse) {
+  if (!c || !p || (count > 0 && (!out || !in))) return t_status = so3g::fail(so3g::kInvalidParameter, "null argument");
+  for (int i = 0; i < count; i++)
+    if (!out[i] || !in[i]) return t_status = so3g::fail(so3g::kInvalidParameter, "null signal pointer");
+  DeviceScope ds(c->device);
+  std::lock_guard<std::mutex> lk(c->mu);
+  Device* D = so3g::device_state(c->device);
+  const int real = p->reality != 0;
+  int rc = inverse ? so3g::run_inverse_batch(D, &c->wk, *p, real, count, in, out, precision, c->stream)
+                   : so3g::run_forward_batch(D, &c->wk, *p, real, count, in, out, precision, c->stream);
+  return t_status = rc;
+}
+
+int so3gpu_inverse_batch(so3gpu_context* c, void* const* f, const void* const* flmn, int count,
+                         const so3_parameters_t* p, int precision) {
+  return ctx_batch(c, f, flmn, count, p, precision, true);
+}
+int so3gpu_forward_batch(so3gpu_context* c, void* const* flmn, const void* const* f, int count,
+                         const so3_parameters_t* p, int precision) {
+  return ctx_batch(c, flmn, f, count, p, precision, false);
+}
+
 int so3gpu_s2toso3_harmonic_convolution(so3gpu_context* c, void* hlmn, const so3_parameters_t* hp, const void* flm,
                                         const void* glm) {
   if (!c || !hp) return t_status = so3g::fail(so3g::kInvalidParameter, "null argument");
@@ -502,6 +525,17 @@ double so3gpu_measure_fp64_peak(int device) {
   }
   t_status = 0;
   return tf;
+}
+
+double so3gpu_measure_int8_mma_peak(int device) {
+  DeviceScope ds(device);
+  double tops = 0.0;
+  if (so3g::measure_int8_mma_rate(&tops)) {
+    t_status = so3g::kCudaError;
+    return 0.0;
+  }
+  t_status = 0;
+  return tops;
 }
 
 int so3gpu_get_stage_variants(int device, const so3_parameters_t* p, int* var) {

@@ -342,4 +342,116 @@ int run_forward_staged(Device* D, Workspace* wk, const so3_parameters_t& p, int 
   return kOk;
 }
 
+// ------------------------------------------------------------ batches
+namespace {
+
+// Workspace layout of a split-precision batch: nsig scratch plane sets, the
+// sliced operand, and the table of per-signal coefficient pointers.
+struct BatchLayout {
+  size_t wbytes, scratch_off, table_off, total;
+};
+BatchLayout batch_layout(const Geometry& g, const so3_parameters_t& p, int real, int nsig) {
+  BatchLayout b;
+  b.wbytes = (workspace_bytes(p, real) + 255) & ~size_t(255);
+  b.scratch_off = b.wbytes * nsig;
+  b.table_off = b.scratch_off + ((mixed_scratch_bytes(g, nsig) + 255) & ~size_t(255));
+  b.total = b.table_off + sizeof(void*) * (size_t)nsig;
+  return b;
+}
+
+int upload_table(void* dst, const void* const* ptrs, int nsig, cudaStream_t s) {
+  std::vector<const void*> host(ptrs, ptrs + nsig);
+  SO3G_CUDA(cudaMemcpyAsync(dst, host.data(), sizeof(void*) * (size_t)nsig, cudaMemcpyHostToDevice, s));
+  return cudaStreamSynchronize(s) == cudaSuccess ? kOk : fail(kCudaError, "pointer table upload");
+}
+
+}  // namespace
+
+int run_inverse_batch(Device* D, Workspace* wk, const so3_parameters_t& p, int real, int nsig,
+                      const void* const* flmn_d, void* const* f_d, int precision, cudaStream_t s) {
+  if (nsig < 0) return fail(kInvalidParameter, "negative batch size");
+  if (precision != kPrecFp64 && precision != kPrecMixedInt8) return fail(kInvalidParameter, "unknown precision");
+  if (precision == kPrecFp64 || real) {
+    for (int b = 0; b < nsig; b++)
+      if (int rc = run_inverse(D, wk, p, flmn_d[b], f_d[b], real, s)) return rc;
+    return kOk;
+  }
+  if (nsig == 0) return kOk;
+  Resources r;
+  if (int rc = acquire(D, p, real, s, &r, false)) return rc;
+  const BatchLayout bl = batch_layout(r.g, p, real, nsig);
+  void* ws = nullptr;
+  if (int rc = ensure_ws(wk, bl.total, &ws)) return rc;
+  char* base = static_cast<char*>(ws);
+  double2* W = reinterpret_cast<double2*>(base);
+  if (int rc = ensure_tuned(D, p, real, &r, W, s)) return rc;
+  if (int rc = upload_table(base + bl.table_off, flmn_d, nsig, s)) return rc;
+  StageTimer* T = &wk->timer;
+  cudaEvent_t ev;
+  int rc;
+  const long long wstride = (long long)(bl.wbytes / sizeof(double2));
+  timer_begin(T, s, &ev);
+  rc = launch_mixed_inverse(r.g, p.n_mode, reinterpret_cast<const double2* const*>(base + bl.table_off), nsig, r.bases,
+                            r.dl, W, wstride, base + bl.scratch_off, s);
+  if (rc) return rc;
+  timer_end(T, s, kStMixInv, ev);
+  for (int b = 0; b < nsig; b++) {
+    double2* Wb = W + (size_t)b * wstride;
+    timer_begin(T, s, &ev);
+    if ((rc = launch_inv_beta(r.g, r.pP, Wb, s))) return rc;
+    timer_end(T, s, kStInvBeta, ev);
+    timer_begin(T, s, &ev);
+    if ((rc = launch_inv_alpha(r.g, r.pP, Wb, s))) return rc;
+    timer_end(T, s, kStInvAlpha, ev);
+    timer_begin(T, s, &ev);
+    if ((rc = launch_inv_gamma(r.g, r.pg, Wb, f_d[b], s))) return rc;
+    timer_end(T, s, kStInvGamma, ev);
+  }
+  return kOk;
+}
+
+int run_forward_batch(Device* D, Workspace* wk, const so3_parameters_t& p, int real, int nsig, const void* const* f_d,
+                      void* const* flmn_d, int precision, cudaStream_t s) {
+  if (nsig < 0) return fail(kInvalidParameter, "negative batch size");
+  if (precision != kPrecFp64 && precision != kPrecMixedInt8) return fail(kInvalidParameter, "unknown precision");
+  if (precision == kPrecFp64 || real) {
+    for (int b = 0; b < nsig; b++)
+      if (int rc = run_forward(D, wk, p, f_d[b], flmn_d[b], real, s)) return rc;
+    return kOk;
+  }
+  if (nsig == 0) return kOk;
+  Resources r;
+  if (int rc = acquire(D, p, real, s, &r, true)) return rc;
+  const BatchLayout bl = batch_layout(r.g, p, real, nsig);
+  void* ws = nullptr;
+  if (int rc = ensure_ws(wk, bl.total, &ws)) return rc;
+  char* base = static_cast<char*>(ws);
+  double2* W = reinterpret_cast<double2*>(base);
+  if (int rc = ensure_tuned(D, p, real, &r, W, s)) return rc;
+  if (int rc = upload_table(base + bl.table_off, flmn_d, nsig, s)) return rc;
+  StageTimer* T = &wk->timer;
+  cudaEvent_t ev;
+  int rc;
+  const long long wstride = (long long)(bl.wbytes / sizeof(double2));
+  for (int b = 0; b < nsig; b++) {
+    double2* Wb = W + (size_t)b * wstride;
+    timer_begin(T, s, &ev);
+    if ((rc = launch_fwd_gamma(r.g, r.pg, f_d[b], Wb, s))) return rc;
+    timer_end(T, s, kStFwdGamma, ev);
+    timer_begin(T, s, &ev);
+    if ((rc = launch_fwd_alpha(r.g, r.pP, Wb, s))) return rc;
+    timer_end(T, s, kStFwdAlpha, ev);
+    timer_begin(T, s, &ev);
+    if ((rc = launch_fwd_beta_conv(r.g, r.pP, r.pc, r.wr, Wb, s))) return rc;
+    timer_end(T, s, kStFwdBetaConv, ev);
+  }
+  timer_begin(T, s, &ev);
+  rc = launch_mixed_forward(r.g, p.n_mode, W, wstride, nsig, r.bases, r.dl,
+                            reinterpret_cast<double2* const*>(base + bl.table_off), p.storage == SO3_STORAGE_COMPACT,
+                            base + bl.scratch_off, s);
+  if (rc) return rc;
+  timer_end(T, s, kStMixFwd, ev);
+  return kOk;
+}
+
 }  // namespace so3g

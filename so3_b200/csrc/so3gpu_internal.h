@@ -102,6 +102,8 @@ enum Stage : int {
   kStFwdAlpha,
   kStFwdBetaConv,
   kStFwdContract,
+  kStMixInv,  // split-precision contraction (slicing + tensor-core products), inverse
+  kStMixFwd,  // split-precision contraction, forward
   kStCount = 16
 };
 struct StageTimer {
@@ -185,8 +187,24 @@ int autotune_stages(Geometry* g, const FftPlan& pP, const FftPlan& pg, const Fft
 // Number of kernel variants the tuner can choose from for a stage.
 int stage_variants(const Geometry& g, const FftPlan& pP, const FftPlan& pg, const FftPlan& pc, int stage);
 int measure_fp64_fma_rate(double* tflops);
+int measure_int8_mma_rate(double* tops);
+
+// Split-precision (int8 tensor-core) contractions of a batch of complex
+// signals sharing one parameter set.  flmn_dev / W: per-signal coefficient
+// pointers (a device array of nsig pointers) and scratch planes (signal b at
+// W + b * wstride); scratch: mixed_scratch_bytes(g, nsig) bytes.
+size_t mixed_scratch_bytes(const Geometry& g, int nsig);
+int launch_mixed_inverse(const Geometry& g, int n_mode, const double2* const* flmn_dev, int nsig,
+                         const long long* bases, const double* dl, double2* W, long long wstride, void* scratch,
+                         cudaStream_t s);
+int launch_mixed_forward(const Geometry& g, int n_mode, const double2* W, long long wstride, int nsig,
+                         const long long* bases, const double* dl, double2* const* flmn_dev, int storage_compact,
+                         void* scratch, cudaStream_t s);
 
 // ---------------------------------------------------------------- drivers
+// Contraction arithmetic of a batch: FP64 (the reference-exact path) or the
+// int8 split (complex signals only; real signals always use FP64).
+enum Precision : int { kPrecFp64 = 0, kPrecMixedInt8 = 1 };
 // Lock-protected creation of the per-device read-only resources a transform
 // with parameters p needs; safe to call before stream capture.
 // Tuned / pinned stage variants of a geometry (get: 1 if known, else 0).
@@ -200,6 +218,11 @@ int run_inverse(Device* D, Workspace* wk, const so3_parameters_t& p, const void*
                 cudaStream_t s);
 int run_forward(Device* D, Workspace* wk, const so3_parameters_t& p, const void* f_d, void* flmn_d, int real,
                 cudaStream_t s);
+// Batches: f_d / flmn_d are host arrays of nsig device pointers.
+int run_inverse_batch(Device* D, Workspace* wk, const so3_parameters_t& p, int real, int nsig,
+                      const void* const* flmn_d, void* const* f_d, int precision, cudaStream_t s);
+int run_forward_batch(Device* D, Workspace* wk, const so3_parameters_t& p, int real, int nsig, const void* const* f_d,
+                      void* const* flmn_d, int precision, cudaStream_t s);
 
 // Drop-in calls on caller buffers that may live in host memory: the
 // transform runs in chunks (|n| ranges for the contractions, beta-row ranges

@@ -1,0 +1,111 @@
+"""Split-precision batch path: int8 tensor-core contractions (7-slice Ozaki
+split) against the FP64 path on the same inputs.  Tolerance: normwise
+relative error 1e-10 (the split path's contract); measured values sit near
+1e-12.  The FP64 path itself is pinned to the oracle by test_gpu_parity."""
+import numpy as np
+import pytest
+
+import so3_b200 as so3
+from so3_b200 import synth
+from tests.helpers import params, rel_err
+
+pytestmark = pytest.mark.gpu
+
+TOL_MIXED = 1e-10
+
+
+def _run(p, nsig, seed, dist="uniform"):
+    import torch
+    ctx = so3.Context(0)
+    fls = [torch.from_numpy(synth.gen_flmn(p, seed + i, dist)).cuda() for i in range(nsig)]
+    f64 = ctx.inverse_batch(fls, p, "fp64")
+    fmx = ctx.inverse_batch(fls, p, "mixed")
+    # forward from the same (FP64) samples
+    b64 = ctx.forward_batch(f64, p, "fp64")
+    bmx = ctx.forward_batch(f64, p, "mixed")
+    torch.cuda.synchronize()
+    return ([x.cpu().numpy() for x in fls], [x.cpu().numpy() for x in f64], [x.cpu().numpy() for x in fmx],
+            [x.cpu().numpy() for x in b64], [x.cpu().numpy() for x in bmx])
+
+
+CASES = [
+    dict(L=32, N=8, nsig=3),
+    dict(L=24, N=5, nsig=9, order=0, storage=1, L0=2),  # two signal groups, compact, zero-first
+    dict(L=20, N=6, nsig=4, mode=1),                    # even n only
+    dict(L=20, N=6, nsig=2, mode=3),                    # |n| = N-1 only
+    dict(L=20, N=6, nsig=2, mode=4),                    # l = |n| only
+    dict(L=33, N=4, nsig=5, sampling=1, method=1),      # MWSS, Trapani, L not a multiple of 32
+    dict(L=1, N=1, nsig=2),
+    dict(L=8, N=8, nsig=1),
+]
+
+
+@pytest.mark.parametrize("kw", CASES, ids=[str(i) for i in range(len(CASES))])
+def test_mixed_batch_matches_fp64(kw):
+    kw = dict(kw)
+    nsig = kw.pop("nsig")
+    L, N = kw.pop("L"), kw.pop("N")
+    p = params(L, N, **kw)
+    fls, f64, fmx, b64, bmx = _run(p, nsig, 100)
+    for i in range(nsig):
+        assert rel_err(fmx[i], f64[i]) < TOL_MIXED, (i, rel_err(fmx[i], f64[i]))
+        assert rel_err(bmx[i], b64[i]) < TOL_MIXED, (i, rel_err(bmx[i], b64[i]))
+        if p.n_mode == 0:
+            assert rel_err(bmx[i], fls[i]) < 1e-10  # round trip
+
+
+def test_mixed_fp64_batch_equals_single_transforms():
+    """precision "fp64" of the batch API is the single-signal path."""
+    import torch
+    p = params(24, 6)
+    ctx = so3.Context(0)
+    fls = [torch.from_numpy(synth.gen_flmn(p, 7 + i)).cuda() for i in range(3)]
+    outs = ctx.inverse_batch(fls, p, "fp64")
+    for x, o in zip(fls, outs):
+        ref = ctx.inverse(x, p)
+        torch.cuda.synchronize()
+        assert np.array_equal(o.cpu().numpy(), ref.cpu().numpy())
+
+
+def test_mixed_real_signals_use_fp64():
+    import torch
+    p = params(24, 6, reality=1)
+    ctx = so3.Context(0)
+    fls = [torch.from_numpy(synth.gen_flmn(p, 3 + i)).cuda() for i in range(2)]
+    a = ctx.inverse_batch(fls, p, "fp64")
+    b = ctx.inverse_batch(fls, p, "mixed")
+    torch.cuda.synchronize()
+    for x, y in zip(a, b):
+        assert np.array_equal(x.cpu().numpy(), y.cpu().numpy())
+
+
+def test_mixed_batched_config_L128_N16_gauss():
+    """The batched configuration's shape (L=128, N=16, MW, padded, Risbo,
+    complex Gaussian with variance ~ (l+1)^-2, dynamic range ~1e4), 8 signals."""
+    p = params(128, 16)
+    fls, f64, fmx, b64, bmx = _run(p, 8, 500, "gauss")
+    errs = [rel_err(fmx[i], f64[i]) for i in range(8)] + [rel_err(bmx[i], b64[i]) for i in range(8)]
+    assert max(errs) < TOL_MIXED, errs
+
+
+def test_mixed_metric_size_L512():
+    """L=512 (the metric's band limit) with a few n-planes, 2 signals."""
+    p = params(512, 3)
+    fls, f64, fmx, b64, bmx = _run(p, 2, 900)
+    for i in range(2):
+        assert rel_err(fmx[i], f64[i]) < TOL_MIXED
+        assert rel_err(bmx[i], b64[i]) < TOL_MIXED
+
+
+def test_mixed_forward_leaves_skipped_blocks():
+    import torch
+    p = params(20, 6, mode=1)
+    ctx = so3.Context(0)
+    fls = [torch.from_numpy(synth.gen_flmn(p, 1)).cuda()]
+    f = ctx.inverse_batch(fls, p, "fp64")
+    out = [torch.full((so3.flmn_size(p),), 7.0 + 1j, dtype=torch.complex128, device="cuda")]
+    ctx.forward_batch(f, p, "mixed", outs=out)
+    ref = [torch.full((so3.flmn_size(p),), 7.0 + 1j, dtype=torch.complex128, device="cuda")]
+    ctx.forward_batch(f, p, "fp64", outs=ref)
+    torch.cuda.synchronize()
+    assert rel_err(out[0].cpu().numpy(), ref[0].cpu().numpy()) < TOL_MIXED

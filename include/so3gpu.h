@@ -108,6 +108,39 @@ int so3gpu_set_stage_variants(int device, const so3_parameters_t *p, const int *
  * overlaps race: serialise them. */
 int so3gpu_inverse_noalloc(void *f, const void *flmn, const so3_parameters_t *parameters, void *stream);
 
+/* Request server (no counterpart in the reference): inverse (kind 0),
+ * forward (kind 1) and directional-convolution (kind 2: in = flm, in2 = glm,
+ * both L*L complex; out = samples of the inverse transform of the
+ * so3_conv_s2toso3_harmonic_convolution result) requests of any parameters,
+ * submitted from any host thread, run on one device with continuous
+ * batching.  Up to max_inflight units run at once on separate streams;
+ * queued split-precision (SO3GPU_PRECISION_MIXED_INT8) requests with
+ * identical parameters and direction are admitted together, up to
+ * max_batch per unit.  Each unit reserves its scratch from memory_budget
+ * bytes (stream-ordered allocations) and is admitted when a slot and the
+ * budget allow, first come first served; a request that alone exceeds the
+ * budget completes with status 4.  max_L (> 0) builds the Wigner tables up
+ * to that band limit at creation and rejects larger requests; 0 lets the
+ * tables grow, which synchronises the device when it happens.  Buffers are
+ * device pointers owned by the caller until the request completes.
+ * submit returns the request id (>= 0) or minus a status code.  poll / wait
+ * return 1 once the request is done (filling queueing and total latency in
+ * microseconds, the size of the unit it ran in, and its status; the request
+ * is then forgotten), poll returns 0 while it is pending, -1 for unknown ids.
+ * destroy waits for every submitted request. */
+typedef struct so3gpu_server so3gpu_server;
+so3gpu_server *so3gpu_server_create(int device, size_t memory_budget, int max_inflight, int max_batch, int max_L);
+void so3gpu_server_destroy(so3gpu_server *server);
+long long so3gpu_server_submit(so3gpu_server *server, int kind, const so3_parameters_t *parameters,
+                               const void *in, const void *in2, void *out, int precision);
+int so3gpu_server_poll(so3gpu_server *server, long long id, double *queue_us, double *total_us, int *batch,
+                       int *status);
+int so3gpu_server_wait(so3gpu_server *server, long long id, double *queue_us, double *total_us, int *batch,
+                       int *status);
+void so3gpu_server_drain(so3gpu_server *server);
+void so3gpu_server_stats(so3gpu_server *server, long long *submitted, long long *completed, long long *units,
+                         size_t *peak_bytes);
+
 /* Diagnostics. */
 int so3gpu_last_status(void);
 const char *so3gpu_last_error(void);

@@ -88,6 +88,13 @@ SIGNATURES = {
     "so3gpu_measure_int8_mma_peak": (ctypes.c_double, [_I]),
     "so3gpu_get_stage_variants": (_I, [_I, _P, _VP]),
     "so3gpu_inverse_batch": (_I, [_VP, _VP, _VP, _I, _P, _I]),
+    "so3gpu_server_create": (_VP, [_I, ctypes.c_size_t, _I, _I, _I]),
+    "so3gpu_server_destroy": (None, [_VP]),
+    "so3gpu_server_submit": (ctypes.c_longlong, [_VP, _I, _P, _VP, _VP, _VP, _I]),
+    "so3gpu_server_poll": (_I, [_VP, ctypes.c_longlong, _VP, _VP, _VP, _VP]),
+    "so3gpu_server_wait": (_I, [_VP, ctypes.c_longlong, _VP, _VP, _VP, _VP]),
+    "so3gpu_server_drain": (None, [_VP]),
+    "so3gpu_server_stats": (None, [_VP, _VP, _VP, _VP, _VP]),
     "so3gpu_forward_batch": (_I, [_VP, _VP, _VP, _I, _P, _I]),
     "so3gpu_set_stage_variants": (_I, [_I, _P, _VP]),
     "so3gpu_inverse_noalloc": (_I, [_VP, _VP, _P, _VP]),

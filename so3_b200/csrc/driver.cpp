@@ -367,6 +367,11 @@ int upload_table(void* dst, const void* const* ptrs, int nsig, cudaStream_t s) {
 
 }  // namespace
 
+size_t batch_workspace_bytes(const so3_parameters_t& p, int real, int nsig, int precision) {
+  if (precision == kPrecFp64 || real || nsig <= 0) return workspace_bytes(p, real);
+  return batch_layout(make_geometry(p, real), p, real, nsig).total;
+}
+
 int run_inverse_batch(Device* D, Workspace* wk, const so3_parameters_t& p, int real, int nsig,
                       const void* const* flmn_d, void* const* f_d, int precision, cudaStream_t s) {
   if (nsig < 0) return fail(kInvalidParameter, "negative batch size");

@@ -1,0 +1,415 @@
+// Request-serving loop: inverse, forward and directional-convolution requests
+// of mixed (L, N) submitted from any host thread, run on one GPU with
+// continuous batching.
+//
+//  * Slots: up to max_inflight requests (or batches) are on the device at
+//    once, each on its own CUDA stream with its own scratch, so their kernels
+//    overlap.  A request that arrives while others run is admitted as soon as
+//    a slot and memory free up; it never waits for the running ones to end.
+//  * Memory admission: every admitted unit reserves its scratch bytes from a
+//    budget; scratch comes from the stream-ordered allocator
+//    (cudaMallocAsync / cudaFreeAsync on the slot's stream), so admitting and
+//    retiring work never synchronises the device.  A request that alone
+//    exceeds the budget fails with status 4.
+//  * Batching: queued split-precision requests with identical parameters and
+//    direction are admitted together (up to max_batch) and share one
+//    int8 contraction launch; everything else runs one request per slot.
+//    Results do not depend on batch companions: the split is per signal and
+//    the int32 accumulation is exact.
+//  * Resident state: Wigner tables, DFT plans, index tables and tuned kernel
+//    variants are the per-device ones of the library, shared by all slots;
+//    the Delta tables are built up to max_L at creation so they never grow
+//    (a growing table would be reallocated under running work).
+//  * Completion: a host callback enqueued after each unit stamps its finish
+//    time and wakes the worker thread, which retires the slot and admits more.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "so3/so3_sampling.h"
+#include "so3gpu.h"
+#include "so3gpu_internal.h"
+
+namespace so3g {
+namespace {
+
+double now_us() {
+  return std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+struct Req {
+  long long id = 0;
+  int kind = 0;  // 0 inverse, 1 forward, 2 directional convolution + inverse
+  so3_parameters_t p{};
+  const void* in = nullptr;
+  const void* in2 = nullptr;
+  void* out = nullptr;
+  int precision = 0;
+  double t_submit = 0, t_admit = 0, t_done = 0;
+  int status = 0;
+  bool done = false;
+  int batch = 1;
+};
+
+struct Slot {
+  cudaStream_t s = nullptr;
+  Workspace wk;
+  std::vector<Req*> reqs;
+  size_t bytes = 0;
+  bool busy = false;
+  int status = 0;
+  std::atomic<bool> finished{false};
+  std::atomic<double> t_finish{0.0};
+  void* owner = nullptr;
+};
+
+bool same_batch(const Req& a, const Req& b) {
+  return a.kind == b.kind && a.precision == b.precision && a.p.L == b.p.L && a.p.N == b.p.N &&
+         a.p.L0 == b.p.L0 && a.p.sampling_scheme == b.p.sampling_scheme && a.p.n_order == b.p.n_order &&
+         a.p.storage == b.p.storage && a.p.n_mode == b.p.n_mode && a.p.dl_method == b.p.dl_method &&
+         a.p.reality == b.p.reality;
+}
+
+}  // namespace
+
+class Server {
+ public:
+  Server(int device, size_t budget, int slots, int max_batch, int max_L)
+      : device_(device), budget_(budget), max_batch_(max_batch < 1 ? 1 : (max_batch > 64 ? 64 : max_batch)) {
+    nslots_ = slots < 1 ? 1 : slots;
+    max_L_ = max_L;
+  }
+
+  int start() {
+    SO3G_CUDA(cudaSetDevice(device_));
+    D_ = device_state(device_);
+    slots_.reserve(nslots_);
+    for (int i = 0; i < nslots_; i++) {
+      auto sl = std::make_unique<Slot>();
+      SO3G_CUDA(cudaStreamCreateWithFlags(&sl->s, cudaStreamNonBlocking));
+      sl->owner = this;
+      slots_.push_back(std::move(sl));
+    }
+    // keep freed scratch in the pool up to the budget (no release to the OS
+    // between requests)
+    cudaMemPool_t pool;
+    SO3G_CUDA(cudaDeviceGetDefaultMemPool(&pool, device_));
+    unsigned long long thr = budget_;
+    SO3G_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    if (max_L_ > 0) {
+      const double* t;
+      std::lock_guard<std::mutex> lk(D_->mu);
+      for (int m = 0; m < 2; m++)
+        if (int rc = ensure_dl(D_, max_L_, m, slots_[0]->s, &t)) return rc;
+    }
+    worker_ = std::thread([this] { loop(); });
+    return kOk;
+  }
+
+  ~Server() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    if (worker_.joinable()) worker_.join();
+    for (auto& sl : slots_)
+      if (sl->s) {
+        cudaStreamSynchronize(sl->s);
+        cudaStreamDestroy(sl->s);
+      }
+    for (auto& kv : reqs_) delete kv.second;
+  }
+
+  long long submit(int kind, const so3_parameters_t& p, const void* in, const void* in2, void* out, int precision) {
+    if (kind < 0 || kind > 2 || !in || !out || (kind == 2 && !in2))
+      return -fail(kInvalidParameter, "server request: bad kind or null buffer");
+    if (precision != kPrecFp64 && precision != kPrecMixedInt8) return -fail(kInvalidParameter, "unknown precision");
+    if (int rc = validate(p, p.reality != 0)) return -rc;
+    if (kind == 2 && p.reality) return -fail(kUnsupported, "convolution requests produce complex samples");
+    if (max_L_ > 0 && p.L > max_L_) return -fail(kUnsupported, "request band limit above the server's max_L");
+    Req* r = new Req();
+    r->kind = kind;
+    r->p = p;
+    r->in = in;
+    r->in2 = in2;
+    r->out = out;
+    r->precision = (kind == 2 || p.reality) ? kPrecFp64 : precision;
+    r->t_submit = now_us();
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      r->id = next_id_++;
+      reqs_[r->id] = r;
+      queue_.push_back(r);
+    }
+    cv_.notify_all();
+    return r->id;
+  }
+
+  // 1 done (fills outputs and forgets the request), 0 pending, <0 unknown id
+  int query(long long id, bool wait, double* queue_us, double* total_us, int* batch, int* status) {
+    std::unique_lock<std::mutex> lk(mu_);
+    auto it = reqs_.find(id);
+    if (it == reqs_.end()) return -1;
+    Req* r = it->second;
+    if (wait) done_cv_.wait(lk, [&] { return r->done; });
+    if (!r->done) return 0;
+    if (queue_us) *queue_us = r->t_admit - r->t_submit;
+    if (total_us) *total_us = r->t_done - r->t_submit;
+    if (batch) *batch = r->batch;
+    if (status) *status = r->status;
+    reqs_.erase(it);
+    delete r;
+    return 1;
+  }
+
+  void drain() {
+    std::unique_lock<std::mutex> lk(mu_);
+    done_cv_.wait(lk, [&] { return queue_.empty() && busy_ == 0; });
+  }
+
+  void stats(long long* submitted, long long* completed, long long* batches, size_t* peak_bytes) {
+    std::lock_guard<std::mutex> lk(mu_);
+    if (submitted) *submitted = next_id_;
+    if (completed) *completed = completed_;
+    if (batches) *batches = units_;
+    if (peak_bytes) *peak_bytes = peak_bytes_;
+  }
+
+ private:
+  static void CUDART_CB on_done(void* arg) {
+    Slot* sl = static_cast<Slot*>(arg);
+    sl->t_finish.store(now_us());
+    sl->finished.store(true);
+    Server* sv = static_cast<Server*>(sl->owner);
+    { std::lock_guard<std::mutex> lk(sv->mu_); }
+    sv->cv_.notify_all();
+  }
+
+  size_t unit_bytes(const std::vector<Req*>& b) const {
+    const Req& r = *b[0];
+    const int real = r.p.reality != 0;
+    size_t need = batch_workspace_bytes(r.p, real, (int)b.size(), r.precision);
+    if (r.kind == 2) need = ((need + 255) & ~size_t(255)) + (size_t)so3_sampling_flmn_size(&r.p) * sizeof(double2);
+    return need;
+  }
+
+  // Enqueues the unit's work, the release of its scratch and the completion
+  // callback on the slot's stream (worker thread, no lock held).
+  void launch(Slot* sl) {
+    const Req& r = *sl->reqs[0];
+    const int real = r.p.reality != 0;
+    const int n = (int)sl->reqs.size();
+    int rc = kOk;
+    void* ws = nullptr;
+    if (cudaMallocAsync(&ws, sl->bytes, sl->s) != cudaSuccess) {
+      cudaGetLastError();
+      rc = fail(kOutOfMemory, "server scratch allocation failed");
+    }
+    if (rc == kOk) {
+      sl->wk.ws = ws;
+      sl->wk.ws_bytes = sl->bytes;
+      if (r.kind == 2) {
+        const size_t wb = (workspace_bytes(r.p, 0) + 255) & ~size_t(255);
+        double2* hlmn = reinterpret_cast<double2*>(static_cast<char*>(ws) + wb);
+        const long long* hb = nullptr;
+        {
+          std::lock_guard<std::mutex> lk(D_->mu);
+          rc = ensure_bases(D_, r.p, 0, &hb);
+        }
+        if (rc == kOk)
+          rc = launch_s2toso3(r.p, hb, static_cast<const double2*>(r.in), static_cast<const double2*>(r.in2), hlmn,
+                              sl->s);
+        if (rc == kOk) rc = run_inverse(D_, &sl->wk, r.p, hlmn, r.out, 0, sl->s);
+      } else {
+        std::vector<const void*> ins(n);
+        std::vector<void*> outs(n);
+        for (int i = 0; i < n; i++) {
+          ins[i] = sl->reqs[i]->in;
+          outs[i] = sl->reqs[i]->out;
+        }
+        rc = r.kind == 0 ? run_inverse_batch(D_, &sl->wk, r.p, real, n, ins.data(), outs.data(), r.precision, sl->s)
+                         : run_forward_batch(D_, &sl->wk, r.p, real, n, ins.data(), outs.data(), r.precision, sl->s);
+      }
+      cudaFreeAsync(ws, sl->s);
+      sl->wk.ws = nullptr;
+      sl->wk.ws_bytes = 0;
+    }
+    sl->status = rc;
+    if (cudaLaunchHostFunc(sl->s, on_done, sl) != cudaSuccess) {
+      cudaGetLastError();
+      cudaStreamSynchronize(sl->s);
+      sl->status = sl->status ? sl->status : fail(kCudaError, "server completion callback");
+      on_done(sl);
+    }
+  }
+
+  void retire_locked() {
+    for (auto& sl : slots_) {
+      if (!sl->busy || !sl->finished.load()) continue;
+      const double t = sl->t_finish.load();
+      for (Req* r : sl->reqs) {
+        r->t_done = t;
+        r->status = sl->status;
+        r->done = true;
+        completed_++;
+      }
+      sl->reqs.clear();
+      sl->busy = false;
+      sl->finished.store(false);
+      inflight_bytes_ -= sl->bytes;
+      sl->bytes = 0;
+      busy_--;
+    }
+  }
+
+  void loop() {
+    cudaSetDevice(device_);
+    std::unique_lock<std::mutex> lk(mu_);
+    for (;;) {
+      retire_locked();
+      done_cv_.notify_all();
+      if (stop_ && queue_.empty() && busy_ == 0) break;
+      // admission: first-come first-served, as long as a slot and the budget allow
+      bool launched = false;
+      while (!queue_.empty()) {
+        Slot* free_slot = nullptr;
+        for (auto& sl : slots_)
+          if (!sl->busy) {
+            free_slot = sl.get();
+            break;
+          }
+        if (!free_slot) break;
+        std::vector<Req*> unit{queue_.front()};
+        if (unit[0]->precision == kPrecMixedInt8 && unit[0]->kind != 2) {
+          for (size_t i = 1; i < queue_.size() && (int)unit.size() < max_batch_; i++)
+            if (same_batch(*queue_[i], *unit[0])) unit.push_back(queue_[i]);
+        }
+        size_t need = unit_bytes(unit);
+        while (need > budget_ && unit.size() > 1) {  // shrink the batch to fit
+          unit.pop_back();
+          need = unit_bytes(unit);
+        }
+        if (need > budget_) {  // can never run
+          Req* r = unit[0];
+          queue_.pop_front();
+          r->status = fail(kOutOfMemory, "request scratch exceeds the server memory budget");
+          r->t_admit = r->t_done = now_us();
+          r->done = true;
+          completed_++;
+          continue;
+        }
+        if (inflight_bytes_ + need > budget_) break;  // wait for memory
+        for (Req* r : unit) {
+          for (auto it = queue_.begin(); it != queue_.end(); ++it)
+            if (*it == r) {
+              queue_.erase(it);
+              break;
+            }
+          r->t_admit = now_us();
+          r->batch = (int)unit.size();
+        }
+        free_slot->reqs = unit;
+        free_slot->bytes = need;
+        free_slot->busy = true;
+        free_slot->finished.store(false);
+        inflight_bytes_ += need;
+        if (inflight_bytes_ > peak_bytes_) peak_bytes_ = inflight_bytes_;
+        busy_++;
+        units_++;
+        lk.unlock();
+        launch(free_slot);
+        lk.lock();
+        launched = true;
+      }
+      if (!launched)
+        cv_.wait_for(lk, std::chrono::microseconds(200), [&] {
+          if (stop_) return true;
+          for (auto& sl : slots_)
+            if (sl->busy && sl->finished.load()) return true;
+          if (queue_.empty()) return false;
+          for (auto& sl : slots_)
+            if (!sl->busy) return true;
+          return false;
+        });
+    }
+    done_cv_.notify_all();
+  }
+
+  int device_;
+  size_t budget_;
+  int nslots_ = 1, max_batch_ = 8, max_L_ = 0;
+  Device* D_ = nullptr;
+  std::vector<std::unique_ptr<Slot>> slots_;
+  std::thread worker_;
+  std::mutex mu_;
+  std::condition_variable cv_, done_cv_;
+  std::deque<Req*> queue_;
+  std::unordered_map<long long, Req*> reqs_;
+  long long next_id_ = 0, completed_ = 0, units_ = 0;
+  size_t inflight_bytes_ = 0, peak_bytes_ = 0;
+  int busy_ = 0;
+  bool stop_ = false;
+};
+
+}  // namespace so3g
+
+struct so3gpu_server {
+  std::unique_ptr<so3g::Server> impl;
+};
+
+extern "C" {
+
+so3gpu_server* so3gpu_server_create(int device, size_t memory_budget, int max_inflight, int max_batch, int max_L) {
+  auto* s = new so3gpu_server();
+  s->impl = std::make_unique<so3g::Server>(device, memory_budget, max_inflight, max_batch, max_L);
+  const int rc = s->impl->start();
+  so3g_record_status(rc);
+  if (rc) {
+    delete s;
+    return nullptr;
+  }
+  return s;
+}
+
+void so3gpu_server_destroy(so3gpu_server* s) { delete s; }
+
+long long so3gpu_server_submit(so3gpu_server* s, int kind, const so3_parameters_t* p, const void* in, const void* in2,
+                               void* out, int precision) {
+  if (!s || !p) {
+    so3g_record_status(so3g::fail(so3g::kInvalidParameter, "null server or parameters"));
+    return -so3g::kInvalidParameter;
+  }
+  const long long id = s->impl->submit(kind, *p, in, in2, out, precision);
+  so3g_record_status(id < 0 ? (int)-id : 0);
+  return id;
+}
+
+int so3gpu_server_poll(so3gpu_server* s, long long id, double* queue_us, double* total_us, int* batch,
+                       int* status) {
+  return s ? s->impl->query(id, false, queue_us, total_us, batch, status) : -1;
+}
+
+int so3gpu_server_wait(so3gpu_server* s, long long id, double* queue_us, double* total_us, int* batch,
+                       int* status) {
+  return s ? s->impl->query(id, true, queue_us, total_us, batch, status) : -1;
+}
+
+void so3gpu_server_drain(so3gpu_server* s) {
+  if (s) s->impl->drain();
+}
+
+void so3gpu_server_stats(so3gpu_server* s, long long* submitted, long long* completed, long long* units,
+                         size_t* peak_bytes) {
+  if (s) s->impl->stats(submitted, completed, units, peak_bytes);
+}
+
+}  // extern "C"

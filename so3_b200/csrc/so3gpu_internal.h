@@ -218,6 +218,8 @@ int run_inverse(Device* D, Workspace* wk, const so3_parameters_t& p, const void*
                 cudaStream_t s);
 int run_forward(Device* D, Workspace* wk, const so3_parameters_t& p, const void* f_d, void* flmn_d, int real,
                 cudaStream_t s);
+// Workspace bytes a batch of nsig signals needs (run_*_batch).
+size_t batch_workspace_bytes(const so3_parameters_t& p, int real, int nsig, int precision);
 // Batches: f_d / flmn_d are host arrays of nsig device pointers.
 int run_inverse_batch(Device* D, Workspace* wk, const so3_parameters_t& p, int real, int nsig,
                       const void* const* flmn_d, void* const* f_d, int precision, cudaStream_t s);

@@ -1,0 +1,174 @@
+"""Request serving on one GPU: Python face of the so3gpu_server C API.
+
+The loop itself is native (so3_b200/csrc/server.cpp): continuous batching of
+split-precision requests with identical parameters, one CUDA stream per
+in-flight unit, admission by a device-memory budget, per-request queueing and
+total latency.  This module adds device buffers for requests, a seeded
+Poisson request trace, and a trace replayer reporting p50 / p99 latency and
+throughput.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import time
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from .api import SO3Parameters, f_size, flmn_size
+
+KINDS = {"inverse": 0, "forward": 1, "convolve": 2}
+PRECISIONS = {"fp64": 0, "mixed": 1}
+
+
+@dataclass
+class Done:
+    id: int
+    queue_us: float
+    total_us: float
+    batch: int
+    status: int
+
+
+class Server:
+    """so3gpu_server bound to one device.  Buffers are torch CUDA tensors that
+    the caller keeps alive until the request is done."""
+
+    def __init__(self, device: int = 0, memory_budget: int = 120 << 30, max_inflight: int = 8, max_batch: int = 8,
+                 max_L: int = 0):
+        self._lib = _lib.load()
+        self._s = self._lib.so3gpu_server_create(device, memory_budget, max_inflight, max_batch, max_L)
+        if not self._s:
+            _lib.check("so3gpu_server_create")
+        self.device = device
+
+    def close(self):
+        if getattr(self, "_s", None):
+            self._lib.so3gpu_server_destroy(self._s)
+            self._s = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, kind: str, p: SO3Parameters, inp, out, precision: str = "fp64", inp2=None) -> int:
+        q = p.to_struct()
+        rid = self._lib.so3gpu_server_submit(self._s, KINDS[kind], ctypes.byref(q), inp.data_ptr(),
+                                             inp2.data_ptr() if inp2 is not None else None, out.data_ptr(),
+                                             PRECISIONS[precision])
+        if rid < 0:
+            _lib.check("so3gpu_server_submit")
+        return rid
+
+    def _query(self, fn, rid):
+        qu, tu = ctypes.c_double(), ctypes.c_double()
+        b, st = ctypes.c_int(), ctypes.c_int()
+        r = fn(self._s, rid, ctypes.byref(qu), ctypes.byref(tu), ctypes.byref(b), ctypes.byref(st))
+        if r < 0:
+            raise KeyError(rid)
+        return Done(rid, qu.value, tu.value, b.value, st.value) if r == 1 else None
+
+    def wait(self, rid: int) -> Done:
+        return self._query(self._lib.so3gpu_server_wait, rid)
+
+    def poll(self, rid: int):
+        return self._query(self._lib.so3gpu_server_poll, rid)
+
+    def drain(self):
+        self._lib.so3gpu_server_drain(self._s)
+
+    def stats(self) -> dict:
+        a, b, c = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        d = ctypes.c_size_t()
+        self._lib.so3gpu_server_stats(self._s, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(d))
+        return {"submitted": a.value, "completed": b.value, "units": c.value, "peak_bytes": d.value}
+
+
+# --------------------------------------------------------------------- traces
+def make_trace(n: int, rate: float, seed: int, L_range=(16, 1024), N_max: int = 64, p_inverse: float = 0.6,
+               p_convolve: float = 0.0, precision: str = "fp64"):
+    """Seeded request trace: Poisson arrivals at `rate` per second; inverse
+    with probability p_inverse, directional convolution with p_convolve, else
+    forward; complex MW, L log-uniform in L_range (rounded), N uniform in
+    [1, min(L, N_max)]."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, n))
+    lo, hi = math.log(L_range[0]), math.log(L_range[1])
+    out = []
+    for i in range(n):
+        L = int(round(math.exp(rng.uniform(lo, hi))))
+        N = int(rng.integers(1, min(L, N_max) + 1))
+        u = rng.uniform()
+        kind = "inverse" if u < p_inverse else ("convolve" if u < p_inverse + p_convolve else "forward")
+        out.append({"t": float(t[i]), "kind": kind, "L": L, "N": N, "seed": int(rng.integers(1 << 31)),
+                    "precision": precision})
+    return out
+
+
+def request_buffers(req, device="cuda"):
+    """Seeded device input (U(-1,1) real and imaginary parts) and an output
+    buffer for one trace request."""
+    import torch
+    p = SO3Parameters(L=req["L"], N=req["N"])
+    g = torch.Generator(device=device)
+    g.manual_seed(req["seed"])
+
+    def u(n):
+        x = torch.rand(2 * n, dtype=torch.float64, device=device, generator=g) * 2 - 1
+        return torch.view_as_complex(x.view(n, 2))
+
+    if req["kind"] == "inverse":
+        return p, u(flmn_size(p)), None, torch.empty(f_size(p), dtype=torch.complex128, device=device)
+    if req["kind"] == "forward":
+        return p, u(f_size(p)), None, torch.zeros(flmn_size(p), dtype=torch.complex128, device=device)
+    # directional convolution: flm over all l < L, glm only |m| < min(8, N)
+    flm = u(p.L * p.L)
+    glm = u(p.L * p.L)
+    el = torch.arange(p.L * p.L, device=device)
+    l = torch.floor(torch.sqrt(el.double())).long()
+    m = el - l * l - l
+    glm[m.abs() >= min(8, p.N)] = 0
+    return p, flm, glm, torch.empty(f_size(p), dtype=torch.complex128, device=device)
+
+
+def replay(server: Server, trace, keep_outputs: bool = False, time_scale: float = 1.0):
+    """Submits every request at its arrival time (scaled), waits for all, and
+    returns (per-request results, wall seconds).  Inputs are generated before
+    the clock starts."""
+    import torch
+    bufs = [request_buffers(r) for r in trace]
+    torch.cuda.synchronize()
+    ids = []
+    t0 = time.perf_counter()
+    for r, (p, a, b, o) in zip(trace, bufs):
+        dt = r["t"] * time_scale - (time.perf_counter() - t0)
+        if dt > 0:
+            time.sleep(dt)
+        ids.append(server.submit(r["kind"], p, a, o, r["precision"], inp2=b))
+    res = [server.wait(i) for i in ids]
+    wall = time.perf_counter() - t0
+    outs = [b[3] for b in bufs] if keep_outputs else None
+    return res, wall, outs
+
+
+def latency_summary(res, wall):
+    tot = sorted(r.total_us for r in res)
+    q = sorted(r.queue_us for r in res)
+
+    def pct(v, f):
+        return v[min(len(v) - 1, max(0, math.ceil(f * len(v)) - 1))] / 1e3 if v else None
+
+    return {"requests": len(res), "wall_s": wall, "throughput_rps": len(res) / wall if wall > 0 else None,
+            "p50_ms": pct(tot, 0.50), "p99_ms": pct(tot, 0.99), "queue_p50_ms": pct(q, 0.50),
+            "queue_p99_ms": pct(q, 0.99), "failed": sum(1 for r in res if r.status != 0),
+            "mean_batch": float(np.mean([r.batch for r in res])) if res else None}

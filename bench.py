@@ -8,7 +8,7 @@ one forward transform; the metric is units per second, split precision
 against FP64.
 
   * headline step: inverse_batch + forward_batch of --batch signals (default
-    8) with the int8 tensor-core (Ozaki split) contractions, FP64 everywhere
+    16) with the int8 tensor-core (Ozaki split) contractions, FP64 everywhere
     else; its error against the FP64 path is measured on the same inputs;
   * "fp64": one FP64 inverse + forward per step (reference-exact path);
   * "e2e": the FP64 drop-in so3_core_{inverse,forward}_via_ssht on pinned host
@@ -47,7 +47,7 @@ def args_():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--L", type=int, default=512)
     ap.add_argument("--N", type=int, default=64)
-    ap.add_argument("--batch", type=int, default=8,
+    ap.add_argument("--batch", type=int, default=16,
                     help="signals per split-precision step (0: time the FP64 path only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -242,20 +242,25 @@ def stage_work(L, N):
     }
 
 
-def mixed_mma_count(L, N):
-    """mma.sync m16n8k32 instructions one split-precision contraction issues
-    per group of 8 signals (both directions issue the same number): 56 per warp
-    and 32-step of the reduction, 8 warps per CTA."""
+def mixed_tc_macs(L, N, fwd):
+    """int8 multiply-adds the split-precision tensor-core kernel issues per
+    group of 16 signals in one direction: per CTA (pair (mu, nu), 64-row
+    tile) nk reduction chunks of 64, each 2 x 28 tcgen05.mma of 128 x 64 x 32."""
     import numpy as np
-    T = 32
+    T = 64
     MT = (L + T - 1) // T
     mu = np.arange(L)[:, None, None]
     nu = np.arange(N)[None, :, None]
-    t = np.arange(MT)[None, None, :]
+    r0 = (np.arange(MT) * T)[None, None, :]
     lmin = np.maximum(mu, nu)
-    kfirst = (np.maximum(lmin, t * T) // T) * T
-    nk_inv = np.where(kfirst < L, (L - kfirst + T - 1) // T, 0)
-    return int(nk_inv.sum()) * 8 * 56
+    if fwd:
+        any_row = (r0 + T > lmin) & (r0 < L)
+        kend = np.minimum(L, r0 + T)
+        nk = np.where(any_row, (kend + T - 1) // T, 0)
+    else:
+        kstart = (np.maximum(lmin, r0) // T) * T
+        nk = np.where(kstart < L, (L - kstart + T - 1) // T, 0)
+    return int(nk.sum()) * 2 * 28 * 128 * 64 * 32
 
 
 def timed_steps(step, steps, warmup, stream, ctx, so3, sdist, local, world):
@@ -369,14 +374,15 @@ def run_ours(a):
     dom = max(per_signal, key=per_signal.get)
     t_launch = per_launch[dom] / 1e3
     if dom.startswith("mixed"):
-        mmas = mixed_mma_count(L, N) * ((B + 7) // 8)
-        ops = mmas * 2.0 * 16 * 8 * 32
+        macs = mixed_tc_macs(L, N, dom == "mixed_fwd_contract") * ((B + 15) // 16)
+        ops = 2.0 * macs
         achieved = ops / t_launch / 1e12
         roof = {"kernel": dom, "bound": "tensor", "achieved": achieved, "peak": int8_peak, "unit": "TOP/s",
                 "frac": achieved / int8_peak,
-                "peak_source": "int8 mma.sync m16n8k32 chain microbenchmark on this GPU "
-                               "(so3gpu_measure_int8_mma_peak); nominal tcgen05 int8 dense peak 4500 TOP/s",
-                "algorithmic": f"{mmas} mma.sync m16n8k32 s8 per launch (28 slice products, batch {B})"}
+                "peak_source": "tcgen05.mma kind::i8 128x256x32 back-to-back on this GPU "
+                               "(so3gpu_measure_int8_mma_peak); nominal int8 dense peak 4500 TOP/s",
+                "algorithmic": f"{macs:.4g} int8 MACs per launch (28 digit products, batch {B}, "
+                               f"stage = slicing kernel + tensor-core kernel)"}
     else:
         kind, amount, desc = work[dom]
         achieved = amount / t_launch / 1e12

@@ -83,7 +83,8 @@ int so3gpu_stage_times(so3gpu_context *ctx, double *total_ms, long long *counts,
  * (2 flops per FMA), from a register-resident FMA chain kernel. */
 double so3gpu_measure_fp64_peak(int device);
 /* Measured int8 tensor-core throughput in TOP/s (2 ops per multiply-add) of
- * mma.sync m16n8k32, the instruction of the split-precision contractions. */
+ * tcgen05.mma kind::i8 (M=128, N=256, K=32, shared-memory operands, tensor-
+ * memory accumulators), the instruction of the split-precision contractions. */
 double so3gpu_measure_int8_mma_peak(int device);
 
 /* Kernel variants of the DFT stages for the geometry of p (L, N, sampling,
@@ -101,8 +102,8 @@ int so3gpu_set_stage_variants(int device, const so3_parameters_t *p, const int *
  * loops that must not allocate after start-up).  f and flmn are device
  * pointers; stream is a cudaStream_t (NULL: legacy default stream).  Its
  * scratch, Wigner tables and FFT tables are file-scope device arrays (about
- * 18 MB, held by every GPU that loads the library until exit); transforms
- * needing more than 16 MiB of scratch, L > 64 or N > 64 return status 3.
+ * 34 MB, held by every GPU that loads the library until exit); transforms
+ * needing more than 32 MiB of scratch, L > 64 or N > 64 return status 3.
  * The first call on a device builds the tables and waits for them: make it
  * before any stream capture.  Calls share the arrays, so calls whose GPU work
  * overlaps race: serialise them. */
@@ -149,6 +150,11 @@ const char *so3gpu_last_error(void);
 void so3gpu_set_error_mode(int mode);
 /* Number of kernels this library has launched since load (all devices). */
 long long so3gpu_launch_count(void);
+/* Reads and clears the current device's flag that the tensor-core kernels set
+ * when one of their bounded waits gave up (0: none; a nonzero value means the
+ * results of the split-precision calls since the last read are invalid).
+ * Synchronous. */
+int so3gpu_take_kernel_error(void);
 
 #ifdef __cplusplus
 }

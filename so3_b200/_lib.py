@@ -102,6 +102,7 @@ SIGNATURES = {
     "so3gpu_last_error": (ctypes.c_char_p, []),
     "so3gpu_set_error_mode": (None, [_I]),
     "so3gpu_launch_count": (ctypes.c_longlong, []),
+    "so3gpu_take_kernel_error": (ctypes.c_int, []),
 }
 
 _lib = None

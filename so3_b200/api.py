@@ -375,4 +375,10 @@ def launch_count() -> int:
     return _lib.load().so3gpu_launch_count()
 
 
+def take_kernel_error() -> int:
+    """Reads and clears the tensor-core kernels' wait-timeout flag of the
+    current device (0: none)."""
+    return _lib.load().so3gpu_take_kernel_error()
+
+
 __all__ = [n for n in dir() if not n.startswith("_")] + ["SO3Error"]

@@ -553,5 +553,6 @@ int so3gpu_last_status(void) { return t_status; }
 const char* so3gpu_last_error(void) { return so3g::last_error().c_str(); }
 void so3gpu_set_error_mode(int mode) { g_error_mode.store(mode ? 1 : 0); }
 long long so3gpu_launch_count(void) { return so3g::g_launches.load(); }
+int so3gpu_take_kernel_error(void) { return so3g::mixed_take_error(); }
 
 }  // extern "C"

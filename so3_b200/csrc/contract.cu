@@ -115,7 +115,7 @@ struct InvArgs {
   double2* W;
   int L, N, L0, plane0, n_mode, real, sym_n0;
   int nu_lo, nu_hi;  // |n| range [nu_lo, nu_hi) of this launch
-  long long RS, PS;
+  long long CS, QS;  // column-major scratch strides
 };
 
 // ------------------------------------------------------------------ inverse
@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(kThreads, 1) inverse_contract_kernel(InvArgs a
         double2 v = acc[i][j][s];
         if (ms * ns < 0) v = sc(v, odd_mp);
         v = ipow_mul(v, n - m + 4 * L);
-        a.W[(long long)(a.plane0 + n) * a.PS + (long long)mp * a.RS + (m + L - 1)] = v;
+        a.W[(long long)(a.plane0 + n) * a.QS + (long long)(m + L - 1) * a.CS + mp] = v;
       }
     }
   }
@@ -233,7 +233,7 @@ int launch_inverse_contract(const Geometry& g, int n_mode, const double2* flmn, 
                             const double* dl, double2* W, int sym_n0, cudaStream_t s, int nu_lo, int nu_hi) {
   if (nu_hi < 0 || nu_hi > g.N) nu_hi = g.N;
   if (nu_lo >= nu_hi) return kOk;
-  InvArgs a{flmn, bases, dl, W, g.L, g.N, g.L0, g.plane0, n_mode, g.real, sym_n0, nu_lo, nu_hi, g.RS, g.PS};
+  InvArgs a{flmn, bases, dl, W + g.QOFF, g.L, g.N, g.L0, g.plane0, n_mode, g.real, sym_n0, nu_lo, nu_hi, g.CS, g.QS};
   dim3 grid((nu_hi - nu_lo + kNG - 1) / kNG, (g.L + kRows - 1) / kRows, (g.L + kCols - 1) / kCols);
   if (g.real) {
     SO3G_CUDA(cudaFuncSetAttribute(inverse_contract_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));
@@ -255,7 +255,7 @@ struct FwdArgs {
   double2* flmn;
   int L, N, L0, plane0, n_mode, real, compact;
   int nu_lo, nu_hi;  // |n| range [nu_lo, nu_hi) of this launch
-  long long RS, PS;
+  long long CS, QS;  // column-major scratch strides
 };
 
 template <int NSIGN>
@@ -299,13 +299,14 @@ __global__ void __launch_bounds__(kThreads, 1) forward_contract_kernel(FwdArgs a
       cp_async8(&S.A[mc][r][j], src, ok);
     }
     for (int idx = tid; idx < kChunk * kCols * kNG * NSIGN; idx += kThreads) {
-      const int mc = idx / (kCols * kNG * NSIGN), rem = idx - mc * kCols * kNG * NSIGN;
+      // m' fastest: consecutive threads read consecutive entries of a column
+      const int mc = idx % kChunk, rem = idx / kChunk;
       const int col = rem / (kNG * NSIGN), rem2 = rem - col * kNG * NSIGN, j = rem2 / NSIGN, sg = rem2 - j * NSIGN;
       const int mp = mbase + mc, nu = nu0 + j, mu = mu0 + col;
       const bool ok = mp < L && act[j] && mu < L;
       const int n = (sg & 2) ? -nu : nu, m = (sg & 1) ? -mu : mu;
       const double2* src =
-          ok ? a.W + (long long)(a.plane0 + n) * a.PS + (long long)mp * a.RS + (L - 1) + m : a.W;
+          ok ? a.W + (long long)(a.plane0 + n) * a.QS + (long long)(L - 1 + m) * a.CS + mp : a.W;
       cp_async16(&S.H[mc][col][j][sg], src, ok);
     }
   };
@@ -364,7 +365,8 @@ int launch_forward_contract(const Geometry& g, int n_mode, const double2* W, con
                             int nu_hi) {
   if (nu_hi < 0 || nu_hi > g.N) nu_hi = g.N;
   if (nu_lo >= nu_hi) return kOk;
-  FwdArgs a{W, bases, dl, flmn, g.L, g.N, g.L0, g.plane0, n_mode, g.real, storage_compact, nu_lo, nu_hi, g.RS, g.PS};
+  FwdArgs a{W + g.QOFF, bases, dl, flmn, g.L, g.N, g.L0, g.plane0, n_mode, g.real, storage_compact, nu_lo, nu_hi,
+            g.CS, g.QS};
   dim3 grid((nu_hi - nu_lo + kNG - 1) / kNG, (g.L + kRows - 1) / kRows, (g.L + kCols - 1) / kCols);
   if (g.real) {
     SO3G_CUDA(cudaFuncSetAttribute(forward_contract_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));

@@ -1,5 +1,5 @@
-// Split-precision Wigner contractions on the int8 tensor cores (Ozaki
-// scheme), for batches of complex signals.
+// Split-precision Wigner contractions on the 5th-generation tensor cores
+// (tcgen05.mma kind::i8, Ozaki scheme), for batches of complex signals.
 //
 // For fixed |m| = mu, |n| = nu the FP64 contractions of contract.cu are
 // matrix products shared by every signal of a batch:
@@ -12,89 +12,99 @@
 // goes into X, the other is applied to the output.
 //
 // Each operand is scaled by a power of two (A: 2, every column of X: the
-// smallest power of two above twice its largest magnitude) and split into 7
-// int8 slices, r = sum_i q_i 2^{-7i}: the balanced base-128 digits of the
-// 49-bit fixed-point value (q_2..q_7 in [-64, 63], q_1 in [-65, 65]), so that
-// the dropped low-order products carry no common sign.  The 28
-// slice products with i + j <= 8 are accumulated exactly in int32 on
-// mma.sync m16n8k32 (one accumulator per diagonal i + j) and combined in FP64.
-// The dropped products and the 49-bit rounding leave a normwise error near
-// 1e-12 of the contraction, far inside the 1e-10 budget of the split path;
-// Delta, the quadrature weights, the DFT stages and the final combination
-// stay FP64.
+// smallest power of two above twice its largest magnitude), rounded to 49-bit
+// fixed point and cut into 7 balanced base-128 digits q_i in [-64, 64]
+// (offset-binary extraction: the digits of v + sum_i 64*128^i, minus 64), so
+// r = sum_i q_i 2^{-7(i+1)} exactly and the dropped low-order products carry
+// no common sign.  The 28 digit products with i + j <= 6 are accumulated
+// exactly in int32, one accumulator per diagonal d = i + j, and combined in
+// FP64 with weights 2^{-7(d+2)}.  Delta, the quadrature weights, the DFT
+// stages and the final combination stay FP64.
 //
-// A is generated per CTA from the FP64 Delta table (rows of the quarter
-// planes read contiguously through the transpose symmetry
-// Delta^l_{m' k} = (-1)^{m'-k} Delta^l_{k m'}), split in registers and staged
-// in shared memory; X is split once per batch by a slicing kernel.
+// Kernel: one CTA per (pair (mu, nu), 64-row tile of the output index, group
+// of 16 signals).  Tensor-core product D_d[c, r] += Xs_i[c, k] As_j[r, k]
+// with M = 128 signal columns c, N = 64 output rows r, K = the reduction
+// index in chunks of 64 through a 2-stage shared-memory ring.  The 7
+// accumulators live in tensor memory (7 x 64 int32 columns of 128 lanes).
+// Warp roles: warp 0 allocates tensor memory and one of its threads issues
+// the MMAs; warp 1 streams the pre-sliced X chunk of each stage with one bulk
+// copy; warps 2-9 generate the A digits of each stage from the FP64 Delta
+// table and, after the last chunk, read the accumulators back, combine the
+// diagonals in FP64 and store.  X is sliced once per batch by slice_kernel
+// into the exact shared-memory image of a stage.
 #include <cstdint>
 
 #include "so3gpu_internal.h"
+#include "tc_sm100.cuh"
 
 namespace so3g {
 
 namespace {
 
-constexpr int kS = 7;            // slices per operand
-constexpr int kND = kS;          // diagonals i + j = 2 .. kS + 1
-constexpr int kGrp = 8;          // signals per CTA column group
-constexpr int kCol = 8;          // columns per signal
-constexpr int kRowsB = kGrp * kCol;  // 64 B-operand rows per group
-constexpr int kTile = 32;        // CTA rows and K per step
-constexpr int kThreads = 256;
+constexpr int kS = 7;                  // digits per operand
+constexpr int kND = kS;                // diagonals d = i + j = 0 .. 6
+constexpr int kSig = 16;               // signals per group
+constexpr int kCol = 8;                // columns per signal
+constexpr int kM = kSig * kCol;        // 128 MMA rows (signal columns)
+constexpr int kN = 64;                 // MMA columns (output rows of the Wigner index)
+constexpr int kKC = 64;                // reduction entries per stage
+constexpr int kStages = 2;
+constexpr int kXStage = kS * kM * kKC;  // 57344 bytes
+constexpr int kAStage = kS * kN * kKC;  // 28672 bytes
+constexpr int kThreads = 320;           // 10 warps
+constexpr int kGen = 256;               // generator / epilogue threads (warps 2-9)
+constexpr int kTmemCols = 512;
 constexpr double kInv8Pi2 = 0.012665147955292221430803304553147533;  // 1/(8 pi^2)
+constexpr long long kDigitOffset = 283691315109952LL;                 // sum_{i<7} 64 * 128^i
 
-struct MixSmem {
-  uint8_t A[2][kS][kTile][32];    // [buffer][slice][row][k bytes], 16-byte chunks swizzled
-  uint8_t B[2][kS][kRowsB][32];   // [buffer][slice][signal * 8 + column][k bytes]
+// Byte offset of (row, k) inside one digit plane of an operand tile with
+// `rows` rows and kKC reduction bytes: core matrices of 8 rows x 16 bytes,
+// row groups 128 bytes apart, 16-byte k groups rows*16 bytes apart.
+__host__ __device__ constexpr int tile_off(int rows, int row, int k) {
+  return (k >> 4) * (rows * 16) + (row >> 3) * 128 + (row & 7) * 16 + (k & 15);
+}
+
+struct __align__(16) TcSmem {
+  uint8_t X[kStages][kXStage];   // [stage][digit][tile_off(kM, c, k)]
+  uint8_t A[kStages][kAStage];   // [stage][digit][tile_off(kN, r, k)]
+  unsigned long long full[kStages];
+  unsigned long long empty[kStages];
+  unsigned long long accum;
+  uint32_t tmem_base;
 };
 
-__device__ __forceinline__ int swz(int row, int chunk) { return chunk ^ ((row >> 2) & 1); }
+__device__ int g_tc_error;  // bit 1: a wait gave up (see tc::mbar_wait)
 
-// Splits r in [-1/2, 1/2] into 7 balanced digits (see the file comment);
-// q[0] is the most significant.
-__device__ __forceinline__ void split7(double r, int (&q)[kS]) {
-  const double shifter = 6755399441055744.0;                 // 1.5 * 2^52
-  const double y = fma(r, 562949953421312.0, shifter);       // rint(r * 2^49) + shifter
-  const long long v = __double_as_longlong(y) - __double_as_longlong(shifter);
-  const unsigned lo = (unsigned)v;
-  const int hi = (int)(v >> 32);
-  q[6] = lo & 127;
-  q[5] = (lo >> 7) & 127;
-  q[4] = (lo >> 14) & 127;
-  q[3] = (lo >> 21) & 127;
-  q[2] = ((lo >> 28) | ((unsigned)hi << 4)) & 127;
-  q[1] = (hi >> 3) & 127;
-  q[0] = hi >> 10;
-  // balanced digits in [-64, 63] (carry upwards): the dropped low-order
-  // products then have no common sign, so their sum does not grow with K
+// 7 digits of 4 values r in [-1/2, 1/2], packed: byte e of w[i] = digit i of
+// value e (digit 0 most significant).
+__device__ __forceinline__ void split_pack4(const double (&r)[4], uint32_t (&w)[kS]) {
 #pragma unroll
-  for (int i = kS - 1; i > 0; i--) {
-    const int c = q[i] >= 64;
-    q[i] -= c << 7;
-    q[i - 1] += c;
+  for (int i = 0; i < kS; i++) w[i] = 0u;
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    const double shifter = 6755399441055744.0;                  // 1.5 * 2^52
+    const double y = fma(r[e], 562949953421312.0, shifter);     // rint(r * 2^49) + shifter
+    const long long v = __double_as_longlong(y) - __double_as_longlong(shifter);
+    const unsigned long long u = (unsigned long long)(v + kDigitOffset);
+    const uint32_t lo = (uint32_t)u, hi = (uint32_t)(u >> 32);
+    uint32_t d[kS];
+    d[6] = lo & 127u;
+    d[5] = (lo >> 7) & 127u;
+    d[4] = (lo >> 14) & 127u;
+    d[3] = (lo >> 21) & 127u;
+    d[2] = ((lo >> 28) | (hi << 4)) & 127u;
+    d[1] = (hi >> 3) & 127u;
+    d[0] = hi >> 10;  // up to 128
+#pragma unroll
+    for (int i = 0; i < kS; i++) w[i] |= ((d[i] - 64u) & 255u) << (8 * e);
   }
 }
 
-__device__ __forceinline__ void cp16(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
-}
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
-
-__device__ __forceinline__ void ldsm_x4(unsigned (&r)[4], const void* p) {
-  const unsigned a = (unsigned)__cvta_generic_to_shared(p);
-  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-               : "r"(a));
-}
-
-__device__ __forceinline__ void mma_s8(int (&c)[4], const unsigned (&a)[4], unsigned b0, unsigned b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k32.row.col.s32.s8.s8.s32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-      : "+r"(c[0]), "+r"(c[1]), "+r"(c[2]), "+r"(c[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+// Exact int32 -> FP64 on the FP64 pipe: the bits 0x43300000:(x + 2^31) are
+// the double 2^52 + 2^31 + x; one subtraction leaves x.  (The conversion
+// instruction runs on a narrow unit that would otherwise bound the epilogue.)
+__device__ __forceinline__ double int_to_double(int x) {
+  return __hiloint2double(0x43300000, x ^ (int)0x80000000) - 4503601774854144.0;
 }
 
 __device__ __forceinline__ double2 ipow(double2 v, int k) {  // v * i^k
@@ -106,387 +116,399 @@ __device__ __forceinline__ double2 ipow(double2 v, int k) {  // v * i^k
   }
 }
 
-// Stores the 7 slice words of 4 consecutive K entries of A row `row`.
-__device__ __forceinline__ void store_a(MixSmem& S, int buf, int row, int word, const double (&x)[4]) {
-  unsigned w[kS];
-#pragma unroll
-  for (int i = 0; i < kS; i++) w[i] = 0u;
-#pragma unroll
-  for (int e = 0; e < 4; e++) {
-    int q[kS];
-    split7(0.5 * x[e], q);  // A scale 2
-#pragma unroll
-    for (int i = 0; i < kS; i++) w[i] |= (unsigned)(q[i] & 255) << (8 * e);
-  }
-  const int off = row * 32 + swz(row, word >> 2) * 16 + (word & 3) * 4;
-#pragma unroll
-  for (int i = 0; i < kS; i++) *reinterpret_cast<unsigned*>(&S.A[buf][i][0][0] + off) = w[i];
-}
-
-// B tile of one K step: 7 slices x 64 rows x 32 bytes from the sliced
-// operand (layout [slice][row][Lp]).
-__device__ __forceinline__ void load_b(MixSmem& S, int buf, const uint8_t* __restrict__ xs, int Lp, int k0) {
-  for (int idx = threadIdx.x; idx < kS * kRowsB * 2; idx += kThreads) {
-    const int i = idx / (kRowsB * 2), rem = idx - i * kRowsB * 2, row = rem >> 1, chunk = rem & 1;
-    const uint8_t* src = xs + ((size_t)i * kRowsB + row) * Lp + k0 + chunk * 16;
-    cp16(&S.B[buf][i][row][swz(row, chunk) * 16], src);
-  }
-}
-
-// 28 slice products of one K step for a warp tile of 16 rows x 2 signals.
-// B slices 0..3 first, then 4..6 (only A slices 0..2 pair with those), so at
-// most four B fragments are live.
-__device__ __forceinline__ void mma_step(const MixSmem& S, int buf, int msub, int npair, int lane,
-                                         int (&acc)[kND][2][4]) {
-  const int r8 = lane & 7, which = lane >> 3;
-  // B: matrices (sig0, chunk0) (sig0, chunk1) (sig1, chunk0) (sig1, chunk1)
-  const int brow = npair * 16 + (which >> 1) * 8 + r8, bchunk = which & 1;
-  // A: matrices (rows 0-7, chunk0) (rows 8-15, chunk0) (rows 0-7, chunk1) (rows 8-15, chunk1)
-  const int arow = msub * 16 + (which & 1) * 8 + r8, achunk = which >> 1;
-  unsigned b[4][4];
-#pragma unroll
-  for (int j = 0; j < 4; j++) ldsm_x4(b[j], &S.B[buf][j][brow][swz(brow, bchunk) * 16]);
-#pragma unroll
-  for (int i = 0; i < kS; i++) {
-    unsigned a[4];
-    ldsm_x4(a, &S.A[buf][i][arow][swz(arow, achunk) * 16]);
-#pragma unroll
-    for (int j = 0; j < 4 && j < kS - i; j++) {
-      mma_s8(acc[i + j][0], a, b[j][0], b[j][1]);
-      mma_s8(acc[i + j][1], a, b[j][2], b[j][3]);
-    }
-  }
-#pragma unroll
-  for (int j = 4; j < kS; j++) ldsm_x4(b[j - 4], &S.B[buf][j][brow][swz(brow, bchunk) * 16]);
-#pragma unroll
-  for (int i = 0; i < kS - 4; i++) {
-    unsigned a[4];
-    ldsm_x4(a, &S.A[buf][i][arow][swz(arow, achunk) * 16]);
-#pragma unroll
-    for (int j = 4; j < kS - i; j++) {
-      mma_s8(acc[i + j][0], a, b[j - 4][0], b[j - 4][1]);
-      mma_s8(acc[i + j][1], a, b[j - 4][2], b[j - 4][3]);
-    }
-  }
-}
-
-// FP64 value of one accumulator element (A scale 2 folded in).
-__device__ __forceinline__ double combine(const int (&acc)[kND][2][4], int nt, int e) {
-  double v = 0.0, w = 2.0 * 0.000061035156250000000;  // 2 * 2^{-14} (diagonal i + j = 2)
-#pragma unroll
-  for (int d = 0; d < kND; d++) {
-    v = fma((double)acc[d][nt][e], w, v);
-    w *= 0.0078125;  // 2^{-7}
-  }
-  return v;
-}
-
 struct MixArgs {
-  const uint8_t* xs;       // [grp][mu * N + nu][7][64][Lp]
-  const double* xscale;    // [grp][mu * N + nu][64]
+  const uint8_t* xs;       // [grp][pair][chunk][kXStage]
+  const double* xscale;    // [grp][pair][kM]
   const double* dl;        // Delta quarter planes
   const long long* base;   // block bases per plane
-  double2* W;              // inverse: per-signal scratch, signal b at W + b * wstride
+  double2* W;              // inverse: column-major scratch part of signal 0; signal b at W + b * wstride
   double2* const* flmn;    // forward: per-signal coefficient arrays
   long long wstride;
-  int L, N, L0, Lp, MT, plane0, n_mode, nsig, compact;
-  long long RS, PS;
+  int L, N, L0, nchunk, MT, plane0, n_mode, nsig, compact;
+  long long CS, QS;  // column-major scratch strides
 };
 
-__device__ __forceinline__ void decode(const MixArgs& a, int bx, int* mu, int* nu, int* t) {
-  *nu = bx % a.N;
-  const int rest = bx / a.N;
-  *t = rest % a.MT;
-  *mu = rest / a.MT;
-}
-
-// ---------------------------------------------------------------- inverse
-__global__ void __launch_bounds__(kThreads, 2) mixed_inverse_kernel(MixArgs a) {
-  extern __shared__ __align__(128) unsigned char smraw[];
-  MixSmem& S = *reinterpret_cast<MixSmem*>(smraw);
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  int mu, nu, mt;
-  decode(a, blockIdx.x, &mu, &nu, &mt);
-  const int grp = blockIdx.y, L = a.L;
-  const int m0 = mt * kTile;
-  const int lmin = max(max(mu, nu), a.L0);
-  const int kfirst = max(lmin, m0) & ~(kTile - 1);
-  const int nk = kfirst < L ? (L - kfirst + kTile - 1) / kTile : 0;
-  const size_t gp = (size_t)grp * a.L * a.N + (size_t)mu * a.N + nu;  // slicing-kernel order
-  const uint8_t* xs = a.xs + gp * kS * kRowsB * (size_t)a.Lp;
-
-  int acc[kND][2][4];
+// A digits of one stage.  Thread task (row rho = 8*w + lane%8, quad q =
+// 4*it + lane/8, it = 0..3): the 4 reduction entries k0 + 4q .. +3 of row
+// rho; the 32 lanes of a warp store 32 distinct banks.
+//   inverse: row = m' (r0 + rho), reduction = l;  A^T[l, m'] = Delta_{mu m'} Delta_{nu m'} (l >= m', l >= lmin)
+//   forward: row = l  (r0 + rho), reduction = m'; same product
+// Delta_{mu m'} is read as row mu of the quarter plane (the transpose
+// symmetry's sign (-1)^{mu+nu} is applied in the epilogue).
+template <bool FWD>
+__device__ __forceinline__ void gen_load(const MixArgs& a, int mu, int nu, int lmin, int r0, int k0, int gw, int lane,
+                                         double (&x)[4][4]) {
+  const int rho = 8 * gw + (lane & 7);
 #pragma unroll
-  for (int d = 0; d < kND; d++)
-#pragma unroll
-    for (int n = 0; n < 2; n++)
-#pragma unroll
-      for (int e = 0; e < 4; e++) acc[d][n][e] = 0;
-
-  // A generation: thread -> row m' = m0 + 8*(warp%4) + lane%8 and K entries
-  // l = k0 + 4*word .. +3 with word = 4*(warp/4) + lane/8: the Delta loads of a
-  // warp read 8 consecutive m' per plane, and its 32 slice-word stores hit 32
-  // distinct banks.
-  const int grow = 8 * (warp & 3) + (lane & 7), gword = 4 * (warp >> 2) + (lane >> 3), mp = m0 + grow;
-  auto fetch = [&](int k0, double (&x)[4]) {
+  for (int it = 0; it < 4; it++) {
+    const int q = 4 * it + (lane >> 3);
 #pragma unroll
     for (int e = 0; e < 4; e++) {
-      const int l = k0 + 4 * gword + e;
+      const int kk = k0 + 4 * q + e;
+      int l, mp;
+      if (FWD) {
+        l = r0 + rho;
+        mp = kk;
+      } else {
+        l = kk;
+        mp = r0 + rho;
+      }
       double v = 0.0;
-      if (l < L && l >= lmin && mp <= l) {
+      if (l < a.L && l >= lmin && mp <= l) {
         const double* P = a.dl + dl_plane_offset(l);
         v = P[(long long)mu * (l + 1) + mp] * P[(long long)nu * (l + 1) + mp];
       }
-      x[e] = v;
-    }
-  };
-
-  const int msub = warp & 1, npair = warp >> 1;
-  if (nk > 0) {
-    double x[4];
-    fetch(kfirst, x);
-    load_b(S, 0, xs, a.Lp, kfirst);
-    cp_commit();
-    store_a(S, 0, grow, gword, x);
-    for (int k = 0; k < nk; k++) {
-      const int buf = k & 1;
-      cp_wait_all();
-      __syncthreads();
-      const bool more = k + 1 < nk;
-      if (more) {
-        fetch(kfirst + (k + 1) * kTile, x);
-        load_b(S, buf ^ 1, xs, a.Lp, kfirst + (k + 1) * kTile);
-        cp_commit();
-      }
-      mma_step(S, buf, msub, npair, lane, acc);
-      if (more) store_a(S, buf ^ 1, grow, gword, x);
-    }
-  }
-
-  // epilogue: thread holds rows g, g+8 of its 16-row sub-tile, columns 2t
-  // (re) and 2t+1 (im) of sign combination t, for two signals
-  const int g = lane >> 2, t = lane & 3;
-  const int ms = (t & 1) ? -1 : 1, ns = (t & 2) ? -1 : 1;
-  if ((ms < 0 && mu == 0) || (ns < 0 && nu == 0)) return;
-  const int m = ms * mu, n = ns * nu;
-  const bool one_neg = ms * ns < 0;
-  const double sgn_mn = ((mu + nu) & 1) ? -1.0 : 1.0;
-  const double* sc = a.xscale + gp * kRowsB;
-#pragma unroll
-  for (int nt = 0; nt < 2; nt++) {
-    const int b = npair * 2 + nt, sig = grp * kGrp + b;
-    if (sig >= a.nsig) continue;
-    const double sre = sc[b * kCol + 2 * t], sim = sc[b * kCol + 2 * t + 1];
-    double2* W = a.W + (long long)sig * a.wstride + (long long)(a.plane0 + n) * a.PS + (m + L - 1);
-#pragma unroll
-    for (int h = 0; h < 2; h++) {
-      const int row = m0 + msub * 16 + g + 8 * h;
-      if (row >= L) continue;
-      double2 v = make_double2(combine(acc, nt, 2 * h) * sre, combine(acc, nt, 2 * h + 1) * sim);
-      const double s = (one_neg && (row & 1)) ? -sgn_mn : sgn_mn;
-      v = make_double2(v.x * s, v.y * s);
-      W[(long long)row * a.RS] = ipow(v, n - m + 4 * L);
+      x[it][e] = 0.5 * v;  // A scale 2
     }
   }
 }
 
-// ---------------------------------------------------------------- forward
-__global__ void __launch_bounds__(kThreads, 2) mixed_forward_kernel(MixArgs a) {
-  extern __shared__ __align__(128) unsigned char smraw[];
-  MixSmem& S = *reinterpret_cast<MixSmem*>(smraw);
+__device__ __forceinline__ void gen_store(uint8_t* As, int gw, int lane, const double (&x)[4][4]) {
+  const int rho = 8 * gw + (lane & 7);
+#pragma unroll
+  for (int it = 0; it < 4; it++) {
+    const int q = 4 * it + (lane >> 3);
+    uint32_t w[kS];
+    split_pack4(x[it], w);
+    const int off = tile_off(kN, rho, 4 * q);
+#pragma unroll
+    for (int i = 0; i < kS; i++) *reinterpret_cast<uint32_t*>(As + i * (kN * kKC) + off) = w[i];
+  }
+}
+
+template <bool FWD>
+__global__ void __launch_bounds__(kThreads, 1) mixed_tc_kernel(MixArgs a) {
+  extern __shared__ __align__(1024) unsigned char smraw[];
+  TcSmem& S = *reinterpret_cast<TcSmem*>(smraw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  int mu, nu, lt;
-  decode(a, blockIdx.x, &mu, &nu, &lt);
+  const int nu = blockIdx.x % a.N;
+  const int rest = blockIdx.x / a.N;
+  const int t = rest % a.MT, mu = rest / a.MT;  // consecutive CTAs: same mu and tile, all nu
   const int grp = blockIdx.y, L = a.L;
-  const int l0 = lt * kTile;
+  const int r0 = t * kN;
   const int lmin = max(max(mu, nu), a.L0);
-  const bool any_row = l0 + kTile > lmin && l0 < L;
-  const int kend = min(L, l0 + kTile);  // m' < kend (A[m', l] = 0 for m' > l)
-  const int nk = any_row ? (kend + kTile - 1) / kTile : 0;
-  const size_t gp = (size_t)grp * a.L * a.N + (size_t)mu * a.N + nu;
-  const uint8_t* xs = a.xs + gp * kS * kRowsB * (size_t)a.Lp;
+  int kc0, nk;
+  if (FWD) {
+    const bool any_row = r0 + kN > lmin && r0 < L;
+    const int kend = min(L, r0 + kN);  // m' <= l < r0 + 64
+    kc0 = 0;
+    nk = any_row ? (kend + kKC - 1) / kKC : 0;
+  } else {
+    const int kstart = max(lmin, r0) & ~(kKC - 1);
+    kc0 = kstart / kKC;
+    nk = kstart < L ? (L - kstart + kKC - 1) / kKC : 0;
+  }
+  const size_t gp = (size_t)grp * a.L * a.N + (size_t)mu * a.N + nu;  // slicing-kernel order
+  const uint8_t* xs = a.xs + gp * (size_t)a.nchunk * kXStage;
+  // a wait of an earlier CTA gave up: skip the work (the host reports the flag)
+  if (*reinterpret_cast<volatile int*>(&g_tc_error)) return;
 
-  int acc[kND][2][4];
-#pragma unroll
-  for (int d = 0; d < kND; d++)
-#pragma unroll
-    for (int n = 0; n < 2; n++)
-#pragma unroll
-      for (int e = 0; e < 4; e++) acc[d][n][e] = 0;
-
-  // A generation: thread -> row l = l0 + tid/8, K entries m' = k0 + 4*(tid%8) .. +3
-  const int grow = tid >> 3, gword = tid & 7, l = l0 + grow;
-  const bool lrow = l < L && l >= lmin;
-  auto fetch = [&](int k0, double (&x)[4]) {
-    const double* P = a.dl + (lrow ? dl_plane_offset(l) : 0);
-#pragma unroll
-    for (int e = 0; e < 4; e++) {
-      const int mp = k0 + 4 * gword + e;
-      x[e] = (lrow && mp <= l) ? P[(long long)mu * (l + 1) + mp] * P[(long long)nu * (l + 1) + mp] : 0.0;
+  const uint32_t full0 = tc::smem_u32(&S.full[0]), empty0 = tc::smem_u32(&S.empty[0]);
+  const uint32_t accum = tc::smem_u32(&S.accum);
+  if (tid == 0) {
+    for (int s = 0; s < kStages; s++) {
+      tc::mbar_init(full0 + 8 * s, kGen + 1);
+      tc::mbar_init(empty0 + 8 * s, 1);
     }
-  };
+    tc::mbar_init(accum, 1);
+    tc::mbar_fence_init();
+  }
+  if (warp == 0) tc::tmem_alloc(tc::smem_u32(&S.tmem_base), kTmemCols);
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tbase = S.tmem_base;
 
-  const int msub = warp & 1, npair = warp >> 1;
-  if (nk > 0) {
-    double x[4];
-    fetch(0, x);
-    load_b(S, 0, xs, a.Lp, 0);
-    cp_commit();
-    store_a(S, 0, grow, gword, x);
-    for (int k = 0; k < nk; k++) {
-      const int buf = k & 1;
-      cp_wait_all();
-      __syncthreads();
-      const bool more = k + 1 < nk;
-      if (more) {
-        fetch((k + 1) * kTile, x);
-        load_b(S, buf ^ 1, xs, a.Lp, (k + 1) * kTile);
-        cp_commit();
+  if (warp == 0) {
+    // ------------------------------------------------ MMA issue (one thread)
+    if (lane == 0 && nk > 0) {
+      constexpr uint32_t idesc = tc::idesc_s8(kM, kN);
+      for (int k = 0; k < nk; k++) {
+        const int s = k & 1;
+        tc::mbar_wait(full0 + 8 * s, (k >> 1) & 1, &g_tc_error, 2);
+        tc::tc_fence_after();
+        const uint32_t xb = tc::smem_u32(&S.X[s][0]), ab = tc::smem_u32(&S.A[s][0]);
+#pragma unroll
+        for (int ks = 0; ks < kKC / 32; ks++) {
+#pragma unroll
+          for (int i = 0; i < kS; i++) {
+            // X digit i: LBO = 16-byte k groups (kM*16 bytes apart), SBO = 8-row groups (128 bytes)
+            const uint64_t ad = tc::smem_desc(xb + i * (kM * kKC) + ks * 2 * (kM * 16), kM * 16, 128);
+#pragma unroll
+            for (int j = 0; j + i < kND; j++) {
+              const uint64_t bd = tc::smem_desc(ab + j * (kN * kKC) + ks * 2 * (kN * 16), kN * 16, 128);
+              tc::mma_i8(tbase + (uint32_t)(kN * (i + j)), ad, bd, idesc, (k | ks | i) != 0);
+            }
+          }
+        }
+        tc::mma_commit(empty0 + 8 * s);  // stage free once these products have read it
       }
-      mma_step(S, buf, msub, npair, lane, acc);
-      if (more) store_a(S, buf ^ 1, grow, gword, x);
+      tc::mma_commit(accum);
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------ X stream (one thread)
+    if (lane == 0) {
+      for (int k = 0; k < nk; k++) {
+        const int s = k & 1;
+        if (k >= kStages) tc::mbar_wait(empty0 + 8 * s, ((k >> 1) - 1) & 1, &g_tc_error, 2);
+        tc::mbar_arrive_expect_tx(full0 + 8 * s, kXStage);
+        tc::bulk_g2s(tc::smem_u32(&S.X[s][0]), xs + (size_t)(kc0 + k) * kXStage, kXStage, full0 + 8 * s);
+      }
+    }
+  } else {
+    // ------------------------------------------------ A digits, then epilogue
+    const int gw = warp - 2;
+    // the Delta loads of chunk k+1 are in flight while chunk k is split
+    double xa[4][4], xb[4][4];
+    if (nk > 0) gen_load<FWD>(a, mu, nu, lmin, r0, kc0 * kKC, gw, lane, xa);
+    for (int k = 0; k < nk; k += 2) {
+      if (k + 1 < nk) gen_load<FWD>(a, mu, nu, lmin, r0, (kc0 + k + 1) * kKC, gw, lane, xb);
+      if (k >= kStages) tc::mbar_wait(empty0, ((k >> 1) - 1) & 1, &g_tc_error, 2);
+      gen_store(&S.A[0][0], gw, lane, xa);
+      tc::fence_proxy_async_smem();
+      tc::mbar_arrive(full0);
+      if (k + 1 >= nk) break;
+      if (k + 2 < nk) gen_load<FWD>(a, mu, nu, lmin, r0, (kc0 + k + 2) * kKC, gw, lane, xa);
+      if (k + 1 >= kStages) tc::mbar_wait(empty0 + 8, (((k + 1) >> 1) - 1) & 1, &g_tc_error, 2);
+      gen_store(&S.A[1][0], gw, lane, xb);
+      tc::fence_proxy_async_smem();
+      tc::mbar_arrive(full0 + 8);
+    }
+
+    // epilogue: thread <-> TMEM lane c (signal column), 32 output rows
+    const int lq = warp & 3, ch = gw >> 2;
+    const int c = 32 * lq + lane;
+    const int b = c >> 3, combo = (c >> 1) & 3, part = c & 1;
+    const int ms = (combo & 1) ? -1 : 1, ns = (combo & 2) ? -1 : 1;
+    const bool valid_combo = !((ms < 0 && mu == 0) || (ns < 0 && nu == 0));
+    const int m = ms * mu, n = ns * nu;
+    const int sig = grp * kSig + b;
+    const bool one_neg = ms * ns < 0;
+    const double sgn_mn = ((mu + nu) & 1) ? -1.0 : 1.0;
+    const double scale = a.xscale[gp * kM + c];
+    const bool skipped = FWD && plane_skipped(a.n_mode, a.N, n);
+    if (nk > 0) {
+      tc::mbar_wait(accum, 0, &g_tc_error, 2);
+      tc::tc_fence_after();
+    }
+    double2* Wout = nullptr;
+    double2* F = nullptr;
+    long long blk = 0;
+    if (!FWD) Wout = a.W + (long long)sig * a.wstride + (long long)(a.plane0 + n) * a.QS + (long long)(m + L - 1) * a.CS;
+    else if (sig < a.nsig) {
+      F = a.flmn[sig];
+      blk = a.base[a.plane0 + n];
+    }
+#pragma unroll 1
+    for (int g = 0; g < 4; g++) {
+      __syncwarp();  // the tensor-memory loads below are warp-collective
+      const int col = 32 * ch + 8 * g;  // first of the 8 output rows of this group
+      double v[8];
+#pragma unroll
+      for (int e = 0; e < 8; e++) v[e] = 0.0;
+      if (nk > 0) {
+        int acc[kND][8];
+#pragma unroll
+        for (int d = 0; d < kND; d++)
+          tc::tmem_ld8(tbase + ((uint32_t)(32 * lq) << 16) + (uint32_t)(kN * d + col), acc[d]);
+        tc::tmem_wait_ld();
+        double wd = 2.0 * 0.000061035156250000000;  // 2 * 2^{-14}: A scale, diagonal 0
+#pragma unroll
+        for (int d = 0; d < kND; d++) {
+#pragma unroll
+          for (int e = 0; e < 8; e++) v[e] = fma(int_to_double(acc[d][e]), wd, v[e]);
+          wd *= 0.0078125;  // 2^{-7}
+        }
+#pragma unroll
+        for (int e = 0; e < 8; e++) v[e] *= scale;
+      }
+      // lanes c (re) and c^1 (im): the re lane writes rows col..col+3, the im lane col+4..col+7
+      double re[4], im[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const double send = part ? v[q] : v[4 + q];
+        const double recv = __shfl_xor_sync(0xffffffffu, send, 1);
+        re[q] = part ? recv : v[q];
+        im[q] = part ? v[4 + q] : recv;
+      }
+      if (!valid_combo || sig >= a.nsig || skipped) continue;
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int row = r0 + col + 4 * part + q;
+        if (row >= L) continue;
+        const double s = (one_neg && (row & 1)) ? -sgn_mn : sgn_mn;
+        double2 val = make_double2(re[q] * s, im[q] * s);
+        if (!FWD) {
+          Wout[row] = ipow(val, n - m + 4 * L);
+        } else {
+          const int lr = row;
+          if (mu > lr) continue;
+          if (a.compact && lr < nu) continue;  // not stored
+          if (lr < lmin) val = make_double2(0.0, 0.0);
+          else val = ipow(val, m - n + 4 * L);
+          F[blk + (long long)lr * lr + lr + m] = val;
+        }
+      }
     }
   }
 
-  const int g = lane >> 2, t = lane & 3;
-  const int ms = (t & 1) ? -1 : 1, ns = (t & 2) ? -1 : 1;
-  if ((ms < 0 && mu == 0) || (ns < 0 && nu == 0)) return;
-  const int m = ms * mu, n = ns * nu;
-  if (plane_skipped(a.n_mode, a.N, n)) return;  // caller-zeroed blocks stay untouched
-  const bool one_neg = ms * ns < 0;
-  const double sgn_mn = ((mu + nu) & 1) ? -1.0 : 1.0;
-  const double* sc = a.xscale + gp * kRowsB;
-  const long long blk = a.base[a.plane0 + n];
-#pragma unroll
-  for (int nt = 0; nt < 2; nt++) {
-    const int b = npair * 2 + nt, sig = grp * kGrp + b;
-    if (sig >= a.nsig) continue;
-    const double sre = sc[b * kCol + 2 * t], sim = sc[b * kCol + 2 * t + 1];
-    double2* F = a.flmn[sig];
-#pragma unroll
-    for (int h = 0; h < 2; h++) {
-      const int lr = l0 + msub * 16 + g + 8 * h;
-      if (lr >= L || mu > lr) continue;
-      if (a.compact && lr < nu) continue;  // not stored
-      double2 v = make_double2(0.0, 0.0);
-      if (lr >= lmin) {
-        v = make_double2(combine(acc, nt, 2 * h) * sre, combine(acc, nt, 2 * h + 1) * sim);
-        const double s = (one_neg && (lr & 1)) ? -sgn_mn : sgn_mn;
-        v = ipow(make_double2(v.x * s, v.y * s), m - n + 4 * L);
-      }
-      F[blk + (long long)lr * lr + lr + m] = v;
-    }
+  // the products have completed before tensor memory is released (immediate
+  // in the normal case: the epilogue waited for the same commit)
+  if (warp == 0 && lane == 0 && nk > 0) tc::mbar_wait(accum, 0, &g_tc_error, 2);
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    __syncwarp();
+    tc::tc_fence_after();
+    tc::tmem_dealloc(tbase, kTmemCols);
   }
 }
 
 // ---------------------------------------------------------------- slicing
-// One warp per (pair mu * N + nu, signal): column scales over the reduction index, then
-// the 7 slices of the 8 columns.  Inverse: X[l, c] from the coefficients;
-// forward: X'[m', c] from the scratch planes.
+// One CTA per (pair mu * N + nu, group of 16 signals).  Thread -> signal
+// column c = tid % 128 and every other 16-entry block of the reduction index:
+// pass 1 finds the column's largest magnitude, pass 2 writes the 7 digit
+// planes of 16 entries with one 16-byte store each, in the shared-memory
+// image of the tensor-core kernel's stages.
+//   inverse: X[l, c]   = (2l+1)/(8 pi^2) f_{l m n} (times (-1)^l for one negative index)
+//   forward: X'[m', c] = W[n][m'][m]              (times (-1)^{m'} for one negative index)
 struct SliceArgs {
   uint8_t* xs;
   double* xscale;
   const double2* const* flmn;  // inverse input, per signal
-  const double2* W;            // forward input, signal b at W + b * wstride
+  const double2* W;            // forward input: column-major scratch part of signal 0, signal b at W + b * wstride
   const long long* base;
   long long wstride;
-  int L, N, L0, Lp, MT, plane0, n_mode, nsig, npairs;
-  long long RS, PS;
+  int L, N, L0, nchunk, plane0, n_mode, nsig, npairs;
+  long long CS, QS;
+};
+
+// Column c of one pair: the source pointer and the stride between
+// consecutive reduction entries (inverse: l^2 + l + m grows by 2l + 2),
+// resolved once per thread.
+struct Column {
+  const double* src;  // real or imaginary part of entry k = 0 (inverse: of l = 0)
+  bool active, flip_odd;
+  int kmin;
 };
 
 template <bool FWD>
-__device__ __forceinline__ void column_values(const SliceArgs& a, int sig, int mu, int nu, int k, double (&v)[kCol]) {
-  const int lmin = max(max(mu, nu), a.L0);
+__device__ __forceinline__ Column column_of(const SliceArgs& a, int sig, int mu, int nu, int combo, int part) {
+  Column col{nullptr, false, false, 0};
+  const int ms = (combo & 1) ? -1 : 1, ns = (combo & 2) ? -1 : 1;
+  if (sig >= a.nsig || (ms < 0 && mu == 0) || (ns < 0 && nu == 0)) return col;
+  const int m = ms * mu, n = ns * nu;
+  if (plane_skipped(a.n_mode, a.N, n)) return col;
+  col.active = true;
+  col.flip_odd = ms * ns < 0;
+  if (!FWD) {
+    col.kmin = max(max(mu, nu), a.L0);
+    col.src = reinterpret_cast<const double*>(a.flmn[sig] + a.base[a.plane0 + n] + m) + part;
+  } else {
+    col.src = reinterpret_cast<const double*>(a.W + (long long)sig * a.wstride + (long long)(a.plane0 + n) * a.QS +
+                                              (long long)(m + a.L - 1) * a.CS) + part;
+  }
+  return col;
+}
+
+// The 16 entries k0 .. k0+15 of a column (zero outside the band limit).
+template <bool FWD>
+__device__ __forceinline__ void column_block(const SliceArgs& a, const Column& col, int k0, double (&v)[16]) {
 #pragma unroll
-  for (int s = 0; s < 4; s++) {
-    const int ms = (s & 1) ? -1 : 1, ns = (s & 2) ? -1 : 1;
-    double2 x = make_double2(0.0, 0.0);
-    const bool combo = !(ms < 0 && mu == 0) && !(ns < 0 && nu == 0);
-    const int m = ms * mu, n = ns * nu;
-    if (sig < a.nsig && combo && k < a.L && !plane_skipped(a.n_mode, a.N, n)) {
-      const bool one_neg = ms * ns < 0;
-      if (!FWD) {
-        if (k >= lmin) {
-          x = a.flmn[sig][a.base[a.plane0 + n] + (long long)k * k + k + m];
-          double f = (2.0 * k + 1.0) * kInv8Pi2;
-          if (one_neg && (k & 1)) f = -f;
-          x = make_double2(x.x * f, x.y * f);
-        }
-      } else {
-        x = a.W[(long long)sig * a.wstride + (long long)(a.plane0 + n) * a.PS + (long long)k * a.RS + (m + a.L - 1)];
-        if (one_neg && (k & 1)) x = make_double2(-x.x, -x.y);
-      }
+  for (int e = 0; e < 16; e++) {
+    const int k = k0 + e;
+    double x = 0.0;
+    if (col.active && k < a.L && k >= col.kmin) {
+      if (!FWD) x = __ldg(col.src + 2LL * ((long long)k * k + k)) * ((2.0 * k + 1.0) * kInv8Pi2);
+      else x = __ldg(col.src + 2LL * k);
+      if (col.flip_odd && (k & 1)) x = -x;
     }
-    v[2 * s] = x.x;
-    v[2 * s + 1] = x.y;
+    v[e] = x;
   }
 }
 
 template <bool FWD>
 __global__ void __launch_bounds__(256) slice_kernel(SliceArgs a) {
-  const int lane = threadIdx.x & 31, b = threadIdx.x >> 5;  // 8 warps = 8 signals of the group
-  const int pair = blockIdx.x, grp = blockIdx.y, sig = grp * kGrp + b;
+  __shared__ double colmax[2][kM];
+  const int c = threadIdx.x & (kM - 1), half = threadIdx.x >> 7;
+  const int pair = blockIdx.x, grp = blockIdx.y;
   const int nu = pair % a.N, mu = pair / a.N;
+  const int b = c >> 3, combo = (c >> 1) & 3, part = c & 1, sig = grp * kSig + b;
   const size_t gp = (size_t)grp * a.npairs + pair;
-  double mx[kCol];
+  const int nblk = a.nchunk * (kKC / 16);
+  const Column col = column_of<FWD>(a, sig, mu, nu, combo, part);
+  double mx = 0.0;
+  for (int kb = half; kb < nblk; kb += 2) {
+    double v[16];
+    column_block<FWD>(a, col, 16 * kb, v);
 #pragma unroll
-  for (int c = 0; c < kCol; c++) mx[c] = 0.0;
-  for (int k = lane; k < a.Lp; k += 32) {
-    double v[kCol];
-    column_values<FWD>(a, sig, mu, nu, k, v);
-#pragma unroll
-    for (int c = 0; c < kCol; c++) mx[c] = fmax(mx[c], fabs(v[c]));
+    for (int e = 0; e < 16; e++) mx = fmax(mx, fabs(v[e]));
   }
-  double scale[kCol];
+  colmax[half][c] = mx;
+  __syncthreads();
+  mx = fmax(colmax[0][c], colmax[1][c]);
+  int ex = 0;
+  frexp(mx, &ex);
+  const double scale = mx > 0.0 ? ldexp(1.0, ex + 1) : 1.0;  // |x / scale| < 1/2
+  const double inv = 1.0 / scale;                              // exact (power of two)
+  if (half == 0) a.xscale[gp * kM + c] = scale;
+  uint8_t* out = a.xs + gp * (size_t)a.nchunk * kXStage;
+  for (int kb = half; kb < nblk; kb += 2) {
+    double v[16];
+    column_block<FWD>(a, col, 16 * kb, v);
+    uint32_t w[4][kS];
 #pragma unroll
-  for (int c = 0; c < kCol; c++) {
-    double m = mx[c];
+    for (int qd = 0; qd < 4; qd++) {
+      double r[4];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    int e = 0;
-    frexp(m, &e);
-    scale[c] = m > 0.0 ? ldexp(1.0, e + 1) : 1.0;  // |x / scale| < 1/2
-    if (lane == 0) a.xscale[gp * kRowsB + b * kCol + c] = scale[c];
-  }
-  uint8_t* out = a.xs + gp * kS * kRowsB * (size_t)a.Lp;
-  for (int k = lane; k < a.Lp; k += 32) {
-    double v[kCol];
-    column_values<FWD>(a, sig, mu, nu, k, v);
-#pragma unroll
-    for (int c = 0; c < kCol; c++) {
-      int q[kS];
-      split7(v[c] / scale[c], q);
-#pragma unroll
-      for (int i = 0; i < kS; i++) out[((size_t)i * kRowsB + b * kCol + c) * a.Lp + k] = (uint8_t)(q[i] & 255);
+      for (int e = 0; e < 4; e++) r[e] = v[4 * qd + e] * inv;
+      split_pack4(r, w[qd]);
     }
+    const int chunk = kb >> 2, kin = (kb & 3) * 16;
+    uint8_t* dst = out + (size_t)chunk * kXStage + tile_off(kM, c, kin);
+#pragma unroll
+    for (int i = 0; i < kS; i++)
+      *reinterpret_cast<uint4*>(dst + i * (kM * kKC)) = make_uint4(w[0][i], w[1][i], w[2][i], w[3][i]);
   }
 }
 
 }  // namespace
 
 // ---------------------------------------------------------------- host side
+static int nchunks(const Geometry& g) { return (g.L + kKC - 1) / kKC; }
+
 size_t mixed_scratch_bytes(const Geometry& g, int nsig) {
-  const int Lp = (g.L + kTile - 1) / kTile * kTile;
-  const size_t groups = (nsig + kGrp - 1) / kGrp, pairs = (size_t)g.L * g.N;
-  return groups * pairs * (kS * kRowsB * (size_t)Lp + kRowsB * sizeof(double)) + 256;
+  const size_t groups = (nsig + kSig - 1) / kSig, pairs = (size_t)g.L * g.N;
+  return groups * pairs * ((size_t)nchunks(g) * kXStage + kM * sizeof(double)) + 256;
 }
 
 static int mixed_args(const Geometry& g, int n_mode, int nsig, void* scratch, MixArgs* m, SliceArgs* s) {
-  const int Lp = (g.L + kTile - 1) / kTile * kTile, MT = Lp / kTile;
-  const size_t groups = (nsig + kGrp - 1) / kGrp, pairs = (size_t)g.L * g.N;
-  if (pairs * MT > 0x7fffffffu) return fail(kUnsupported, "split-precision grid too large");
+  const int nc = nchunks(g), MT = nc;  // output tiles of 64 rows = reduction chunks of 64
+  const size_t groups = (nsig + kSig - 1) / kSig, pairs = (size_t)g.L * g.N;
+  if (pairs * MT > 0x7fffffffu || groups > 65535) return fail(kUnsupported, "split-precision grid too large");
   uint8_t* xs = static_cast<uint8_t*>(scratch);
-  double* xscale = reinterpret_cast<double*>(xs + ((groups * pairs * kS * kRowsB * (size_t)Lp + 255) & ~size_t(255)));
+  double* xscale = reinterpret_cast<double*>(xs + ((groups * pairs * nc * (size_t)kXStage + 255) & ~size_t(255)));
   *m = MixArgs{};
   m->xs = xs;
   m->xscale = xscale;
-  m->L = g.L, m->N = g.N, m->L0 = g.L0, m->Lp = Lp, m->MT = MT, m->plane0 = g.plane0, m->n_mode = n_mode;
-  m->nsig = nsig, m->RS = g.RS, m->PS = g.PS;
+  m->L = g.L, m->N = g.N, m->L0 = g.L0, m->nchunk = nc, m->MT = MT, m->plane0 = g.plane0, m->n_mode = n_mode;
+  m->nsig = nsig, m->CS = g.CS, m->QS = g.QS;
   *s = SliceArgs{};
   s->xs = xs;
   s->xscale = xscale;
-  s->L = g.L, s->N = g.N, s->L0 = g.L0, s->Lp = Lp, s->MT = MT, s->plane0 = g.plane0, s->n_mode = n_mode;
-  s->nsig = nsig, s->npairs = (int)pairs, s->RS = g.RS, s->PS = g.PS;
+  s->L = g.L, s->N = g.N, s->L0 = g.L0, s->nchunk = nc, s->plane0 = g.plane0, s->n_mode = n_mode;
+  s->nsig = nsig, s->npairs = (int)pairs, s->CS = g.CS, s->QS = g.QS;
+  return kOk;
+}
+
+template <bool FWD>
+static int launch_tc(const MixArgs& m, int nsig, cudaStream_t s) {
+  const dim3 grid((unsigned)(m.L * m.N * m.MT), (nsig + kSig - 1) / kSig);
+  const int smem = (int)sizeof(TcSmem);
+  SO3G_CUDA(cudaFuncSetAttribute(mixed_tc_kernel<FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  mixed_tc_kernel<FWD><<<grid, kThreads, smem, s>>>(m);
+  SO3G_LAUNCHED();
+  SO3G_CUDA(cudaGetLastError());
   return kOk;
 }
 
@@ -499,20 +521,14 @@ int launch_mixed_inverse(const Geometry& g, int n_mode, const double2* const* fl
   if (int rc = mixed_args(g, n_mode, nsig, scratch, &m, &sa)) return rc;
   sa.flmn = flmn_dev;
   sa.base = bases;
-  const dim3 sgrid((unsigned)sa.npairs, (nsig + kGrp - 1) / kGrp);
-  const dim3 grid((unsigned)(sa.npairs * sa.MT), (nsig + kGrp - 1) / kGrp);
-  slice_kernel<false><<<sgrid, 256, 0, s>>>(sa);
+  slice_kernel<false><<<dim3((unsigned)sa.npairs, (nsig + kSig - 1) / kSig), 256, 0, s>>>(sa);
   SO3G_LAUNCHED();
   SO3G_CUDA(cudaGetLastError());
   m.dl = dl;
   m.base = bases;
-  m.W = W;
+  m.W = W + g.QOFF;
   m.wstride = wstride;
-  SO3G_CUDA(cudaFuncSetAttribute(mixed_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MixSmem)));
-  mixed_inverse_kernel<<<grid, kThreads, sizeof(MixSmem), s>>>(m);
-  SO3G_LAUNCHED();
-  SO3G_CUDA(cudaGetLastError());
-  return kOk;
+  return launch_tc<false>(m, nsig, s);
 }
 
 int launch_mixed_forward(const Geometry& g, int n_mode, const double2* W, long long wstride, int nsig,
@@ -522,23 +538,25 @@ int launch_mixed_forward(const Geometry& g, int n_mode, const double2* W, long l
   MixArgs m;
   SliceArgs sa;
   if (int rc = mixed_args(g, n_mode, nsig, scratch, &m, &sa)) return rc;
-  sa.W = W;
+  sa.W = W + g.QOFF;
   sa.wstride = wstride;
   sa.base = bases;
-  const dim3 sgrid((unsigned)sa.npairs, (nsig + kGrp - 1) / kGrp);
-  const dim3 grid((unsigned)(sa.npairs * sa.MT), (nsig + kGrp - 1) / kGrp);
-  slice_kernel<true><<<sgrid, 256, 0, s>>>(sa);
+  slice_kernel<true><<<dim3((unsigned)sa.npairs, (nsig + kSig - 1) / kSig), 256, 0, s>>>(sa);
   SO3G_LAUNCHED();
   SO3G_CUDA(cudaGetLastError());
   m.dl = dl;
   m.base = bases;
   m.flmn = flmn_dev;
   m.compact = storage_compact;
-  SO3G_CUDA(cudaFuncSetAttribute(mixed_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MixSmem)));
-  mixed_forward_kernel<<<grid, kThreads, sizeof(MixSmem), s>>>(m);
-  SO3G_LAUNCHED();
-  SO3G_CUDA(cudaGetLastError());
-  return kOk;
+  return launch_tc<true>(m, nsig, s);
+}
+
+// Reads and clears the tensor-core kernels' wait-timeout flag (0: none).
+int mixed_take_error() {
+  int v = 0, zero = 0;
+  if (cudaMemcpyFromSymbol(&v, g_tc_error, sizeof(int)) != cudaSuccess) return -1;
+  if (v) cudaMemcpyToSymbol(g_tc_error, &zero, sizeof(int));
+  return v;
 }
 
 }  // namespace so3g

@@ -8,7 +8,7 @@
 // in the file-scope device arrays below, which every GPU that loads the
 // library holds until the process exits.
 //
-// Limits: transform scratch of at most kScratchBytes (16 MiB; for example
+// Limits: transform scratch of at most kScratchBytes (32 MiB; for example
 // MW sampling with L <= 64 and N <= 64), L <= kMaxL, N <= kMaxN.  Larger
 // requests are rejected with status 3 and a message.
 //
@@ -37,7 +37,7 @@
 namespace so3g {
 namespace {
 
-constexpr size_t kScratchBytes = 16u << 20;
+constexpr size_t kScratchBytes = 32u << 20;
 constexpr int kMaxL = 64;
 constexpr int kMaxN = 64;
 constexpr int kDlEntries = kMaxL * (kMaxL + 1) * (2 * kMaxL + 1) / 6;
@@ -173,7 +173,7 @@ int run(void* f, const void* flmn, const so3_parameters_t* p, cudaStream_t s) {
   if (p->L > kMaxL || p->N > kMaxN)
     return fail(kUnsupported, "so3gpu_inverse_noalloc: L <= 64 and N <= 64 only");
   if (workspace_bytes(*p, 0) > kScratchBytes)
-    return fail(kUnsupported, "so3gpu_inverse_noalloc: transform scratch exceeds the 16 MiB static array");
+    return fail(kUnsupported, "so3gpu_inverse_noalloc: transform scratch exceeds the 32 MiB static array");
   int dev = 0;
   SO3G_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return fail(kUnsupported, "device ordinal out of range");

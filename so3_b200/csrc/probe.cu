@@ -1,10 +1,11 @@
 // Throughput probes: the denominators the contraction kernels are reported
 // against (the measured peaks file of this pool carries HBM and BF16 figures
 // only).  FP64: each thread runs 8 independent FMA chains in registers.
-// int8 tensor cores: each warp runs 8 independent mma.sync m16n8k32 s8
-// accumulator chains on register operands (the instruction the split-precision
-// contractions issue).
+// int8 tensor cores: back-to-back tcgen05.mma kind::i8 products from shared
+// memory into tensor memory (the instruction the split-precision contractions
+// issue).
 #include "so3gpu_internal.h"
+#include "tc_sm100.cuh"
 
 namespace so3g {
 
@@ -22,40 +23,67 @@ __global__ void fp64_fma_chain(double* out, int iters, double a, double b) {
   if (s == 12345.678) out[0] = s;  // keeps the chains live
 }
 
-__global__ void int8_mma_chain(int* out, int iters) {
-  const unsigned a0 = threadIdx.x * 0x01010101u, a1 = a0 ^ 0x5a5a5a5au, a2 = a0 + 3u, a3 = a0 * 7u;
-  const unsigned b0 = a0 ^ 0x33333333u, b1 = a0 + 11u;
-  int c[8][4] = {};
-  for (int it = 0; it < iters; it++) {
-#pragma unroll
-    for (int j = 0; j < 8; j++)
-      asm volatile(
-          "mma.sync.aligned.m16n8k32.row.col.s32.s8.s8.s32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-          : "+r"(c[j][0]), "+r"(c[j][1]), "+r"(c[j][2]), "+r"(c[j][3])
-          : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+// One CTA per SM; one thread issues tcgen05.mma kind::i8 M=128 N=256 K=32
+// products from shared memory into two tensor-memory accumulators, 64 per
+// batch, with at most two batches in flight (commit to alternating
+// mbarriers).  Operand contents do not matter (zeros).
+__global__ void __launch_bounds__(128, 1) int8_tc_chain(int iters, int* flag) {
+  __shared__ __align__(1024) uint8_t sa[128 * 32];
+  __shared__ __align__(1024) uint8_t sb[256 * 32];
+  __shared__ unsigned long long bar[2];
+  __shared__ uint32_t slot;
+  for (int i = threadIdx.x; i < 128 * 32 / 4; i += blockDim.x) reinterpret_cast<uint32_t*>(sa)[i] = 0u;
+  for (int i = threadIdx.x; i < 256 * 32 / 4; i += blockDim.x) reinterpret_cast<uint32_t*>(sb)[i] = 0u;
+  tc::fence_proxy_async_smem();
+  const uint32_t b0 = tc::smem_u32(&bar[0]);
+  if (threadIdx.x == 0) {
+    tc::mbar_init(b0, 1);
+    tc::mbar_init(b0 + 8, 1);
+    tc::mbar_fence_init();
   }
-  int s = 0;
-#pragma unroll
-  for (int j = 0; j < 8; j++) s += c[j][0] + c[j][1] + c[j][2] + c[j][3];
-  if (s == 0x7fffffff) out[0] = s;  // keeps the chains live
+  if (threadIdx.x < 32) tc::tmem_alloc(tc::smem_u32(&slot), 512);
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tbase = slot;
+  if (threadIdx.x == 0) {
+    constexpr uint32_t idesc = tc::idesc_s8(128, 256);
+    const uint64_t ad = tc::smem_desc(tc::smem_u32(sa), 128 * 16, 128);
+    const uint64_t bd = tc::smem_desc(tc::smem_u32(sb), 256 * 16, 128);
+    for (int it = 0; it < iters; it++) {
+#pragma unroll 8
+      for (int j = 0; j < 64; j++) tc::mma_i8(tbase + 256u * (j & 1), ad, bd, idesc, 1u);
+      tc::mma_commit(b0 + 8 * (it & 1));
+      if (it >= 1) tc::mbar_wait(b0 + 8 * ((it - 1) & 1), ((it - 1) >> 1) & 1, flag, 1);
+    }
+    tc::mbar_wait(b0 + 8 * ((iters - 1) & 1), ((iters - 1) >> 1) & 1, flag, 1);
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    __syncwarp();
+    tc::tc_fence_after();
+    tc::tmem_dealloc(tbase, 512);
+  }
 }
 
 int measure_int8_mma_rate(double* tops) {
   int dev = 0, sms = 0;
   SO3G_CUDA(cudaGetDevice(&dev));
   SO3G_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  int* out = nullptr;
-  SO3G_CUDA(cudaMalloc(&out, sizeof(int)));
+  int* flag = nullptr;
+  SO3G_CUDA(cudaMalloc(&flag, sizeof(int)));
+  SO3G_CUDA(cudaMemset(flag, 0, sizeof(int)));
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  const int blocks = sms * 4, threads = 256, iters = 2048;
-  int8_mma_chain<<<blocks, threads>>>(out, iters);  // warm-up
+  const int blocks = sms, iters = 256;
+  int8_tc_chain<<<blocks, 128>>>(iters, flag);  // warm-up
   SO3G_LAUNCHED();
   float best = 1e30f;
   for (int r = 0; r < 5; r++) {
     cudaEventRecord(e0);
-    int8_mma_chain<<<blocks, threads>>>(out, iters);
+    int8_tc_chain<<<blocks, 128>>>(iters, flag);
     SO3G_LAUNCHED();
     cudaEventRecord(e1);
     cudaEventSynchronize(e1);
@@ -63,11 +91,14 @@ int measure_int8_mma_rate(double* tops) {
     cudaEventElapsedTime(&ms, e0, e1);
     if (ms < best) best = ms;
   }
+  int h = 0;
+  cudaMemcpy(&h, flag, sizeof(int), cudaMemcpyDeviceToHost);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  cudaFree(out);
+  cudaFree(flag);
   SO3G_CUDA(cudaGetLastError());
-  const double ops = 2.0 * 16 * 8 * 32 * 8.0 * iters * (double)blocks * (threads / 32);
+  if (h) return fail(kCudaError, "int8 tensor-core probe: a wait timed out");
+  const double ops = 2.0 * 128 * 256 * 32 * 64.0 * iters * (double)blocks;
   *tops = ops / (best * 1e-3) / 1e12;
   return kOk;
 }

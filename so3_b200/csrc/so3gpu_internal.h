@@ -39,10 +39,18 @@ extern std::atomic<long long> g_launches;
 #define SO3G_LAUNCHED() (::so3g::g_launches.fetch_add(1, std::memory_order_relaxed))
 
 // ---------------------------------------------------------------- geometry
-// Scratch layout: W[plane][row][col], complex FP64, col stride 1, row stride
-// RS (>= 2L, multiple of 8 so every row starts on a 128-byte boundary), plane
-// stride PS = RS * nb.  Plane index = n + plane0 (plane0 = N-1 for complex
-// signals, 0 for real ones, which keep n >= 0 only).  Column index c = m+L-1.
+// Scratch of one transform, two parts, complex FP64.  Plane index = n +
+// plane0 (plane0 = N-1 for complex signals, 0 for real ones, which keep
+// n >= 0 only); column index c = m + L - 1.
+//  * row-major part W[plane][row][col] at the workspace start: col stride 1,
+//    row stride RS (>= 2L, multiple of 8 so every row starts on a 128-byte
+//    boundary), plane stride PS = RS * nb.  Rows are beta samples (after the
+//    beta stage) and the alpha / gamma stages work on it.
+//  * column-major part Wc[plane][col][m'] at offset QOFF = nplanes * PS:
+//    m' stride 1, column stride CS (>= L, multiple of 8), plane stride QS =
+//    CS * (2L - 1).  It holds the beta-Fourier spectra F(n, m', m) between a
+//    contraction and a beta stage, so that both read and write whole columns
+//    contiguously; the beta stages transpose between the two parts.
 struct Geometry {
   int L, N, L0;
   int mw;       // 1 MW, 0 MWSS
@@ -53,6 +61,7 @@ struct Geometry {
   int nplanes;  // 2N-1 (complex) or N (real)
   int plane0;
   long RS, PS;
+  long CS, QS, QOFF;  // column-major part (see above)
   int Pc;       // weight-convolution length (power of two >= 4L-3)
   // Kernel variant of each DFT stage (index = Stage below; 0 = default),
   // chosen by the autotuner for this geometry.
@@ -200,6 +209,9 @@ int launch_mixed_inverse(const Geometry& g, int n_mode, const double2* const* fl
 int launch_mixed_forward(const Geometry& g, int n_mode, const double2* W, long long wstride, int nsig,
                          const long long* bases, const double* dl, double2* const* flmn_dev, int storage_compact,
                          void* scratch, cudaStream_t s);
+// Reads and clears the flag the tensor-core kernels set when a bounded wait
+// gave up (0: none; synchronous).
+int mixed_take_error();
 
 // ---------------------------------------------------------------- drivers
 // Contraction arithmetic of a batch: FP64 (the reference-exact path) or the

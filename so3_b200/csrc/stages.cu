@@ -129,12 +129,13 @@ __global__ void __launch_bounds__(E::NT, E::MINB) inv_beta_kernel(Geometry g, Ff
   double2* b = sm + (size_t)T * ld;
   const int plane = blockIdx.y, n = plane - g.plane0;
   const int c0 = blockIdx.x * T, ncols = 2 * g.L - 1, L = g.L, Pn = g.P;
-  double2* base = W + (long long)plane * g.PS;
+  double2* base = W + (long long)plane * g.PS;                        // row-major output
+  const double2* cbase = W + g.QOFF + (long long)plane * g.QS;        // column-major input
   if (!g.mw)
     for (int t = threadIdx.x; t < T; t += E::NT) a[t * ld + E::at(L)] = make_double2(0.0, 0.0);
   for (int idx = threadIdx.x; idx < L * T; idx += E::NT) {
-    const int t = idx % T, mp = idx / T, c = c0 + t;
-    double2 v = c < ncols ? base[(long long)mp * g.RS + c] : make_double2(0.0, 0.0);
+    const int mp = idx % L, t = idx / L, c = c0 + t;  // m' fastest: whole columns read contiguously
+    double2 v = c < ncols ? cbase[(long long)c * g.CS + mp] : make_double2(0.0, 0.0);
     const int m = c - (L - 1);
     const double sg = ((m + n) & 1) ? -1.0 : 1.0;
     double2 xp = v, xn = make_double2(sg * v.x, sg * v.y);
@@ -334,8 +335,9 @@ __global__ void __launch_bounds__(E::NT, E::MINB) fwd_beta_conv_kernel(Geometry 
   __syncthreads();
   double2* q2 = (q == a) ? b : a;
   double2* G = E::runC(q, q2, T, ld, Pc);
+  double2* cbase = W + g.QOFF + (long long)plane * g.QS;  // column-major output
   for (int idx = threadIdx.x; idx < L * T; idx += E::NT) {
-    const int t = idx % T, mp = idx / T, c = c0 + t;
+    const int mp = idx % L, t = idx / L, c = c0 + t;  // m' fastest: whole columns written contiguously
     if (c >= ncols) continue;
     const int m = c - (L - 1);
     const double sg = ((m + n) & 1) ? -1.0 : 1.0;
@@ -344,7 +346,7 @@ __global__ void __launch_bounds__(E::NT, E::MINB) fwd_beta_conv_kernel(Geometry 
       const double2 u = G[t * ld + E::atC(pc - mp)];
       v = make_double2(v.x + sg * u.x, v.y + sg * u.y);
     }
-    base[(long long)mp * g.RS + c] = v;
+    cbase[(long long)c * g.CS + mp] = v;
   }
 }
 

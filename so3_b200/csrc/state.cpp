@@ -37,6 +37,9 @@ Geometry make_geometry(const so3_parameters_t& p, int real) {
   g.plane0 = real ? 0 : p.N - 1;
   g.RS = ((2L * p.L + 7) / 8) * 8;
   g.PS = g.RS * g.nb;
+  g.CS = ((long)p.L + 7) / 8 * 8;
+  g.QS = g.CS * (2L * p.L - 1);
+  g.QOFF = (long)g.nplanes * g.PS;
   int pc = 1;
   while (pc < 4 * p.L - 3) pc <<= 1;
   g.Pc = pc;
@@ -45,7 +48,7 @@ Geometry make_geometry(const so3_parameters_t& p, int real) {
 
 size_t workspace_bytes(const so3_parameters_t& p, int real) {
   Geometry g = make_geometry(p, real);
-  return (size_t)g.nplanes * (size_t)g.PS * sizeof(double2);
+  return (size_t)g.nplanes * (size_t)(g.PS + g.QS) * sizeof(double2);
 }
 
 static long long base_negfirst(long long n, long long L, long long N, int compact) {

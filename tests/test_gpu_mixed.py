@@ -1,5 +1,5 @@
-"""Split-precision batch path: int8 tensor-core contractions (7-slice Ozaki
-split) against the FP64 path on the same inputs.  Tolerance: normwise
+"""Split-precision batch path: int8 tensor-core contractions (tcgen05, 7-digit
+Ozaki split) against the FP64 path on the same inputs.  Tolerance: normwise
 relative error 1e-10 (the split path's contract); measured values sit near
 1e-12.  The FP64 path itself is pinned to the oracle by test_gpu_parity."""
 import numpy as np
@@ -12,6 +12,12 @@ from tests.helpers import params, rel_err
 pytestmark = pytest.mark.gpu
 
 TOL_MIXED = 1e-10
+
+
+@pytest.fixture(autouse=True)
+def _no_kernel_timeouts():
+    yield
+    assert so3.take_kernel_error() == 0  # no bounded wait of the tensor-core kernels gave up
 
 
 def _run(p, nsig, seed, dist="uniform"):
@@ -30,7 +36,8 @@ def _run(p, nsig, seed, dist="uniform"):
 
 CASES = [
     dict(L=32, N=8, nsig=3),
-    dict(L=24, N=5, nsig=9, order=0, storage=1, L0=2),  # two signal groups, compact, zero-first
+    dict(L=24, N=5, nsig=9, order=0, storage=1, L0=2),  # compact, zero-first, L0 > 0
+    dict(L=70, N=3, nsig=18),                           # two groups of 16 signals, L past a 64-row tile
     dict(L=20, N=6, nsig=4, mode=1),                    # even n only
     dict(L=20, N=6, nsig=2, mode=3),                    # |n| = N-1 only
     dict(L=20, N=6, nsig=2, mode=4),                    # l = |n| only

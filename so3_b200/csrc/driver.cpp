@@ -395,9 +395,11 @@ int run_inverse_batch(Device* D, Workspace* wk, const so3_parameters_t& p, int r
   cudaEvent_t ev;
   int rc;
   const long long wstride = (long long)(bl.wbytes / sizeof(double2));
+  const DigitTable* tab = nullptr;
+  if ((rc = ensure_digit_table(D, r.g, p.dl_method, r.dl, s, &tab))) return rc;
   timer_begin(T, s, &ev);
   rc = launch_mixed_inverse(r.g, p.n_mode, reinterpret_cast<const double2* const*>(base + bl.table_off), nsig, r.bases,
-                            r.dl, W, wstride, base + bl.scratch_off, s);
+                            r.dl, tab, W, wstride, base + bl.scratch_off, s);
   if (rc) return rc;
   timer_end(T, s, kStMixInv, ev);
   for (int b = 0; b < nsig; b++) {
@@ -450,8 +452,10 @@ int run_forward_batch(Device* D, Workspace* wk, const so3_parameters_t& p, int r
     if ((rc = launch_fwd_beta_conv(r.g, r.pP, r.pc, r.wr, Wb, s))) return rc;
     timer_end(T, s, kStFwdBetaConv, ev);
   }
+  const DigitTable* tab = nullptr;
+  if ((rc = ensure_digit_table(D, r.g, p.dl_method, r.dl, s, &tab))) return rc;
   timer_begin(T, s, &ev);
-  rc = launch_mixed_forward(r.g, p.n_mode, W, wstride, nsig, r.bases, r.dl,
+  rc = launch_mixed_forward(r.g, p.n_mode, W, wstride, nsig, r.bases, r.dl, tab,
                             reinterpret_cast<double2* const*>(base + bl.table_off), p.storage == SO3_STORAGE_COMPACT,
                             base + bl.scratch_off, s);
   if (rc) return rc;

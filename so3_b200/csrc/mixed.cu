@@ -32,7 +32,11 @@
 // table and, after the last chunk, read the accumulators back, combine the
 // diagonals in FP64 and store.  X is sliced once per batch by slice_kernel
 // into the exact shared-memory image of a stage.
+#include <algorithm>
 #include <cstdint>
+#include <cstdlib>
+#include <memory>
+#include <vector>
 
 #include "so3gpu_internal.h"
 #include "tc_sm100.cuh"
@@ -123,10 +127,25 @@ struct MixArgs {
   const long long* base;   // block bases per plane
   double2* W;              // inverse: column-major scratch part of signal 0; signal b at W + b * wstride
   double2* const* flmn;    // forward: per-signal coefficient arrays
+  const uint8_t* tab;      // resident A-digit blocks (null: generate from Delta)
+  const long long* pair_off;  // first block of each pair in tab
   long long wstride;
   int L, N, L0, nchunk, MT, plane0, n_mode, nsig, compact;
   long long CS, QS;  // column-major scratch strides
 };
+
+// Resident A digits: for every pair (mu, nu) and every block (row tile t of
+// m', chunk kc of l) with kc >= max(t, q), q = max(mu, nu) / 64 (all other
+// blocks are zero: A[m', l] needs l >= m' and l >= max(mu, nu)), the 7 x 64
+// x 64 digits in the inverse kernel's stage image (rows m', reduction l).
+// Blocks of a pair are stored row tile by row tile.
+__host__ __device__ inline long long digit_blocks(int q, int nc) {
+  return (long long)q * (nc - q) + (long long)(nc - q) * (nc - q + 1) / 2;
+}
+__host__ __device__ inline long long digit_block(int t, int kc, int q, int nc) {
+  if (t <= q) return (long long)t * (nc - q) + (kc - q);
+  return (long long)q * (nc - q) + (long long)(t - q) * nc - (long long)(t - q) * (t + q - 1) / 2 + (kc - t);
+}
 
 // A digits of one stage.  Thread task (row rho = 8*w + lane%8, quad q =
 // 4*it + lane/8, it = 0..3): the 4 reduction entries k0 + 4q .. +3 of row
@@ -176,7 +195,7 @@ __device__ __forceinline__ void gen_store(uint8_t* As, int gw, int lane, const d
   }
 }
 
-template <bool FWD>
+template <bool FWD, bool TAB>
 __global__ void __launch_bounds__(kThreads, 1) mixed_tc_kernel(MixArgs a) {
   extern __shared__ __align__(1024) unsigned char smraw[];
   TcSmem& S = *reinterpret_cast<TcSmem*>(smraw);
@@ -207,7 +226,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_tc_kernel(MixArgs a) {
   const uint32_t accum = tc::smem_u32(&S.accum);
   if (tid == 0) {
     for (int s = 0; s < kStages; s++) {
-      tc::mbar_init(full0 + 8 * s, kGen + 1);
+      tc::mbar_init(full0 + 8 * s, TAB ? 1 : kGen + 1);
       tc::mbar_init(empty0 + 8 * s, 1);
     }
     tc::mbar_init(accum, 1);
@@ -222,7 +241,9 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_tc_kernel(MixArgs a) {
   if (warp == 0) {
     // ------------------------------------------------ MMA issue (one thread)
     if (lane == 0 && nk > 0) {
-      constexpr uint32_t idesc = tc::idesc_s8(kM, kN);
+      // resident blocks are stored rows m', reduction l; the forward reads them
+      // transposed as an MN-major operand (16-l units 1024 B apart, 8-m' groups 128 B apart)
+      constexpr uint32_t idesc = tc::idesc_s8(kM, kN) | ((FWD && TAB) ? (1u << 16) : 0u);
       for (int k = 0; k < nk; k++) {
         const int s = k & 1;
         tc::mbar_wait(full0 + 8 * s, (k >> 1) & 1, &g_tc_error, 2);
@@ -236,7 +257,8 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_tc_kernel(MixArgs a) {
             const uint64_t ad = tc::smem_desc(xb + i * (kM * kKC) + ks * 2 * (kM * 16), kM * 16, 128);
 #pragma unroll
             for (int j = 0; j + i < kND; j++) {
-              const uint64_t bd = tc::smem_desc(ab + j * (kN * kKC) + ks * 2 * (kN * 16), kN * 16, 128);
+              const uint64_t bd = (FWD && TAB) ? tc::smem_desc(ab + j * (kN * kKC) + ks * 512, 128, 1024)
+                                               : tc::smem_desc(ab + j * (kN * kKC) + ks * 2 * (kN * 16), kN * 16, 128);
               tc::mma_i8(tbase + (uint32_t)(kN * (i + j)), ad, bd, idesc, (k | ks | i) != 0);
             }
           }
@@ -248,11 +270,17 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_tc_kernel(MixArgs a) {
   } else if (warp == 1) {
     // ------------------------------------------------ X stream (one thread)
     if (lane == 0) {
+      const int q = max(mu, nu) / kKC, ncap = a.nchunk;
+      const uint8_t* tb = TAB ? a.tab + (size_t)a.pair_off[(size_t)mu * a.N + nu] * kAStage : nullptr;
       for (int k = 0; k < nk; k++) {
         const int s = k & 1;
         if (k >= kStages) tc::mbar_wait(empty0 + 8 * s, ((k >> 1) - 1) & 1, &g_tc_error, 2);
-        tc::mbar_arrive_expect_tx(full0 + 8 * s, kXStage);
+        tc::mbar_arrive_expect_tx(full0 + 8 * s, TAB ? kXStage + kAStage : kXStage);
         tc::bulk_g2s(tc::smem_u32(&S.X[s][0]), xs + (size_t)(kc0 + k) * kXStage, kXStage, full0 + 8 * s);
+        if (TAB) {
+          const long long blk = FWD ? digit_block(k, t, q, ncap) : digit_block(t, kc0 + k, q, ncap);
+          tc::bulk_g2s(tc::smem_u32(&S.A[s][0]), tb + blk * kAStage, kAStage, full0 + 8 * s);
+        }
       }
     }
   } else {
@@ -260,8 +288,8 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_tc_kernel(MixArgs a) {
     const int gw = warp - 2;
     // the Delta loads of chunk k+1 are in flight while chunk k is split
     double xa[4][4], xb[4][4];
-    if (nk > 0) gen_load<FWD>(a, mu, nu, lmin, r0, kc0 * kKC, gw, lane, xa);
-    for (int k = 0; k < nk; k += 2) {
+    if (!TAB && nk > 0) gen_load<FWD>(a, mu, nu, lmin, r0, kc0 * kKC, gw, lane, xa);
+    for (int k = 0; k < (TAB ? 0 : nk); k += 2) {
       if (k + 1 < nk) gen_load<FWD>(a, mu, nu, lmin, r0, (kc0 + k + 1) * kKC, gw, lane, xb);
       if (k >= kStages) tc::mbar_wait(empty0, ((k >> 1) - 1) & 1, &g_tc_error, 2);
       gen_store(&S.A[0][0], gw, lane, xa);
@@ -472,6 +500,21 @@ __global__ void __launch_bounds__(256) slice_kernel(SliceArgs a) {
   }
 }
 
+// One CTA per pair: every stored block of the pair, generated exactly as the
+// inverse kernel's producer warps generate a stage (8 warps of 32 lanes).
+__global__ void __launch_bounds__(256) digit_table_kernel(MixArgs a, uint8_t* tab) {
+  const int pair = blockIdx.x, mu = pair / a.N, nu = pair % a.N;
+  const int gw = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int q = max(mu, nu) / kKC, nc = a.nchunk, lmin = max(mu, nu);
+  uint8_t* out = tab + (size_t)a.pair_off[pair] * kAStage;
+  for (int t = 0; t < nc; t++)
+    for (int kc = max(t, q); kc < nc; kc++) {
+      double x[4][4];
+      gen_load<false>(a, mu, nu, lmin, t * kN, kc * kKC, gw, lane, x);
+      gen_store(out + digit_block(t, kc, q, nc) * kAStage, gw, lane, x);
+    }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------- host side
@@ -501,20 +544,82 @@ static int mixed_args(const Geometry& g, int n_mode, int nsig, void* scratch, Mi
   return kOk;
 }
 
+size_t digit_table_bytes(int L, int N) {
+  const int nc = (L + kKC - 1) / kKC;
+  size_t blocks = 0;
+  for (int mu = 0; mu < L; mu++)
+    for (int nu = 0; nu < N; nu++) blocks += (size_t)digit_blocks(std::max(mu, nu) / kKC, nc);
+  return blocks * kAStage;
+}
+
+// Resident digit tables, one per (L, N, Delta recursion), built on first use
+// when it fits: at most a quarter of the device memory in total and 4 GiB
+// of free memory left after it (SO3GPU_DIGIT_TABLE=0 disables them).  Tables
+// are kept until the process exits, so streams that use one never see it
+// change.  Without a table the kernels generate the digits from Delta.
+int ensure_digit_table(Device* D, const Geometry& g, int method, const double* dl, cudaStream_t s,
+                       const DigitTable** out) {
+  *out = nullptr;
+  const char* env = getenv("SO3GPU_DIGIT_TABLE");
+  if (env && env[0] == '0') return kOk;
+  std::lock_guard<std::mutex> lk(D->mu);
+  for (const auto& t : D->digit_tables)
+    if (t->L == g.L && t->N == g.N && t->method == method) {
+      *out = t.get();
+      return kOk;
+    }
+  const size_t bytes = digit_table_bytes(g.L, g.N);
+  size_t used = 0;
+  for (const auto& t : D->digit_tables) used += t->bytes;
+  size_t freeb = 0, total = 0;
+  SO3G_CUDA(cudaMemGetInfo(&freeb, &total));
+  if (used + bytes > total / 4 || freeb < bytes + (size_t(4) << 30)) return kOk;  // generate instead
+  const int nc = (g.L + kKC - 1) / kKC;
+  std::vector<long long> off((size_t)g.L * g.N);
+  long long acc = 0;
+  for (int mu = 0; mu < g.L; mu++)
+    for (int nu = 0; nu < g.N; nu++) {
+      off[(size_t)mu * g.N + nu] = acc;
+      acc += digit_blocks(std::max(mu, nu) / kKC, nc);
+    }
+  auto t = std::make_unique<DigitTable>();
+  t->L = g.L, t->N = g.N, t->method = method, t->bytes = bytes;
+  SO3G_CUDA(cudaMalloc(&t->d, bytes));
+  if (cudaMalloc(&t->pair_off, off.size() * sizeof(long long)) != cudaSuccess) {
+    cudaFree(t->d);
+    return fail(kCudaError, "digit table offsets: cudaMalloc failed");
+  }
+  SO3G_CUDA(cudaMemcpyAsync(t->pair_off, off.data(), off.size() * sizeof(long long), cudaMemcpyHostToDevice, s));
+  MixArgs a{};
+  a.dl = dl, a.pair_off = t->pair_off, a.L = g.L, a.N = g.N, a.nchunk = nc;
+  digit_table_kernel<<<(unsigned)(g.L * g.N), 256, 0, s>>>(a, t->d);
+  SO3G_LAUNCHED();
+  SO3G_CUDA(cudaGetLastError());
+  SO3G_CUDA(cudaStreamSynchronize(s));  // offsets upload complete before the host vector goes
+  *out = t.get();
+  D->digit_tables.push_back(std::move(t));
+  return kOk;
+}
+
 template <bool FWD>
 static int launch_tc(const MixArgs& m, int nsig, cudaStream_t s) {
   const dim3 grid((unsigned)(m.L * m.N * m.MT), (nsig + kSig - 1) / kSig);
   const int smem = (int)sizeof(TcSmem);
-  SO3G_CUDA(cudaFuncSetAttribute(mixed_tc_kernel<FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  mixed_tc_kernel<FWD><<<grid, kThreads, smem, s>>>(m);
+  if (m.tab) {
+    SO3G_CUDA(cudaFuncSetAttribute(mixed_tc_kernel<FWD, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    mixed_tc_kernel<FWD, true><<<grid, kThreads, smem, s>>>(m);
+  } else {
+    SO3G_CUDA(cudaFuncSetAttribute(mixed_tc_kernel<FWD, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    mixed_tc_kernel<FWD, false><<<grid, kThreads, smem, s>>>(m);
+  }
   SO3G_LAUNCHED();
   SO3G_CUDA(cudaGetLastError());
   return kOk;
 }
 
 int launch_mixed_inverse(const Geometry& g, int n_mode, const double2* const* flmn_dev, int nsig,
-                         const long long* bases, const double* dl, double2* W, long long wstride, void* scratch,
-                         cudaStream_t s) {
+                         const long long* bases, const double* dl, const DigitTable* tab, double2* W,
+                         long long wstride, void* scratch, cudaStream_t s) {
   if (g.real) return fail(kUnsupported, "split-precision contractions take complex signals");
   MixArgs m;
   SliceArgs sa;
@@ -528,12 +633,13 @@ int launch_mixed_inverse(const Geometry& g, int n_mode, const double2* const* fl
   m.base = bases;
   m.W = W + g.QOFF;
   m.wstride = wstride;
+  if (tab) m.tab = tab->d, m.pair_off = tab->pair_off;
   return launch_tc<false>(m, nsig, s);
 }
 
 int launch_mixed_forward(const Geometry& g, int n_mode, const double2* W, long long wstride, int nsig,
-                         const long long* bases, const double* dl, double2* const* flmn_dev, int storage_compact,
-                         void* scratch, cudaStream_t s) {
+                         const long long* bases, const double* dl, const DigitTable* tab, double2* const* flmn_dev,
+                         int storage_compact, void* scratch, cudaStream_t s) {
   if (g.real) return fail(kUnsupported, "split-precision contractions take complex signals");
   MixArgs m;
   SliceArgs sa;
@@ -548,6 +654,7 @@ int launch_mixed_forward(const Geometry& g, int n_mode, const double2* W, long l
   m.base = bases;
   m.flmn = flmn_dev;
   m.compact = storage_compact;
+  if (tab) m.tab = tab->d, m.pair_off = tab->pair_off;
   return launch_tc<true>(m, nsig, s);
 }
 

@@ -91,6 +91,15 @@ struct DevPlan {
   double2* mem = nullptr;  // owns roots/mroots/chirp/kern
 };
 
+// Resident int8 digits of the split-precision contractions' Delta products
+// for one (L, N, Delta recursion); see mixed.cu.
+struct DigitTable {
+  int L = 0, N = 0, method = -1;
+  uint8_t* d = nullptr;
+  long long* pair_off = nullptr;
+  size_t bytes = 0;
+};
+
 struct Device {
   int device = 0;
   std::mutex mu;
@@ -99,6 +108,7 @@ struct Device {
   std::map<int, std::unique_ptr<DevPlan>> ffts;  // by length
   std::map<int, double2*> conv_kernels;          // weight kernel by L (MW/MWSS identical)
   std::map<std::string, long long*> bases;       // block bases by parameter key
+  std::vector<std::unique_ptr<DigitTable>> digit_tables;
 };
 
 // Per-stage CUDA-event timing (optional, per caller context).
@@ -203,12 +213,16 @@ int measure_int8_mma_rate(double* tops);
 // pointers (a device array of nsig pointers) and scratch planes (signal b at
 // W + b * wstride); scratch: mixed_scratch_bytes(g, nsig) bytes.
 size_t mixed_scratch_bytes(const Geometry& g, int nsig);
+int ensure_digit_table(Device* D, const Geometry& g, int method, const double* dl, cudaStream_t s,
+                       const DigitTable** out);
+size_t digit_table_bytes(int L, int N);
+// tab: resident digits of (g.L, g.N) or null (digits generated from dl).
 int launch_mixed_inverse(const Geometry& g, int n_mode, const double2* const* flmn_dev, int nsig,
-                         const long long* bases, const double* dl, double2* W, long long wstride, void* scratch,
-                         cudaStream_t s);
+                         const long long* bases, const double* dl, const DigitTable* tab, double2* W,
+                         long long wstride, void* scratch, cudaStream_t s);
 int launch_mixed_forward(const Geometry& g, int n_mode, const double2* W, long long wstride, int nsig,
-                         const long long* bases, const double* dl, double2* const* flmn_dev, int storage_compact,
-                         void* scratch, cudaStream_t s);
+                         const long long* bases, const double* dl, const DigitTable* tab, double2* const* flmn_dev,
+                         int storage_compact, void* scratch, cudaStream_t s);
 // Reads and clears the flag the tensor-core kernels set when a bounded wait
 // gave up (0: none; synchronous).
 int mixed_take_error();

@@ -116,3 +116,25 @@ def test_mixed_forward_leaves_skipped_blocks():
     ctx.forward_batch(f, p, "fp64", outs=ref)
     torch.cuda.synchronize()
     assert rel_err(out[0].cpu().numpy(), ref[0].cpu().numpy()) < TOL_MIXED
+
+
+@pytest.mark.parametrize("L,N,nsig,kw", [(70, 3, 5, {}), (130, 4, 3, dict(L0=5, storage=1)), (64, 64, 2, {})])
+def test_resident_digits_equal_generated_digits(L, N, nsig, kw, monkeypatch):
+    """The resident digit table (read as a K-major operand by the inverse and
+    as an MN-major operand by the forward) and the on-the-fly generation from
+    Delta hold the same digits, and the int32 accumulation is exact: the two
+    paths give bit-identical results."""
+    import torch
+    p = params(L, N, **kw)
+    ctx = so3.Context(0)
+    fls = [torch.from_numpy(synth.gen_flmn(p, 40 + i)).cuda() for i in range(nsig)]
+    f64 = ctx.inverse_batch(fls, p, "fp64")
+    outs = {}
+    for mode in ("0", "1"):
+        monkeypatch.setenv("SO3GPU_DIGIT_TABLE", mode)
+        inv = ctx.inverse_batch(fls, p, "mixed")
+        fwd = ctx.forward_batch(f64, p, "mixed")
+        torch.cuda.synchronize()
+        outs[mode] = ([x.cpu().numpy() for x in inv], [x.cpu().numpy() for x in fwd])
+    for a, b in zip(outs["0"][0] + outs["0"][1], outs["1"][0] + outs["1"][1]):
+        assert np.array_equal(a, b)

@@ -348,7 +348,7 @@ class Context:
 
 
 STAGES = ["inv_contract", "inv_beta", "inv_alpha", "inv_gamma", "fwd_gamma", "fwd_alpha", "fwd_beta_conv",
-          "fwd_contract", "mixed_inv_contract", "mixed_fwd_contract"]
+          "fwd_contract", "mixed_inv_contract", "mixed_fwd_contract", "mixed_fwd_beta"]
 
 PRECISIONS = {"fp64": 0, "mixed": 1}
 

@@ -440,6 +440,10 @@ int run_forward_batch(Device* D, Workspace* wk, const so3_parameters_t& p, int r
   cudaEvent_t ev;
   int rc;
   const long long wstride = (long long)(bl.wbytes / sizeof(double2));
+  // forward beta stage: one tensor-core product over the whole batch where
+  // supported (complex MW), else the FP64 DFT + weight convolution per signal
+  const BetaTable* bt = nullptr;
+  if (mixed_beta_supported(r.g) && (rc = ensure_beta_table(D, r.g, s, &bt))) return rc;
   for (int b = 0; b < nsig; b++) {
     double2* Wb = W + (size_t)b * wstride;
     timer_begin(T, s, &ev);
@@ -448,9 +452,15 @@ int run_forward_batch(Device* D, Workspace* wk, const so3_parameters_t& p, int r
     timer_begin(T, s, &ev);
     if ((rc = launch_fwd_alpha(r.g, r.pP, Wb, s))) return rc;
     timer_end(T, s, kStFwdAlpha, ev);
+    if (bt) continue;
     timer_begin(T, s, &ev);
     if ((rc = launch_fwd_beta_conv(r.g, r.pP, r.pc, r.wr, Wb, s))) return rc;
     timer_end(T, s, kStFwdBetaConv, ev);
+  }
+  if (bt) {
+    timer_begin(T, s, &ev);
+    if ((rc = launch_mixed_fwd_beta(r.g, W, wstride, nsig, bt, base + bl.scratch_off, s))) return rc;
+    timer_end(T, s, kStMixFwdBeta, ev);
   }
   const DigitTable* tab = nullptr;
   if ((rc = ensure_digit_table(D, r.g, p.dl_method, r.dl, s, &tab))) return rc;

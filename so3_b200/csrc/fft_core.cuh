@@ -29,6 +29,7 @@ struct FftPlan {
   const double2* mroots;     // e^{-2 pi i k/m}, k < m     (Bluestein)
   const double2* chirp;      // e^{-i pi k^2/n}, k < n     (Bluestein)
   const double2* kern;       // FFT_m(conj chirp) / m      (Bluestein)
+  const double2* half;       // e^{-i pi k/n}, k < n       (half-step roots: the MW beta phases)
   int ld() const { return blue ? m : n; }
   // any radix above 8 (needs the large-radix kernel instances)
   bool big() const {

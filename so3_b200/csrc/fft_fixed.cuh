@@ -113,7 +113,11 @@ __device__ __forceinline__ void odd_group(const double2* __restrict__ in, int j,
 
 // One Stockham pass of radix R at stride NS over T sequences of length N
 // (sequence t at src[t * LD]).  NG > 1 splits each butterfly into NG output
-// groups handled by different threads (odd R only).
+// groups handled by different threads (odd R only).  The sequence index runs
+// fastest over the threads, so the lanes of a warp that work on the same
+// butterfly of different sequences read the same twiddles (one cache sector
+// for up to T lanes) and, with the pitch LD = 8/T (mod 8) slots, hit
+// distinct shared-memory banks.
 template <int N, int R, int NS, int T, int LD, int NT, int NG, bool SK>
 __device__ __forceinline__ void pass(const double2* __restrict__ src, double2* __restrict__ dst,
                                      const double2* __restrict__ roots) {
@@ -122,8 +126,8 @@ __device__ __forceinline__ void pass(const double2* __restrict__ src, double2* _
   constexpr int UNITS = M * NG;
   constexpr bool TW = NS > 1;
   for (int u = threadIdx.x; u < T * UNITS; u += NT) {
-    const int t = u / UNITS;
-    const int rem = u - t * UNITS;
+    const int t = u % T;
+    const int rem = u / T;
     const int g = NG == 1 ? 0 : rem / M;
     const int j = NG == 1 ? rem : rem - g * M;
     const int k = j % NS;
@@ -217,14 +221,14 @@ struct P127 {
   static constexpr int n = 127, ld = extent<sk>(256);
   static __device__ __forceinline__ double2* run(double2* a, double2* b, const FftPlan& P) {
     for (int w = threadIdx.x; w < T * 256; w += NT) {
-      const int t = w >> 8, k = w & 255;
+      const int t = w % T, k = w / T;  // t fastest: lanes of one k share the chirp load
       double2* s = a + t * LD;
       s[phys<true>(k)] = k < 127 ? cmul(s[phys<true>(k)], __ldg(P.chirp + k)) : make_double2(0.0, 0.0);
     }
     __syncthreads();
     double2* r = fft256<T, LD, NT>(a, b, P.mroots);
     for (int w = threadIdx.x; w < T * 256; w += NT) {
-      const int t = w >> 8, k = w & 255;
+      const int t = w % T, k = w / T;
       double2* s = r + t * LD;
       s[phys<true>(k)] = cconj(cmul(s[phys<true>(k)], __ldg(P.kern + k)));
     }
@@ -232,7 +236,7 @@ struct P127 {
     double2* o = r == a ? b : a;
     r = fft256<T, LD, NT>(r, o, P.mroots);
     for (int w = threadIdx.x; w < T * 127; w += NT) {
-      const int t = w / 127, k = w - t * 127;
+      const int t = w % T, k = w / T;
       double2* s = r + t * LD;
       s[phys<true>(k)] = cmul(__ldg(P.chirp + k), cconj(s[phys<true>(k)]));
     }

@@ -33,6 +33,7 @@
 // diagonals in FP64 and store.  X is sliced once per batch by slice_kernel
 // into the exact shared-memory image of a stage.
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstdlib>
 #include <memory>
@@ -515,14 +516,273 @@ __global__ void __launch_bounds__(256) digit_table_kernel(MixArgs a, uint8_t* ta
     }
 }
 
+// ---------------------------------------------------------------- forward beta stage
+// The forward beta stage of one (n, m) column (extension onto the circle,
+// DFT, MW phase, quadrature-weight convolution, fold; stages.cu) is a fixed
+// linear map of the L beta samples g_b onto the L outputs m' >= 0 that
+// depends only on L and on s = (-1)^{m+n}:
+//   out(m') = sum_b R_s(m', b) g_b                   (s = +1, and m' = 0)
+//   out(m') = i sum_b R_s(m', b) g_b                 (s = -1, m' >= 1)
+// with R_s real:  R_s(m', b) = sum_{m''} c_b(m'') W_s(m'', m'),
+//   c_b(m'') = (e^{-i m'' beta_b} + s e^{i m'' beta_b}) / (2L-1)  (b < L-1),
+//   c_{L-1}(m'') = (-1)^{m''} / (2L-1)     (beta_b = pi (2b+1)/(2L-1), MW),
+//   W_s(m'', m') = 2 pi (w(m'-m'') + s w(-m'-m'')) for m' >= 1, 2 pi w(-m'') for m' = 0,
+// w the quadrature weights of so3_sampling.c:32-51.  For the split-precision
+// batch path the stage runs as one more int8 Ozaki product on the tensor
+// cores: the columns of a parity class form the 128-row operand (64 columns
+// x re/im), R_s (FP64, sliced once per L) the resident 64-row operand.
+__device__ __forceinline__ double2 quad_weight(int p, int L) {
+  if (p > 2 * (L - 1) || p < -2 * (L - 1)) return make_double2(0.0, 0.0);
+  if (p == 1) return make_double2(0.0, -1.5707963267948966192313216916397514);
+  if (p == -1) return make_double2(0.0, 1.5707963267948966192313216916397514);
+  if (p & 1) return make_double2(0.0, 0.0);
+  return make_double2(2.0 / (1.0 - (double)p * (double)p), 0.0);
+}
+
+// R_s in FP64: out[(sc * L + m') * L + b], sc = 0 (s = +1) or 1 (s = -1).
+__global__ void beta_matrix_kernel(int L, double* out) {
+  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= 2LL * L * L) return;
+  const int b = (int)(id % L), mp = (int)((id / L) % L), sc = (int)(id / ((long long)L * L));
+  const double s = sc ? -1.0 : 1.0;
+  const int P = 2 * L - 1;
+  double2 acc = make_double2(0.0, 0.0);
+  for (int mpp = -(L - 1); mpp <= L - 1; mpp++) {
+    double2 c;
+    if (b < L - 1) {
+      // e^{-i pi m'' (2b+1) / P}: angle reduced exactly modulo 2P
+      long long k = ((long long)mpp * (2 * b + 1)) % (2LL * P);
+      if (k < 0) k += 2LL * P;
+      double sn, cs;
+      sincospi((double)k / (double)P, &sn, &cs);
+      c = make_double2((1.0 + s) * cs / P, (-1.0 + s) * sn / P);  // e^{-ix} + s e^{ix}
+    } else {
+      c = make_double2(((mpp & 1) ? -1.0 : 1.0) / P, 0.0);
+    }
+    double2 Wv;
+    if (mp >= 1) {
+      const double2 w1 = quad_weight(mp - mpp, L), w2 = quad_weight(-mp - mpp, L);
+      Wv = make_double2(w1.x + s * w2.x, w1.y + s * w2.y);
+    } else {
+      Wv = quad_weight(-mpp, L);
+    }
+    acc.x = fma(c.x, Wv.x, fma(-c.y, Wv.y, acc.x));
+    acc.y = fma(c.x, Wv.y, fma(c.y, Wv.x, acc.y));
+  }
+  acc.x *= 6.283185307179586476925286766559005768;
+  acc.y *= 6.283185307179586476925286766559005768;
+  out[id] = (sc == 1 && mp >= 1) ? acc.y : acc.x;  // the real factor (see above)
+}
+
+struct BetaArgs {
+  uint8_t* xs;           // [sig][tile][chunk][kXStage]
+  double* xscale;        // [sig][tile][kM]
+  const double2* W;      // row-major scratch part of signal 0, signal b at W + b * wstride (slicing input)
+  double2* Wc;           // column-major scratch part of signal 0 (products' output)
+  const uint8_t* tab;    // R digits: [sc][tile t][chunk kc][kAStage]
+  double rscale;         // R = rscale * (digit value)
+  long long wstride;
+  int L, nplanes, plane0, ct, nchunk, MT, nsig;
+  long long RS, PS, CS, QS;
+};
+
+// Column tile (p, sc, ct): the columns m = m_first + 2 (64 ct + j), j < 64, of
+// plane p whose parity class (m + n) mod 2 is sc.
+__device__ __forceinline__ int beta_first_m(int L, int n, int sc) {
+  const int m = -(L - 1);
+  return (((m + n) & 1) == sc) ? m : m + 1;
+}
+
+// One CTA per (signal, column tile): 128 rows c = 2 j + part (column j of the
+// tile, real / imaginary part), reduction b < L; scales, then 7 digit planes
+// in the stage image of beta_tc_kernel.
+__global__ void __launch_bounds__(256) beta_slice_kernel(BetaArgs a) {
+  __shared__ double colmax[2][kM];
+  const int c = threadIdx.x & (kM - 1), half = threadIdx.x >> 7;
+  const int tile = blockIdx.x, sig = blockIdx.y;
+  const int ct = tile % a.ct, sc = (tile / a.ct) & 1, p = tile / (2 * a.ct);
+  const int n = p - a.plane0, L = a.L, j = c >> 1, part = c & 1;
+  const int m = beta_first_m(L, n, sc) + 2 * (64 * ct + j);
+  const bool active = m <= L - 1 && sig < a.nsig;
+  const double* src = reinterpret_cast<const double*>(a.W + (long long)sig * a.wstride + (long long)p * a.PS +
+                                                      (active ? m + L - 1 : 0)) + part;
+  const int nblk = a.nchunk * (kKC / 16);
+  double mx = 0.0;
+  for (int kb = half; kb < nblk; kb += 2)
+#pragma unroll
+    for (int e = 0; e < 16; e++) {
+      const int bb = 16 * kb + e;
+      if (active && bb < L) mx = fmax(mx, fabs(__ldg(src + 2LL * bb * a.RS)));
+    }
+  colmax[half][c] = mx;
+  __syncthreads();
+  mx = fmax(colmax[0][c], colmax[1][c]);
+  int ex = 0;
+  frexp(mx, &ex);
+  const double scale = mx > 0.0 ? ldexp(1.0, ex + 1) : 1.0;
+  const double inv = 1.0 / scale;
+  const size_t gt = (size_t)sig * gridDim.x + tile;
+  if (half == 0) a.xscale[gt * kM + c] = scale;
+  uint8_t* out = a.xs + gt * (size_t)a.nchunk * kXStage;
+  for (int kb = half; kb < nblk; kb += 2) {
+    double v[16];
+#pragma unroll
+    for (int e = 0; e < 16; e++) {
+      const int bb = 16 * kb + e;
+      v[e] = (active && bb < L) ? __ldg(src + 2LL * bb * a.RS) * inv : 0.0;
+    }
+    uint32_t w[4][kS];
+#pragma unroll
+    for (int qd = 0; qd < 4; qd++) {
+      double r[4];
+#pragma unroll
+      for (int e = 0; e < 4; e++) r[e] = v[4 * qd + e];
+      split_pack4(r, w[qd]);
+    }
+    uint8_t* dst = out + (size_t)(kb >> 2) * kXStage + tile_off(kM, c, (kb & 3) * 16);
+#pragma unroll
+    for (int i = 0; i < kS; i++)
+      *reinterpret_cast<uint4*>(dst + i * (kM * kKC)) = make_uint4(w[0][i], w[1][i], w[2][i], w[3][i]);
+  }
+}
+
+// One CTA per (column tile, 64-row tile of m', signal): D_d[c, m'] over the
+// L beta samples in chunks of 64, both operands streamed by bulk copies.
+__global__ void __launch_bounds__(kThreads, 1) beta_tc_kernel(BetaArgs a) {
+  extern __shared__ __align__(1024) unsigned char smraw[];
+  TcSmem& S = *reinterpret_cast<TcSmem*>(smraw);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tile = blockIdx.x, t = blockIdx.y, sig = blockIdx.z;
+  const int ct = tile % a.ct, sc = (tile / a.ct) & 1, p = tile / (2 * a.ct);
+  const int n = p - a.plane0, L = a.L, r0 = t * kN, nk = a.nchunk;
+  const size_t gt = (size_t)sig * gridDim.x + tile;
+  const uint8_t* xs = a.xs + gt * (size_t)nk * kXStage;
+  const uint8_t* tb = a.tab + (size_t)(sc * a.MT + t) * nk * kAStage;
+  if (*reinterpret_cast<volatile int*>(&g_tc_error)) return;
+
+  const uint32_t full0 = tc::smem_u32(&S.full[0]), empty0 = tc::smem_u32(&S.empty[0]);
+  const uint32_t accum = tc::smem_u32(&S.accum);
+  if (tid == 0) {
+    for (int st = 0; st < kStages; st++) {
+      tc::mbar_init(full0 + 8 * st, 1);
+      tc::mbar_init(empty0 + 8 * st, 1);
+    }
+    tc::mbar_init(accum, 1);
+    tc::mbar_fence_init();
+  }
+  if (warp == 0) tc::tmem_alloc(tc::smem_u32(&S.tmem_base), kTmemCols);
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tbase = S.tmem_base;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      constexpr uint32_t idesc = tc::idesc_s8(kM, kN);
+      for (int k = 0; k < nk; k++) {
+        const int st = k & 1;
+        tc::mbar_wait(full0 + 8 * st, (k >> 1) & 1, &g_tc_error, 2);
+        tc::tc_fence_after();
+        const uint32_t xb = tc::smem_u32(&S.X[st][0]), ab = tc::smem_u32(&S.A[st][0]);
+#pragma unroll
+        for (int ks = 0; ks < kKC / 32; ks++) {
+#pragma unroll
+          for (int i = 0; i < kS; i++) {
+            const uint64_t ad = tc::smem_desc(xb + i * (kM * kKC) + ks * 2 * (kM * 16), kM * 16, 128);
+#pragma unroll
+            for (int jj = 0; jj + i < kND; jj++) {
+              const uint64_t bd = tc::smem_desc(ab + jj * (kN * kKC) + ks * 2 * (kN * 16), kN * 16, 128);
+              tc::mma_i8(tbase + (uint32_t)(kN * (i + jj)), ad, bd, idesc, (k | ks | i) != 0);
+            }
+          }
+        }
+        tc::mma_commit(empty0 + 8 * st);
+      }
+      tc::mma_commit(accum);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      for (int k = 0; k < nk; k++) {
+        const int st = k & 1;
+        if (k >= kStages) tc::mbar_wait(empty0 + 8 * st, ((k >> 1) - 1) & 1, &g_tc_error, 2);
+        tc::mbar_arrive_expect_tx(full0 + 8 * st, kXStage + kAStage);
+        tc::bulk_g2s(tc::smem_u32(&S.X[st][0]), xs + (size_t)k * kXStage, kXStage, full0 + 8 * st);
+        tc::bulk_g2s(tc::smem_u32(&S.A[st][0]), tb + (size_t)k * kAStage, kAStage, full0 + 8 * st);
+      }
+    }
+  } else {
+    // epilogue: thread <-> TMEM lane c = 2 j + part, 32 output rows m'
+    const int gw = warp - 2, lq = warp & 3, ch = gw >> 2;
+    const int c = 32 * lq + lane, j = c >> 1, part = c & 1;
+    const int m = beta_first_m(L, n, sc) + 2 * (64 * ct + j);
+    const bool active = m <= L - 1 && sig < a.nsig;
+    const double scale = a.xscale[gt * kM + c];
+    tc::mbar_wait(accum, 0, &g_tc_error, 2);
+    tc::tc_fence_after();
+    double2* out = a.Wc + (long long)sig * a.wstride + (long long)p * a.QS + (long long)(m + L - 1) * a.CS;
+#pragma unroll 1
+    for (int g = 0; g < 4; g++) {
+      __syncwarp();
+      const int col = 32 * ch + 8 * g;
+      double v[8];
+#pragma unroll
+      for (int e = 0; e < 8; e++) v[e] = 0.0;
+      int acc[kND][8];
+#pragma unroll
+      for (int d = 0; d < kND; d++)
+        tc::tmem_ld8(tbase + ((uint32_t)(32 * lq) << 16) + (uint32_t)(kN * d + col), acc[d]);
+      tc::tmem_wait_ld();
+      double wd = a.rscale * 0.000061035156250000000;  // R scale x 2^{-14}: diagonal 0
+#pragma unroll
+      for (int d = 0; d < kND; d++) {
+#pragma unroll
+        for (int e = 0; e < 8; e++) v[e] = fma(int_to_double(acc[d][e]), wd, v[e]);
+        wd *= 0.0078125;
+      }
+      double re[4], im[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const double send = part ? v[q] * scale : v[4 + q] * scale;
+        const double recv = __shfl_xor_sync(0xffffffffu, send, 1);
+        re[q] = part ? recv : v[q] * scale;
+        im[q] = part ? v[4 + q] * scale : recv;
+      }
+      if (!active) continue;
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int row = r0 + col + 4 * part + q;
+        if (row >= L) continue;
+        double2 val = make_double2(re[q], im[q]);
+        if (sc == 1 && row >= 1) val = make_double2(-val.y, val.x);  // times i
+        out[row] = val;
+      }
+    }
+  }
+
+  if (warp == 0 && lane == 0) tc::mbar_wait(accum, 0, &g_tc_error, 2);
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    __syncwarp();
+    tc::tc_fence_after();
+    tc::tmem_dealloc(tbase, kTmemCols);
+  }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------- host side
 static int nchunks(const Geometry& g) { return (g.L + kKC - 1) / kKC; }
 
+static size_t beta_scratch_bytes(const Geometry& g, int nsig);
+bool mixed_beta_supported(const Geometry& g);
+
+// Sliced operands of the contractions and of the forward beta products (the
+// two never live at the same time, so they share one region).
 size_t mixed_scratch_bytes(const Geometry& g, int nsig) {
   const size_t groups = (nsig + kSig - 1) / kSig, pairs = (size_t)g.L * g.N;
-  return groups * pairs * ((size_t)nchunks(g) * kXStage + kM * sizeof(double)) + 256;
+  const size_t contr = groups * pairs * ((size_t)nchunks(g) * kXStage + kM * sizeof(double)) + 256;
+  return mixed_beta_supported(g) ? std::max(contr, beta_scratch_bytes(g, nsig)) : contr;
 }
 
 static int mixed_args(const Geometry& g, int n_mode, int nsig, void* scratch, MixArgs* m, SliceArgs* s) {
@@ -656,6 +916,99 @@ int launch_mixed_forward(const Geometry& g, int n_mode, const double2* W, long l
   m.compact = storage_compact;
   if (tab) m.tab = tab->d, m.pair_off = tab->pair_off;
   return launch_tc<true>(m, nsig, s);
+}
+
+// ---------------------------------------------------------------- forward beta (host)
+static int beta_tiles(const Geometry& g, int* ct) {
+  *ct = (g.L + 63) / 64;  // column tiles per parity class (a class holds at most L columns)
+  return g.nplanes * 2 * *ct;
+}
+
+static size_t beta_scratch_bytes(const Geometry& g, int nsig) {
+  int ct = 0;
+  const size_t tiles = beta_tiles(g, &ct);
+  return (size_t)nsig * tiles * ((size_t)nchunks(g) * kXStage + kM * sizeof(double)) + 256;
+}
+
+bool mixed_beta_supported(const Geometry& g) { return g.mw && !g.real && g.nb == g.L; }
+
+// The 7 digits of r in [-1/2, 1/2] (host copy of split_pack4's rule).
+static void split_host(double r, uint8_t* q) {
+  const long long v = (long long)std::nearbyint(r * 562949953421312.0);
+  const unsigned long long u = (unsigned long long)(v + kDigitOffset);
+  for (int i = 0; i < kS; i++) {
+    const int d = (int)((u >> (7 * (kS - 1 - i))) & (i == 0 ? 255u : 127u));
+    q[i] = (uint8_t)((d - 64) & 255);
+  }
+}
+
+// Resident digits of R_s for this L (MW), one table per device and L.
+int ensure_beta_table(Device* D, const Geometry& g, cudaStream_t s, const BetaTable** out) {
+  *out = nullptr;
+  std::lock_guard<std::mutex> lk(D->mu);
+  for (const auto& t : D->beta_tables)
+    if (t->L == g.L) {
+      *out = t.get();
+      return kOk;
+    }
+  const int L = g.L, nc = nchunks(g), MT = nc;
+  double* dR = nullptr;
+  SO3G_CUDA(cudaMalloc(&dR, 2 * (size_t)L * L * sizeof(double)));
+  beta_matrix_kernel<<<(unsigned)((2LL * L * L + 255) / 256), 256, 0, s>>>(L, dR);
+  SO3G_LAUNCHED();
+  std::vector<double> R(2 * (size_t)L * L);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(R.data(), dR, R.size() * sizeof(double), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(dR);
+  if (e != cudaSuccess) return fail(kCudaError, std::string("beta matrix: ") + cudaGetErrorString(e));
+  double mx = 0.0;
+  for (double v : R) mx = std::max(mx, std::fabs(v));
+  int ex = 0;
+  std::frexp(mx, &ex);
+  const double rscale = mx > 0.0 ? std::ldexp(1.0, ex + 1) : 1.0;  // |R / rscale| < 1/2
+  const size_t bytes = (size_t)2 * MT * nc * kAStage;
+  std::vector<uint8_t> host(bytes, 0);
+  uint8_t q[kS];
+  for (int sc = 0; sc < 2; sc++)
+    for (int mp = 0; mp < L; mp++)
+      for (int b = 0; b < L; b++) {
+        split_host(R[((size_t)sc * L + mp) * L + b] / rscale, q);
+        uint8_t* blk = host.data() + ((size_t)(sc * MT + mp / kN) * nc + b / kKC) * kAStage;
+        const int off = tile_off(kN, mp % kN, b % kKC);
+        for (int i = 0; i < kS; i++) blk[i * (kN * kKC) + off] = q[i];
+      }
+  auto t = std::make_unique<BetaTable>();
+  t->L = L, t->rscale = rscale;
+  SO3G_CUDA(cudaMalloc(&t->d, bytes));
+  SO3G_CUDA(cudaMemcpyAsync(t->d, host.data(), bytes, cudaMemcpyHostToDevice, s));
+  SO3G_CUDA(cudaStreamSynchronize(s));  // the host image goes out of scope
+  *out = t.get();
+  D->beta_tables.push_back(std::move(t));
+  return kOk;
+}
+
+int launch_mixed_fwd_beta(const Geometry& g, double2* W, long long wstride, int nsig, const BetaTable* tab,
+                          void* scratch, cudaStream_t s) {
+  if (!mixed_beta_supported(g)) return fail(kUnsupported, "split-precision beta stage: complex MW signals only");
+  BetaArgs a{};
+  int ct = 0;
+  const int tiles = beta_tiles(g, &ct);
+  if (nsig > 65535) return fail(kUnsupported, "split-precision beta stage: batch too large");
+  a.xs = static_cast<uint8_t*>(scratch);
+  a.xscale = reinterpret_cast<double*>(a.xs + (((size_t)nsig * tiles * nchunks(g) * kXStage + 255) & ~size_t(255)));
+  a.W = W, a.Wc = W + g.QOFF, a.tab = tab->d, a.rscale = tab->rscale, a.wstride = wstride;
+  a.L = g.L, a.nplanes = g.nplanes, a.plane0 = g.plane0, a.ct = ct, a.nchunk = nchunks(g), a.MT = nchunks(g);
+  a.nsig = nsig, a.RS = g.RS, a.PS = g.PS, a.CS = g.CS, a.QS = g.QS;
+  beta_slice_kernel<<<dim3((unsigned)tiles, (unsigned)nsig), 256, 0, s>>>(a);
+  SO3G_LAUNCHED();
+  SO3G_CUDA(cudaGetLastError());
+  const int smem = (int)sizeof(TcSmem);
+  SO3G_CUDA(cudaFuncSetAttribute(beta_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  beta_tc_kernel<<<dim3((unsigned)tiles, (unsigned)a.MT, (unsigned)nsig), kThreads, smem, s>>>(a);
+  SO3G_LAUNCHED();
+  SO3G_CUDA(cudaGetLastError());
+  return kOk;
 }
 
 // Reads and clears the tensor-core kernels' wait-timeout flag (0: none).

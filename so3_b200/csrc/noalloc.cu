@@ -42,7 +42,7 @@ constexpr int kMaxL = 64;
 constexpr int kMaxN = 64;
 constexpr int kDlEntries = kMaxL * (kMaxL + 1) * (2 * kMaxL + 1) / 6;
 constexpr int kRisboWork = 2 * (kMaxL + 6) * (kMaxL + 6);
-constexpr int kFftSlot = 2 * 256 + 128;  // Bluestein m + n + m for n <= 128
+constexpr int kFftSlot = 2 * 256 + 2 * 128;  // Bluestein m + n + m, then n half-step roots, for n <= 128
 constexpr int kMaxPlanes = 2 * kMaxN - 1;
 
 static __device__ __align__(256) double2 g_scratch[kScratchBytes / sizeof(double2)];
@@ -110,6 +110,15 @@ void fft_ld_fixed(cld* x, int n, int sign) {
       }
 }
 
+// Half-step roots e^{-i pi k/n} of a plan, at slot offset `at`.
+void half_table(int n, FftPlan* P, double2* h, const double2* dev, int at) {
+  for (int k = 0; k < n; k++) {
+    const cld r = root_l(k, 2LL * n);
+    h[at + k] = make_double2((double)r.real(), (double)r.imag());
+  }
+  P->half = dev + at;
+}
+
 // Fills plan tables for length n into host slot h; device pointers point at dev.
 void plan_tables(int n, FftPlan* P, double2* h, const double2* dev) {
   *P = FftPlan{};
@@ -122,6 +131,7 @@ void plan_tables(int n, FftPlan* P, double2* h, const double2* dev) {
       h[k] = make_double2((double)r.real(), (double)r.imag());
     }
     P->roots = dev;
+    half_table(n, P, h, dev, n);
     return;
   }
   int m = 1;
@@ -150,6 +160,7 @@ void plan_tables(int n, FftPlan* P, double2* h, const double2* dev) {
   P->mroots = dev;
   P->chirp = dev + m;
   P->kern = dev + m + n;
+  half_table(n, P, h, dev, 2 * m + n);
 }
 
 int setup_device(NoAllocDevice& S, cudaStream_t s) {

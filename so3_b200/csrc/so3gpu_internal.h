@@ -100,6 +100,14 @@ struct DigitTable {
   size_t bytes = 0;
 };
 
+// Resident int8 digits of the forward beta stage's real matrices R_s for one
+// L (MW sampling); see mixed.cu.
+struct BetaTable {
+  int L = 0;
+  uint8_t* d = nullptr;
+  double rscale = 1.0;
+};
+
 struct Device {
   int device = 0;
   std::mutex mu;
@@ -109,6 +117,7 @@ struct Device {
   std::map<int, double2*> conv_kernels;          // weight kernel by L (MW/MWSS identical)
   std::map<std::string, long long*> bases;       // block bases by parameter key
   std::vector<std::unique_ptr<DigitTable>> digit_tables;
+  std::vector<std::unique_ptr<BetaTable>> beta_tables;
 };
 
 // Per-stage CUDA-event timing (optional, per caller context).
@@ -123,6 +132,7 @@ enum Stage : int {
   kStFwdContract,
   kStMixInv,  // split-precision contraction (slicing + tensor-core products), inverse
   kStMixFwd,  // split-precision contraction, forward
+  kStMixFwdBeta,  // split-precision forward beta stage (slicing + tensor-core products)
   kStCount = 16
 };
 struct StageTimer {
@@ -216,6 +226,13 @@ size_t mixed_scratch_bytes(const Geometry& g, int nsig);
 int ensure_digit_table(Device* D, const Geometry& g, int method, const double* dl, cudaStream_t s,
                        const DigitTable** out);
 size_t digit_table_bytes(int L, int N);
+// Forward beta stage of a split-precision batch as an int8 tensor-core
+// product (complex MW signals; W: row-major scratch of signal 0, output into
+// the column-major parts).
+bool mixed_beta_supported(const Geometry& g);
+int ensure_beta_table(Device* D, const Geometry& g, cudaStream_t s, const BetaTable** out);
+int launch_mixed_fwd_beta(const Geometry& g, double2* W, long long wstride, int nsig, const BetaTable* tab,
+                          void* scratch, cudaStream_t s);
 // tab: resident digits of (g.L, g.N) or null (digits generated from dl).
 int launch_mixed_inverse(const Geometry& g, int n_mode, const double2* const* flmn_dev, int nsig,
                          const long long* bases, const double* dl, const DigitTable* tab, double2* W,

@@ -82,8 +82,10 @@ struct Fix {
   static constexpr int NT = NT_, MINB = MINB_, T = T_;
   static constexpr int ldP = PP<1, 1, 1>::ld, ldC = PC<1, 1, 1>::ld;
   static constexpr int ldmax = ldP > ldC ? ldP : ldC;
-  // pitch = 2 (mod 8) slots: T-interleaved staging loops hit distinct banks
-  static constexpr int LD = T_ > 1 ? ldmax + ((10 - ldmax % 8) % 8) : ldmax;
+  // pitch = 8/T (mod 8) 16-byte slots: the T sequences of one index, which
+  // consecutive threads handle, fall into distinct banks
+  static constexpr int LDMOD = T_ >= 8 ? 1 : T_ == 4 ? 2 : T_ == 2 ? 4 : 0;
+  static constexpr int LD = T_ > 1 ? ldmax + ((LDMOD - ldmax % 8 + 8) % 8) : ldmax;
   // element k of a sequence in the buffers of the runP / runC lengths
   static __device__ __forceinline__ int at(int k) { return fx::phys<PP<1, 1, 1>::sk>(k); }
   static __device__ __forceinline__ int atC(int k) { return fx::phys<PC<1, 1, 1>::sk>(k); }
@@ -112,11 +114,6 @@ __device__ __forceinline__ int wrapi(int k, int P) {
   k %= P;
   return k < 0 ? k + P : k;
 }
-__device__ __forceinline__ double2 phase(int k, int den, double sign) {  // e^{sign i pi k/den}
-  double s, c;
-  sincospi((double)k / (double)den, &s, &c);
-  return make_double2(c, sign * s);
-}
 }  // namespace
 
 // ------------------------------------------------------------------ inverse
@@ -140,7 +137,7 @@ __global__ void __launch_bounds__(E::NT, E::MINB) inv_beta_kernel(Geometry g, Ff
     const double sg = ((m + n) & 1) ? -1.0 : 1.0;
     double2 xp = v, xn = make_double2(sg * v.x, sg * v.y);
     if (g.mw) {
-      const double2 e = phase(mp, 2 * L - 1, 1.0);
+      const double2 e = cconj(__ldg(P.half + mp));  // e^{i pi m'/(2L-1)}
       xp = cmul(xp, e);
       xn = cmul(xn, cconj(e));
     }
@@ -322,7 +319,10 @@ __global__ void __launch_bounds__(E::NT, E::MINB) fwd_beta_conv_kernel(Geometry 
   for (int idx = threadIdx.x; idx < T * (2 * L - 1); idx += E::NT) {
     const int t = idx / (2 * L - 1), mpp = idx - t * (2 * L - 1) - (L - 1);
     double2 v = cscale(r[t * ld + E::at(wrapi(mpp, Pn))], invP);
-    if (g.mw) v = cmul(v, phase(mpp, 2 * L - 1, -1.0));
+    if (g.mw) {  // e^{-i pi m''/(2L-1)}
+      const double2 e = __ldg(P.half + (mpp < 0 ? -mpp : mpp));
+      v = cmul(v, mpp < 0 ? cconj(e) : e);
+    }
     o[t * ld + E::atC(wrapi(mpp, pc))] = cconj(v);
   }
   __syncthreads();

@@ -312,10 +312,17 @@ int ensure_fft(Device* D, int n, FftPlan* out) {
       host[(size_t)m + n + k] = make_double2((double)v.real(), (double)v.imag());
     }
   }
+  const size_t half_at = host.size();
+  host.resize(half_at + n);
+  for (int k = 0; k < n; k++) {
+    cld r = root_l(k, 2LL * n);  // e^{-i pi k/n}
+    host[half_at + k] = make_double2((double)r.real(), (double)r.imag());
+  }
   cudaError_t e = cudaMalloc(&dp->mem, host.size() * sizeof(double2));
   if (e != cudaSuccess) return fail(kOutOfMemory, "FFT table allocation failed");
   e = cudaMemcpy(dp->mem, host.data(), host.size() * sizeof(double2), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return fail(kCudaError, std::string("FFT table upload: ") + cudaGetErrorString(e));
+  P.half = dp->mem + half_at;
   if (!P.blue) {
     P.roots = dp->mem;
   } else {

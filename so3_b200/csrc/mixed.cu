@@ -30,7 +30,8 @@
 // the MMAs; warp 1 streams the pre-sliced X chunk of each stage with one bulk
 // copy; warps 2-9 generate the A digits of each stage from the FP64 Delta
 // table and, after the last chunk, read the accumulators back, combine the
-// diagonals in FP64 and store.  X is sliced once per batch by slice_kernel
+// diagonals in FP64 and store.  X is sliced once per batch (slice_inv_kernel,
+// slice_fwd_kernel)
 // into the exact shared-memory image of a stage.
 #include <algorithm>
 #include <cmath>
@@ -394,13 +395,12 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_tc_kernel(MixArgs a) {
 }
 
 // ---------------------------------------------------------------- slicing
-// One CTA per (pair mu * N + nu, group of 16 signals).  Thread -> signal
-// column c = tid % 128 and every other 16-entry block of the reduction index:
-// pass 1 finds the column's largest magnitude, pass 2 writes the 7 digit
-// planes of 16 entries with one 16-byte store each, in the shared-memory
-// image of the tensor-core kernel's stages.
+// The X operand of a pair (mu, nu): column c = 8 * signal + 2 * combo + part
+// (combo bit 0: m = -mu, bit 1: n = -nu; part: real / imaginary), reduction
+// entries k < 64 * nchunk, cut into the 7 digit planes of every stage image
+// with the column's power-of-two scale.
 //   inverse: X[l, c]   = (2l+1)/(8 pi^2) f_{l m n} (times (-1)^l for one negative index)
-//   forward: X'[m', c] = W[n][m'][m]              (times (-1)^{m'} for one negative index)
+//   forward: X'[m', c] = Wc[n][m][m']             (times (-1)^{m'} for one negative index)
 struct SliceArgs {
   uint8_t* xs;
   double* xscale;
@@ -412,6 +412,15 @@ struct SliceArgs {
   long long CS, QS;
 };
 
+__device__ __forceinline__ double scale_of(double mx) {  // power of two with |x / scale| < 1/2
+  int ex = 0;
+  frexp(mx, &ex);
+  return mx > 0.0 ? ldexp(1.0, ex + 1) : 1.0;
+}
+
+// Two-pass slicing (band limits whose staged columns exceed shared memory):
+// one CTA per (pair, group of 16 signals), thread <-> real column c and every
+// other 16-entry block; pass 1 finds the scales, pass 2 writes the digits.
 // Column c of one pair: the source pointer and the stride between
 // consecutive reduction entries (inverse: l^2 + l + m grows by 2l + 2),
 // resolved once per thread.
@@ -499,6 +508,180 @@ __global__ void __launch_bounds__(256) slice_kernel(SliceArgs a) {
     for (int i = 0; i < kS; i++)
       *reinterpret_cast<uint4*>(dst + i * (kM * kKC)) = make_uint4(w[0][i], w[1][i], w[2][i], w[3][i]);
   }
+}
+
+
+// Single-pass slicing: a CTA stages its columns (complex, all reduction
+// entries) in shared memory with coalesced loads, finds each column's scale
+// with a warp reduction, then writes 16-entry digit slots.
+constexpr int kSliceCols = 16;  // complex columns per slicing CTA
+constexpr int kSliceSmemMax = 200 * 1024;  // staged columns fit (L <= 768)
+
+// Digits of the staged columns: thread <-> (real column c of the CTA's 32,
+// block of 16 entries); c_base: first row of the stage image.
+__device__ __forceinline__ void slice_from_smem(const double2* __restrict__ col, int Lp, const double* scl,
+                                                uint8_t* pb, int c_base) {
+  const int nblk = Lp / 16;
+  for (int w = threadIdx.x; w < 2 * kSliceCols * nblk; w += blockDim.x) {
+    const int c = w & 31, kb = w >> 5, cc = c >> 1, part = c & 1;
+    const double inv = 1.0 / scl[c];
+    uint32_t d[4][kS];
+#pragma unroll
+    for (int qd = 0; qd < 4; qd++) {
+      double r[4];
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const double2 x = col[(size_t)cc * Lp + 16 * kb + 4 * qd + e];
+        r[e] = (part ? x.y : x.x) * inv;
+      }
+      split_pack4(r, d[qd]);
+    }
+    uint8_t* dst = pb + (size_t)(kb >> 2) * kXStage + tile_off(kM, c_base + c, (kb & 3) * 16);
+#pragma unroll
+    for (int i = 0; i < kS; i++)
+      *reinterpret_cast<uint4*>(dst + i * (kM * kKC)) = make_uint4(d[0][i], d[1][i], d[2][i], d[3][i]);
+  }
+}
+
+// Largest magnitude of the real and imaginary parts of each staged column
+// (warp w handles columns w, w + 8); scales into scl[2 cc + part].
+__device__ __forceinline__ void column_scales(const double2* __restrict__ col, int Lp, double* scl) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int cc = warp; cc < kSliceCols; cc += nw) {
+    double mr = 0.0, mi = 0.0;
+    for (int k = lane; k < Lp; k += 32) {
+      const double2 x = col[(size_t)cc * Lp + k];
+      mr = fmax(mr, fabs(x.x));
+      mi = fmax(mi, fabs(x.y));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, o));
+      mi = fmax(mi, __shfl_xor_sync(0xffffffffu, mi, o));
+    }
+    if (lane == 0) scl[2 * cc] = scale_of(mr), scl[2 * cc + 1] = scale_of(mi);
+  }
+}
+
+// Inverse.  One CTA per (nu, block of 4 mu, signal): its 16 complex columns
+// (4 mu x combos (+-m, +-nu)) are the rows 8 * (signal % 16) .. +7 of the
+// stage images of the 4 pairs.  Staging: warp <-> (n = +-nu, l), lanes <->
+// (mu, sign of m): two runs of 4 consecutive m (64 bytes) per (n, l).
+// Entries l < max(mu, nu, L0) are zero.
+__global__ void __launch_bounds__(256) slice_inv_kernel(SliceArgs a) {
+  extern __shared__ __align__(16) double2 colbuf[];  // [4 mu][4 combos][Lp]
+  __shared__ double scl[4][2 * 4];
+  const int Lp = a.nchunk * kKC, L = a.L;
+  const int nu = blockIdx.x % a.N, mu0 = (blockIdx.x / a.N) * 4, sig = blockIdx.y;
+  const int grp = sig / kSig, b = sig % kSig;
+  {
+    // thread <-> (j, combo) fixed (m fastest across lanes), l = l0 + 16 i;
+    // 8 loads in flight per thread
+    const int j = threadIdx.x & 3, combo = (threadIdx.x >> 2) & 3, l0 = threadIdx.x >> 4;
+    const int mu = mu0 + j, ms = (combo & 1) ? -1 : 1, ns = (combo & 2) ? -1 : 1;
+    const int m = ms * mu, n = ns * nu;
+    const bool act = mu < L && sig < a.nsig && !(ms < 0 && mu == 0) && !(ns < 0 && nu == 0) &&
+                     !plane_skipped(a.n_mode, a.N, n);
+    const int lmin = max(max(mu, nu), a.L0);
+    const bool flip = ms * ns < 0;
+    const double2* src = act ? a.flmn[sig] + a.base[a.plane0 + n] + m : nullptr;
+    double2* dst = colbuf + (size_t)(j * 4 + combo) * Lp;
+    for (int l1 = l0; l1 < Lp; l1 += 16 * 8) {
+      double2 x[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int l = l1 + 16 * u;
+        x[u] = (act && l < L && l >= lmin) ? __ldg(src + (long long)l * l + l) : make_double2(0.0, 0.0);
+      }
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int l = l1 + 16 * u;
+        if (l >= Lp) break;
+        double f = (2.0 * l + 1.0) * kInv8Pi2;
+        if (flip && (l & 1)) f = -f;
+        dst[l] = make_double2(x[u].x * f, x[u].y * f);
+      }
+    }
+  }
+  __syncthreads();
+  // scales: column (j, combo) -> scl[j][2 combo + part]
+  column_scales(colbuf, Lp, &scl[0][0]);
+  __syncthreads();
+  for (int j = 0; j < 4; j++) {
+    const int mu = mu0 + j;
+    if (mu >= L) break;
+    const size_t gp = (size_t)grp * a.npairs + (size_t)mu * a.N + nu;
+    if (threadIdx.x < 8) a.xscale[gp * kM + 8 * b + threadIdx.x] = scl[j][threadIdx.x];
+  }
+  // digits: pairs handled one after another (8 real columns each)
+  for (int w = threadIdx.x; w < 4 * 8 * (Lp / 16); w += blockDim.x) {
+    const int c = w & 7, j = (w >> 3) & 3, kb = w >> 5;
+    const int mu = mu0 + j;
+    if (mu >= L) continue;
+    const int combo = c >> 1, part = c & 1;
+    const double inv = 1.0 / scl[j][c];
+    const double2* col = colbuf + (size_t)(j * 4 + combo) * Lp;
+    uint32_t d[4][kS];
+#pragma unroll
+    for (int qd = 0; qd < 4; qd++) {
+      double r[4];
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const double2 x = col[16 * kb + 4 * qd + e];
+        r[e] = (part ? x.y : x.x) * inv;
+      }
+      split_pack4(r, d[qd]);
+    }
+    const size_t gp = (size_t)grp * a.npairs + (size_t)mu * a.N + nu;
+    uint8_t* dst = a.xs + gp * (size_t)a.nchunk * kXStage + (size_t)(kb >> 2) * kXStage +
+                   tile_off(kM, 8 * b + c, (kb & 3) * 16);
+#pragma unroll
+    for (int i = 0; i < kS; i++)
+      *reinterpret_cast<uint4*>(dst + i * (kM * kKC)) = make_uint4(d[0][i], d[1][i], d[2][i], d[3][i]);
+  }
+}
+
+// Forward.  One CTA per (pair, 4 signals): complex columns cc = 4 * signal +
+// combo (rows 32 q .. 32 q + 31 of the pair's stage image for signals
+// 4q .. 4q+3 of the group); warp <-> column, lanes along m' (512-byte runs).
+__global__ void __launch_bounds__(256) slice_fwd_kernel(SliceArgs a) {
+  extern __shared__ __align__(16) double2 colbuf[];  // [16 columns][Lp]
+  __shared__ double scl[2 * kSliceCols];
+  const int Lp = a.nchunk * kKC, L = a.L;
+  const int pair = blockIdx.x, q4 = blockIdx.y;  // q4: quarter of all signals (4 each)
+  const int nu = pair % a.N, mu = pair / a.N;
+  const int grp = (4 * q4) / kSig, qin = q4 % (kSig / 4);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int cc = warp; cc < kSliceCols; cc += 8) {
+    const int sig = 4 * q4 + (cc >> 2), combo = cc & 3;
+    const int ms = (combo & 1) ? -1 : 1, ns = (combo & 2) ? -1 : 1;
+    const int m = ms * mu, n = ns * nu;
+    const bool act = sig < a.nsig && !(ms < 0 && mu == 0) && !(ns < 0 && nu == 0) && !plane_skipped(a.n_mode, a.N, n);
+    const bool flip = ms * ns < 0;
+    const double2* src =
+        act ? a.W + (long long)sig * a.wstride + (long long)(a.plane0 + n) * a.QS + (long long)(m + L - 1) * a.CS
+            : nullptr;
+    for (int k1 = lane; k1 < Lp; k1 += 32 * 8) {  // 8 loads in flight per lane
+      double2 x[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int k = k1 + 32 * u;
+        x[u] = (act && k < L) ? __ldg(src + k) : make_double2(0.0, 0.0);
+      }
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int k = k1 + 32 * u;
+        if (k >= Lp) break;
+        colbuf[(size_t)cc * Lp + k] = (flip && (k & 1)) ? make_double2(-x[u].x, -x[u].y) : x[u];
+      }
+    }
+  }
+  __syncthreads();
+  column_scales(colbuf, Lp, scl);
+  __syncthreads();
+  const size_t gp = (size_t)grp * a.npairs + pair;
+  if (threadIdx.x < 2 * kSliceCols) a.xscale[gp * kM + 32 * qin + threadIdx.x] = scl[threadIdx.x];
+  slice_from_smem(colbuf, Lp, scl, a.xs + gp * (size_t)a.nchunk * kXStage, 32 * qin);
 }
 
 // One CTA per pair: every stored block of the pair, generated exactly as the
@@ -886,7 +1069,15 @@ int launch_mixed_inverse(const Geometry& g, int n_mode, const double2* const* fl
   if (int rc = mixed_args(g, n_mode, nsig, scratch, &m, &sa)) return rc;
   sa.flmn = flmn_dev;
   sa.base = bases;
-  slice_kernel<false><<<dim3((unsigned)sa.npairs, (nsig + kSig - 1) / kSig), 256, 0, s>>>(sa);
+  const int slice_smem = 16 * (int)sizeof(double2) * nchunks(g) * kKC;  // 16 columns x Lp entries
+  if (slice_smem <= kSliceSmemMax) {
+    SO3G_CUDA(cudaFuncSetAttribute(slice_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, slice_smem));
+    // every signal of the last group (zeros past nsig), so the group's stage images are complete
+    slice_inv_kernel<<<dim3((unsigned)(g.N * ((g.L + 3) / 4)), (unsigned)(((nsig + kSig - 1) / kSig) * kSig)), 256,
+                       slice_smem, s>>>(sa);
+  } else {
+    slice_kernel<false><<<dim3((unsigned)sa.npairs, (nsig + kSig - 1) / kSig), 256, 0, s>>>(sa);
+  }
   SO3G_LAUNCHED();
   SO3G_CUDA(cudaGetLastError());
   m.dl = dl;
@@ -907,7 +1098,14 @@ int launch_mixed_forward(const Geometry& g, int n_mode, const double2* W, long l
   sa.W = W + g.QOFF;
   sa.wstride = wstride;
   sa.base = bases;
-  slice_kernel<true><<<dim3((unsigned)sa.npairs, (nsig + kSig - 1) / kSig), 256, 0, s>>>(sa);
+  const int slice_smem = 16 * (int)sizeof(double2) * nchunks(g) * kKC;
+  if (slice_smem <= kSliceSmemMax) {
+    SO3G_CUDA(cudaFuncSetAttribute(slice_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, slice_smem));
+    slice_fwd_kernel<<<dim3((unsigned)sa.npairs, (unsigned)(((nsig + kSig - 1) / kSig) * (kSig / 4))), 256,
+                       slice_smem, s>>>(sa);
+  } else {
+    slice_kernel<true><<<dim3((unsigned)sa.npairs, (nsig + kSig - 1) / kSig), 256, 0, s>>>(sa);
+  }
   SO3G_LAUNCHED();
   SO3G_CUDA(cudaGetLastError());
   m.dl = dl;

@@ -684,6 +684,276 @@ __global__ void __launch_bounds__(256) slice_fwd_kernel(SliceArgs a) {
   slice_from_smem(colbuf, Lp, scl, a.xs + gp * (size_t)a.nchunk * kXStage, 32 * qin);
 }
 
+// ---------------------------------------------------------------- persistent form
+// With the resident digit table, the products run as a persistent kernel:
+// one CTA per SM walks the work items (pair, output tile, signal group) with
+// a stride of the grid size.  The bulk-copy thread runs ahead across item
+// boundaries through the 2-stage ring; the MMA thread starts an item as soon
+// as the epilogue has drained the accumulators of the previous one (mbarrier
+// acce, 256 arrivals), so the epilogue's FP64 combination and global stores
+// overlap the next item's products.
+struct __align__(16) TcpSmem {
+  uint8_t X[kStages][kXStage];
+  uint8_t A[kStages][kAStage];
+  unsigned long long full[kStages];
+  unsigned long long empty[kStages];
+  unsigned long long accf;  // accumulators complete (tcgen05.commit)
+  unsigned long long acce;  // accumulators drained (epilogue threads)
+  uint32_t tmem_base;
+};
+
+struct ItemC {  // one contraction work item
+  int mu, nu, t, grp, kc0, nk, lmin;
+};
+
+template <bool FWD>
+__device__ __forceinline__ ItemC decode_item(const MixArgs& a, int item) {
+  ItemC it;
+  const int per = a.L * a.N * a.MT;
+  const int bx = item % per;
+  it.grp = item / per;
+  it.nu = bx % a.N;
+  const int rest = bx / a.N;
+  it.t = rest % a.MT;
+  it.mu = rest / a.MT;
+  const int r0 = it.t * kN;
+  it.lmin = max(max(it.mu, it.nu), a.L0);
+  if (FWD) {
+    const bool any_row = r0 + kN > it.lmin && r0 < a.L;
+    it.kc0 = 0;
+    it.nk = any_row ? (min(a.L, r0 + kN) + kKC - 1) / kKC : 0;
+  } else {
+    const int kstart = max(it.lmin, r0) & ~(kKC - 1);
+    it.kc0 = kstart / kKC;
+    it.nk = kstart < a.L ? (a.L - kstart + kKC - 1) / kKC : 0;
+  }
+  return it;
+}
+
+// Sum of the 7 diagonals of 8 accumulator columns, as FP64 (weight w0 on
+// diagonal 0, then / 128 per diagonal).  PAIRED (reductions of at most 512
+// entries): diagonals (1,2), (3,4), (5,6) are first folded exactly in int32
+// as 128 acc_d + acc_{d+1} (|digit products| <= 64 * 64, so the largest
+// folded sum, 64 * 64 * 512 * (6 * 128 + 7), stays below 2^31), leaving 4
+// conversions and 4 FMAs per value instead of 7 and 7.
+template <bool PAIRED>
+__device__ __forceinline__ void drain8(uint32_t taddr, double w0, double (&v)[8]) {
+  int acc[kND][8];
+#pragma unroll
+  for (int d = 0; d < kND; d++) tc::tmem_ld8(taddr + (uint32_t)(kN * d), acc[d]);
+  tc::tmem_wait_ld();
+#pragma unroll
+  for (int e = 0; e < 8; e++) v[e] = 0.0;
+  if (PAIRED) {
+    const double w1 = w0 * 0.00006103515625;  // 2^{-14}: pair (1, 2) in units of diagonal 2
+#pragma unroll
+    for (int e = 0; e < 8; e++) {
+      v[e] = fma(int_to_double(acc[0][e]), w0, v[e]);
+      v[e] = fma(int_to_double(acc[1][e] * 128 + acc[2][e]), w1, v[e]);
+      v[e] = fma(int_to_double(acc[3][e] * 128 + acc[4][e]), w1 * 0.00006103515625, v[e]);
+      v[e] = fma(int_to_double(acc[5][e] * 128 + acc[6][e]), w1 * 0.0000000037252902984619140625, v[e]);
+    }
+  } else {
+    double wd = w0;
+#pragma unroll
+    for (int d = 0; d < kND; d++) {
+#pragma unroll
+      for (int e = 0; e < 8; e++) v[e] = fma(int_to_double(acc[d][e]), wd, v[e]);
+      wd *= 0.0078125;
+    }
+  }
+}
+
+// Issue of one item's products from the ring (G: running chunk counter).
+template <bool MNB>
+__device__ __forceinline__ void issue_item(TcpSmem& S, uint32_t tbase, int nk, int& G) {
+  const uint32_t full0 = tc::smem_u32(&S.full[0]), empty0 = tc::smem_u32(&S.empty[0]);
+  constexpr uint32_t idesc = tc::idesc_s8(kM, kN) | (MNB ? (1u << 16) : 0u);
+  for (int k = 0; k < nk; k++, G++) {
+    const int st = G & 1;
+    tc::mbar_wait(full0 + 8 * st, (G >> 1) & 1, &g_tc_error, 2);
+    tc::tc_fence_after();
+    const uint32_t xb = tc::smem_u32(&S.X[st][0]), ab = tc::smem_u32(&S.A[st][0]);
+#pragma unroll
+    for (int ks = 0; ks < kKC / 32; ks++) {
+#pragma unroll
+      for (int i = 0; i < kS; i++) {
+        const uint64_t ad = tc::smem_desc(xb + i * (kM * kKC) + ks * 2 * (kM * 16), kM * 16, 128);
+#pragma unroll
+        for (int j = 0; j + i < kND; j++) {
+          const uint64_t bd = MNB ? tc::smem_desc(ab + j * (kN * kKC) + ks * 512, 128, 1024)
+                                  : tc::smem_desc(ab + j * (kN * kKC) + ks * 2 * (kN * 16), kN * 16, 128);
+          tc::mma_i8(tbase + (uint32_t)(kN * (i + j)), ad, bd, idesc, (k | ks | i) != 0);
+        }
+      }
+    }
+    tc::mma_commit(empty0 + 8 * st);
+  }
+}
+
+__device__ __forceinline__ void load_chunk(TcpSmem& S, int& G, const uint8_t* xsrc, const uint8_t* asrc) {
+  const uint32_t full0 = tc::smem_u32(&S.full[0]), empty0 = tc::smem_u32(&S.empty[0]);
+  const int st = G & 1;
+  if (G >= kStages) tc::mbar_wait(empty0 + 8 * st, ((G >> 1) - 1) & 1, &g_tc_error, 2);
+  tc::mbar_arrive_expect_tx(full0 + 8 * st, kXStage + kAStage);
+  tc::bulk_g2s(tc::smem_u32(&S.X[st][0]), xsrc, kXStage, full0 + 8 * st);
+  tc::bulk_g2s(tc::smem_u32(&S.A[st][0]), asrc, kAStage, full0 + 8 * st);
+  G++;
+}
+
+__device__ __forceinline__ void tcp_setup(TcpSmem& S, int tid, int warp) {
+  if (tid == 0) {
+    for (int st = 0; st < kStages; st++) {
+      tc::mbar_init(tc::smem_u32(&S.full[st]), 1);
+      tc::mbar_init(tc::smem_u32(&S.empty[st]), 1);
+    }
+    tc::mbar_init(tc::smem_u32(&S.accf), 1);
+    tc::mbar_init(tc::smem_u32(&S.acce), kGen);
+    tc::mbar_fence_init();
+  }
+  if (warp == 0) tc::tmem_alloc(tc::smem_u32(&S.tmem_base), kTmemCols);
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+}
+
+__device__ __forceinline__ void tcp_teardown(TcpSmem& S, int warp) {
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    __syncwarp();
+    tc::tc_fence_after();
+    tc::tmem_dealloc(S.tmem_base, kTmemCols);
+  }
+}
+
+// Epilogue drain of one item: the thread's 32 output rows (4 groups of 8)
+// combined into v, then the accumulators are released.
+__device__ __forceinline__ void drain_item(TcpSmem& S, int lq, int ch, double w0, bool paired, int& ia,
+                                           double (&v)[4][8]) {
+  tc::mbar_wait(tc::smem_u32(&S.accf), ia & 1, &g_tc_error, 2);
+  tc::tc_fence_after();
+#pragma unroll
+  for (int g = 0; g < 4; g++) {
+    __syncwarp();
+    const uint32_t ta = S.tmem_base + ((uint32_t)(32 * lq) << 16) + (uint32_t)(32 * ch + 8 * g);
+    if (paired)
+      drain8<true>(ta, w0, v[g]);
+    else
+      drain8<false>(ta, w0, v[g]);
+  }
+  tc::tc_fence_before();
+  tc::mbar_arrive(tc::smem_u32(&S.acce));
+  ia++;
+}
+
+template <bool FWD>
+__global__ void __launch_bounds__(kThreads, 1) mixed_tcp_kernel(MixArgs a, int nitems) {
+  extern __shared__ __align__(1024) unsigned char smraw[];
+  TcpSmem& S = *reinterpret_cast<TcpSmem*>(smraw);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (*reinterpret_cast<volatile int*>(&g_tc_error)) return;
+  tcp_setup(S, tid, warp);
+  if (warp == 0) {
+    if (lane == 0) {
+      int G = 0, ia = 0;
+      for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const ItemC it = decode_item<FWD>(a, item);
+        if (it.nk == 0) continue;
+        if (ia > 0) tc::mbar_wait(tc::smem_u32(&S.acce), (ia - 1) & 1, &g_tc_error, 2);
+        tc::tc_fence_after();
+        issue_item<FWD>(S, S.tmem_base, it.nk, G);
+        tc::mma_commit(tc::smem_u32(&S.accf));
+        ia++;
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      int G = 0;
+      for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const ItemC it = decode_item<FWD>(a, item);
+        if (it.nk == 0) continue;
+        const size_t gp = (size_t)it.grp * a.L * a.N + (size_t)it.mu * a.N + it.nu;
+        const uint8_t* xs = a.xs + gp * (size_t)a.nchunk * kXStage;
+        const int q = max(it.mu, it.nu) / kKC;
+        const uint8_t* tb = a.tab + (size_t)a.pair_off[(size_t)it.mu * a.N + it.nu] * kAStage;
+        for (int k = 0; k < it.nk; k++) {
+          const long long blk = FWD ? digit_block(k, it.t, q, a.nchunk) : digit_block(it.t, it.kc0 + k, q, a.nchunk);
+          load_chunk(S, G, xs + (size_t)(it.kc0 + k) * kXStage, tb + blk * kAStage);
+        }
+      }
+    }
+  } else {
+    const int gw = warp - 2, lq = warp & 3, ch = gw >> 2;
+    const int c = 32 * lq + lane;
+    const int b = c >> 3, combo = (c >> 1) & 3, part = c & 1;
+    const int ms = (combo & 1) ? -1 : 1, ns = (combo & 2) ? -1 : 1;
+    const bool paired = a.nchunk * kKC <= 512;
+    int ia = 0;
+    for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+      const ItemC it = decode_item<FWD>(a, item);
+      // per-item metadata first: these loads overlap the wait for the products
+      const int mu = it.mu, nu = it.nu, L = a.L, r0 = it.t * kN;
+      const bool valid_combo = !((ms < 0 && mu == 0) || (ns < 0 && nu == 0));
+      const int m = ms * mu, n = ns * nu;
+      const int sig = it.grp * kSig + b;
+      const bool one_neg = ms * ns < 0;
+      const double sgn_mn = ((mu + nu) & 1) ? -1.0 : 1.0;
+      const size_t gp = (size_t)it.grp * a.L * a.N + (size_t)mu * a.N + nu;
+      const double scale = a.xscale[gp * kM + c];
+      const bool skipped = FWD && plane_skipped(a.n_mode, a.N, n);
+      double2* Wout = nullptr;
+      double2* F = nullptr;
+      long long blk = 0;
+      if (!FWD) Wout = a.W + (long long)sig * a.wstride + (long long)(a.plane0 + n) * a.QS + (long long)(m + L - 1) * a.CS;
+      else if (sig < a.nsig) {
+        F = a.flmn[sig];
+        blk = a.base[a.plane0 + n];
+      }
+      double v[4][8];
+      if (it.nk > 0) {
+        drain_item(S, lq, ch, 2.0 * 0.000061035156250000000, paired, ia, v);  // A scale 2, 2^{-14}
+      } else {
+#pragma unroll
+        for (int g = 0; g < 4; g++)
+#pragma unroll
+          for (int e = 0; e < 8; e++) v[g][e] = 0.0;
+      }
+#pragma unroll
+      for (int g = 0; g < 4; g++) {
+        const int col = 32 * ch + 8 * g;
+        double re[4], im[4];
+#pragma unroll
+        for (int qq = 0; qq < 4; qq++) {
+          const double send = (part ? v[g][qq] : v[g][4 + qq]) * scale;
+          const double recv = __shfl_xor_sync(0xffffffffu, send, 1);
+          re[qq] = part ? recv : v[g][qq] * scale;
+          im[qq] = part ? v[g][4 + qq] * scale : recv;
+        }
+        if (!valid_combo || sig >= a.nsig || skipped) continue;
+#pragma unroll
+        for (int qq = 0; qq < 4; qq++) {
+          const int row = r0 + col + 4 * part + qq;
+          if (row >= L) continue;
+          const double sgn = (one_neg && (row & 1)) ? -sgn_mn : sgn_mn;
+          double2 val = make_double2(re[qq] * sgn, im[qq] * sgn);
+          if (!FWD) {
+            Wout[row] = ipow(val, n - m + 4 * L);
+          } else {
+            const int lr = row;
+            if (mu > lr) continue;
+            if (a.compact && lr < nu) continue;
+            if (lr < it.lmin) val = make_double2(0.0, 0.0);
+            else val = ipow(val, m - n + 4 * L);
+            F[blk + (long long)lr * lr + lr + m] = val;
+          }
+        }
+      }
+    }
+  }
+  tcp_teardown(S, warp);
+}
+
 // One CTA per pair: every stored block of the pair, generated exactly as the
 // inverse kernel's producer warps generate a stage (8 warps of 32 lanes).
 __global__ void __launch_bounds__(256) digit_table_kernel(MixArgs a, uint8_t* tab) {
@@ -829,127 +1099,77 @@ __global__ void __launch_bounds__(256) beta_slice_kernel(BetaArgs a) {
   }
 }
 
-// One CTA per (column tile, 64-row tile of m', signal): D_d[c, m'] over the
-// L beta samples in chunks of 64, both operands streamed by bulk copies.
-__global__ void __launch_bounds__(kThreads, 1) beta_tc_kernel(BetaArgs a) {
+// Persistent: one CTA per SM walks the items (column tile, 64-row tile of
+// m', signal), column tiles fastest; D_d[c, m'] over the L beta samples in
+// chunks of 64, both operands streamed by bulk copies.
+__global__ void __launch_bounds__(kThreads, 1) beta_tc_kernel(BetaArgs a, int ntiles, int nitems) {
   extern __shared__ __align__(1024) unsigned char smraw[];
-  TcSmem& S = *reinterpret_cast<TcSmem*>(smraw);
+  TcpSmem& S = *reinterpret_cast<TcpSmem*>(smraw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int tile = blockIdx.x, t = blockIdx.y, sig = blockIdx.z;
-  const int ct = tile % a.ct, sc = (tile / a.ct) & 1, p = tile / (2 * a.ct);
-  const int n = p - a.plane0, L = a.L, r0 = t * kN, nk = a.nchunk;
-  const size_t gt = (size_t)sig * gridDim.x + tile;
-  const uint8_t* xs = a.xs + gt * (size_t)nk * kXStage;
-  const uint8_t* tb = a.tab + (size_t)(sc * a.MT + t) * nk * kAStage;
+  const int nk = a.nchunk, L = a.L;
   if (*reinterpret_cast<volatile int*>(&g_tc_error)) return;
-
-  const uint32_t full0 = tc::smem_u32(&S.full[0]), empty0 = tc::smem_u32(&S.empty[0]);
-  const uint32_t accum = tc::smem_u32(&S.accum);
-  if (tid == 0) {
-    for (int st = 0; st < kStages; st++) {
-      tc::mbar_init(full0 + 8 * st, 1);
-      tc::mbar_init(empty0 + 8 * st, 1);
-    }
-    tc::mbar_init(accum, 1);
-    tc::mbar_fence_init();
-  }
-  if (warp == 0) tc::tmem_alloc(tc::smem_u32(&S.tmem_base), kTmemCols);
-  tc::tc_fence_before();
-  __syncthreads();
-  tc::tc_fence_after();
-  const uint32_t tbase = S.tmem_base;
-
+  tcp_setup(S, tid, warp);
   if (warp == 0) {
     if (lane == 0) {
-      constexpr uint32_t idesc = tc::idesc_s8(kM, kN);
-      for (int k = 0; k < nk; k++) {
-        const int st = k & 1;
-        tc::mbar_wait(full0 + 8 * st, (k >> 1) & 1, &g_tc_error, 2);
+      int G = 0, ia = 0;
+      for (int item = blockIdx.x; item < nitems; item += gridDim.x, ia++) {
+        if (ia > 0) tc::mbar_wait(tc::smem_u32(&S.acce), (ia - 1) & 1, &g_tc_error, 2);
         tc::tc_fence_after();
-        const uint32_t xb = tc::smem_u32(&S.X[st][0]), ab = tc::smem_u32(&S.A[st][0]);
-#pragma unroll
-        for (int ks = 0; ks < kKC / 32; ks++) {
-#pragma unroll
-          for (int i = 0; i < kS; i++) {
-            const uint64_t ad = tc::smem_desc(xb + i * (kM * kKC) + ks * 2 * (kM * 16), kM * 16, 128);
-#pragma unroll
-            for (int jj = 0; jj + i < kND; jj++) {
-              const uint64_t bd = tc::smem_desc(ab + jj * (kN * kKC) + ks * 2 * (kN * 16), kN * 16, 128);
-              tc::mma_i8(tbase + (uint32_t)(kN * (i + jj)), ad, bd, idesc, (k | ks | i) != 0);
-            }
-          }
-        }
-        tc::mma_commit(empty0 + 8 * st);
+        issue_item<false>(S, S.tmem_base, nk, G);
+        tc::mma_commit(tc::smem_u32(&S.accf));
       }
-      tc::mma_commit(accum);
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      for (int k = 0; k < nk; k++) {
-        const int st = k & 1;
-        if (k >= kStages) tc::mbar_wait(empty0 + 8 * st, ((k >> 1) - 1) & 1, &g_tc_error, 2);
-        tc::mbar_arrive_expect_tx(full0 + 8 * st, kXStage + kAStage);
-        tc::bulk_g2s(tc::smem_u32(&S.X[st][0]), xs + (size_t)k * kXStage, kXStage, full0 + 8 * st);
-        tc::bulk_g2s(tc::smem_u32(&S.A[st][0]), tb + (size_t)k * kAStage, kAStage, full0 + 8 * st);
+      int G = 0;
+      for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const int tile = item % ntiles, rest = item / ntiles, t = rest % a.MT, sig = rest / a.MT;
+        const int sc = (tile / a.ct) & 1;
+        const size_t gt = (size_t)sig * ntiles + tile;
+        const uint8_t* xs = a.xs + gt * (size_t)nk * kXStage;
+        const uint8_t* tb = a.tab + (size_t)(sc * a.MT + t) * nk * kAStage;
+        for (int k = 0; k < nk; k++) load_chunk(S, G, xs + (size_t)k * kXStage, tb + (size_t)k * kAStage);
       }
     }
   } else {
-    // epilogue: thread <-> TMEM lane c = 2 j + part, 32 output rows m'
     const int gw = warp - 2, lq = warp & 3, ch = gw >> 2;
     const int c = 32 * lq + lane, j = c >> 1, part = c & 1;
-    const int m = beta_first_m(L, n, sc) + 2 * (64 * ct + j);
-    const bool active = m <= L - 1 && sig < a.nsig;
-    const double scale = a.xscale[gt * kM + c];
-    tc::mbar_wait(accum, 0, &g_tc_error, 2);
-    tc::tc_fence_after();
-    double2* out = a.Wc + (long long)sig * a.wstride + (long long)p * a.QS + (long long)(m + L - 1) * a.CS;
-#pragma unroll 1
-    for (int g = 0; g < 4; g++) {
-      __syncwarp();
-      const int col = 32 * ch + 8 * g;
-      double v[8];
+    int ia = 0;
+    for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+      const int tile = item % ntiles, rest = item / ntiles, t = rest % a.MT, sig = rest / a.MT;
+      const int ct = tile % a.ct, sc = (tile / a.ct) & 1, p = tile / (2 * a.ct);
+      const int n = p - a.plane0, r0 = t * kN;
+      const int m = beta_first_m(L, n, sc) + 2 * (64 * ct + j);
+      const bool active = m <= L - 1 && sig < a.nsig;
+      const size_t gt = (size_t)sig * ntiles + tile;
+      const double scale = a.xscale[gt * kM + c];
+      double v[4][8];
+      drain_item(S, lq, ch, a.rscale * 0.000061035156250000000, a.nchunk * kKC <= 512, ia, v);  // R scale x 2^{-14}
+      double2* out = a.Wc + (long long)sig * a.wstride + (long long)p * a.QS + (long long)(m + L - 1) * a.CS;
 #pragma unroll
-      for (int e = 0; e < 8; e++) v[e] = 0.0;
-      int acc[kND][8];
+      for (int g = 0; g < 4; g++) {
+        const int col = 32 * ch + 8 * g;
+        double re[4], im[4];
 #pragma unroll
-      for (int d = 0; d < kND; d++)
-        tc::tmem_ld8(tbase + ((uint32_t)(32 * lq) << 16) + (uint32_t)(kN * d + col), acc[d]);
-      tc::tmem_wait_ld();
-      double wd = a.rscale * 0.000061035156250000000;  // R scale x 2^{-14}: diagonal 0
+        for (int qq = 0; qq < 4; qq++) {
+          const double send = (part ? v[g][qq] : v[g][4 + qq]) * scale;
+          const double recv = __shfl_xor_sync(0xffffffffu, send, 1);
+          re[qq] = part ? recv : v[g][qq] * scale;
+          im[qq] = part ? v[g][4 + qq] * scale : recv;
+        }
+        if (!active) continue;
 #pragma unroll
-      for (int d = 0; d < kND; d++) {
-#pragma unroll
-        for (int e = 0; e < 8; e++) v[e] = fma(int_to_double(acc[d][e]), wd, v[e]);
-        wd *= 0.0078125;
-      }
-      double re[4], im[4];
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        const double send = part ? v[q] * scale : v[4 + q] * scale;
-        const double recv = __shfl_xor_sync(0xffffffffu, send, 1);
-        re[q] = part ? recv : v[q] * scale;
-        im[q] = part ? v[4 + q] * scale : recv;
-      }
-      if (!active) continue;
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        const int row = r0 + col + 4 * part + q;
-        if (row >= L) continue;
-        double2 val = make_double2(re[q], im[q]);
-        if (sc == 1 && row >= 1) val = make_double2(-val.y, val.x);  // times i
-        out[row] = val;
+        for (int qq = 0; qq < 4; qq++) {
+          const int row = r0 + col + 4 * part + qq;
+          if (row >= L) continue;
+          double2 val = make_double2(re[qq], im[qq]);
+          if (sc == 1 && row >= 1) val = make_double2(-val.y, val.x);  // times i
+          out[row] = val;
+        }
       }
     }
   }
-
-  if (warp == 0 && lane == 0) tc::mbar_wait(accum, 0, &g_tc_error, 2);
-  tc::tc_fence_before();
-  __syncthreads();
-  if (warp == 0) {
-    __syncwarp();
-    tc::tc_fence_after();
-    tc::tmem_dealloc(tbase, kTmemCols);
-  }
+  tcp_teardown(S, warp);
 }
 
 }  // namespace
@@ -1044,13 +1264,25 @@ int ensure_digit_table(Device* D, const Geometry& g, int method, const double* d
   return kOk;
 }
 
+// Streaming multiprocessors of the current device (persistent grids).
+static int sm_count() {
+  int dev = 0, n = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      n <= 0)
+    return 148;
+  return n;
+}
+
 template <bool FWD>
 static int launch_tc(const MixArgs& m, int nsig, cudaStream_t s) {
   const dim3 grid((unsigned)(m.L * m.N * m.MT), (nsig + kSig - 1) / kSig);
   const int smem = (int)sizeof(TcSmem);
   if (m.tab) {
-    SO3G_CUDA(cudaFuncSetAttribute(mixed_tc_kernel<FWD, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    mixed_tc_kernel<FWD, true><<<grid, kThreads, smem, s>>>(m);
+    const int psmem = (int)sizeof(TcpSmem);
+    const long long items = (long long)grid.x * grid.y;
+    if (items > 0x7fffffffLL) return fail(kUnsupported, "split-precision contraction: too many work items");
+    SO3G_CUDA(cudaFuncSetAttribute(mixed_tcp_kernel<FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, psmem));
+    mixed_tcp_kernel<FWD><<<(int)std::min<long long>(items, sm_count()), kThreads, psmem, s>>>(m, (int)items);
   } else {
     SO3G_CUDA(cudaFuncSetAttribute(mixed_tc_kernel<FWD, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     mixed_tc_kernel<FWD, false><<<grid, kThreads, smem, s>>>(m);
@@ -1201,9 +1433,12 @@ int launch_mixed_fwd_beta(const Geometry& g, double2* W, long long wstride, int 
   beta_slice_kernel<<<dim3((unsigned)tiles, (unsigned)nsig), 256, 0, s>>>(a);
   SO3G_LAUNCHED();
   SO3G_CUDA(cudaGetLastError());
-  const int smem = (int)sizeof(TcSmem);
+  const int smem = (int)sizeof(TcpSmem);
+  const long long items = (long long)tiles * a.MT * nsig;
+  if (items > 0x7fffffffLL) return fail(kUnsupported, "split-precision beta stage: too many work items");
   SO3G_CUDA(cudaFuncSetAttribute(beta_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  beta_tc_kernel<<<dim3((unsigned)tiles, (unsigned)a.MT, (unsigned)nsig), kThreads, smem, s>>>(a);
+  const int grid = (int)std::min<long long>(items, sm_count());
+  beta_tc_kernel<<<grid, kThreads, smem, s>>>(a, tiles, (int)items);
   SO3G_LAUNCHED();
   SO3G_CUDA(cudaGetLastError());
   return kOk;

@@ -704,18 +704,48 @@ struct __align__(16) TcpSmem {
 
 struct ItemC {  // one contraction work item
   int mu, nu, t, grp, kc0, nk, lmin;
+  bool valid;  // false: padding item past the band limit (no products, no output)
 };
+
+// Item order.  Inverse: (group, mu, tile, nu), nu fastest (the CTAs in
+// flight share mu rows of the digit table and one mu's operands).  Forward:
+// (group, nu, block of 16 mu, tile, mu), mu fastest: the coefficients
+// (l, +-mu) and (l, +-(mu+1)) share 32-byte sectors of the caller's flmn, and
+// CTAs that run at the same time write both halves; one block's operands
+// (16 pairs) stay in L2 across its tiles.
+constexpr int kMuBlock = 16;
+__host__ __device__ inline long long mixed_items(int L, int N, int MT, int groups, bool fwd) {
+  return fwd ? (long long)kMuBlock * MT * ((L + kMuBlock - 1) / kMuBlock) * N * groups : (long long)L * N * MT * groups;
+}
 
 template <bool FWD>
 __device__ __forceinline__ ItemC decode_item(const MixArgs& a, int item) {
   ItemC it;
-  const int per = a.L * a.N * a.MT;
-  const int bx = item % per;
-  it.grp = item / per;
-  it.nu = bx % a.N;
-  const int rest = bx / a.N;
-  it.t = rest % a.MT;
-  it.mu = rest / a.MT;
+  if (FWD) {
+    const int mi = item % kMuBlock;
+    int r = item / kMuBlock;
+    it.t = r % a.MT;
+    r /= a.MT;
+    const int nmb = (a.L + kMuBlock - 1) / kMuBlock;
+    const int mb = r % nmb;
+    r /= nmb;
+    it.nu = r % a.N;
+    it.grp = r / a.N;
+    it.mu = mb * kMuBlock + mi;
+    if (it.mu >= a.L) {  // past the band limit: no work
+      it.mu = a.L - 1, it.kc0 = 0, it.nk = 0, it.lmin = a.L, it.valid = false;
+      return it;
+    }
+  } else {
+    const int per = a.L * a.N * a.MT;
+    const int bx = item % per;
+    it.grp = item / per;
+    it.nu = bx % a.N;
+    const int rest = bx / a.N;
+    it.t = rest % a.MT;
+    it.mu = rest / a.MT;
+  }
+  it.valid = true;
   const int r0 = it.t * kN;
   it.lmin = max(max(it.mu, it.nu), a.L0);
   if (FWD) {
@@ -892,6 +922,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_tcp_kernel(MixArgs a, int n
     int ia = 0;
     for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
       const ItemC it = decode_item<FWD>(a, item);
+      if (!it.valid) continue;
       // per-item metadata first: these loads overlap the wait for the products
       const int mu = it.mu, nu = it.nu, L = a.L, r0 = it.t * kN;
       const bool valid_combo = !((ms < 0 && mu == 0) || (ns < 0 && nu == 0));
@@ -1279,7 +1310,7 @@ static int launch_tc(const MixArgs& m, int nsig, cudaStream_t s) {
   const int smem = (int)sizeof(TcSmem);
   if (m.tab) {
     const int psmem = (int)sizeof(TcpSmem);
-    const long long items = (long long)grid.x * grid.y;
+    const long long items = mixed_items(m.L, m.N, m.MT, (int)grid.y, FWD);
     if (items > 0x7fffffffLL) return fail(kUnsupported, "split-precision contraction: too many work items");
     SO3G_CUDA(cudaFuncSetAttribute(mixed_tcp_kernel<FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, psmem));
     mixed_tcp_kernel<FWD><<<(int)std::min<long long>(items, sm_count()), kThreads, psmem, s>>>(m, (int)items);

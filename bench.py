@@ -49,6 +49,9 @@ def args_():
     ap.add_argument("--N", type=int, default=64)
     ap.add_argument("--batch", type=int, default=16,
                     help="signals per split-precision step (0: time the FP64 path only)")
+    ap.add_argument("--serve", type=int, default=400,
+                    help="requests of the serving-trace sample (0: skip the serving leg)")
+    ap.add_argument("--serve-rate", type=float, default=60.0, help="offered request rate of the serving leg (1/s)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
@@ -368,6 +371,8 @@ def run_ours(a):
             err_fl = max(err_fl, float(((backs[i] - ref).abs().max() / ref.abs().max()).item()))
             err_rt = max(err_rt, float(((backs[i] - fls[i]).abs().max() / fls[i].abs().max()).item()))
             del ref
+        del fls, fs, backs  # release the batch before the end-to-end and serving legs
+        torch.cuda.empty_cache()
         mixed = {"value": mixed_value, "unit": UNIT, "batch": B, "ms_per_step": rmx["total_ms"] / a.steps,
                  "over_fp64": mixed_value / fp64_value,
                  "rel_err_vs_fp64": {"samples": err_f, "coefficients": err_fl, "max": max(err_f, err_fl)},
@@ -410,9 +415,21 @@ def run_ours(a):
     # ---- end to end through the drop-in C ABI with host buffers
     e2e = None
     if not a.no_e2e:
-        del fls, fs, backs
-        torch.cuda.empty_cache()
         e2e = run_e2e(so3, p, fl_host, a.steps, local, world, None)
+
+    # ---- serving: a sample of the request trace (inverse 60 % / forward 40 %, complex MW, L log-uniform
+    # in [16, 1024], N uniform in [1, min(L, 64)], U(-1,1) inputs, Poisson arrivals), FP64 and split
+    serving = None
+    if a.serve > 0:
+        from so3_b200 import serve as sserve
+        ctx.close()  # the batch workspace
+        del d_flmn, d_f
+        torch.cuda.empty_cache()
+        serving = {"trace": f"{a.serve} requests, seed {rank + 11}, Poisson {a.serve_rate:g}/s offered, "
+                            f"L log-uniform [16, 1024], N uniform [1, min(L, 64)], 60% inverse / 40% forward, "
+                            f"complex MW, 120 GB budget, 8 slots, batches of up to 8"}
+        for prec in ("fp64", "mixed"):
+            serving[prec] = sserve.serving_run(a.serve, a.serve_rate, seed=rank + 11, precision=prec, device=local)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -445,6 +462,7 @@ def run_ours(a):
                 "latency_ms": {"p50": statistics.median(lat), "p99": pct(lat, 0.99)},
                 "stage_ms_per_transform": {k: round(v, 4) for k, v in per_signal.items()},
                 "gpu_launches": int(run["launches"]), "roofline": roof, "e2e": e2e, "cpu_baseline": cpu,
+                "serving": serving,
                 "clocks": run["clocks"]}
         print(json.dumps(line), flush=True)
     sdist.finalize()

@@ -38,9 +38,14 @@ static std::string tune_key(const so3_parameters_t& p, int real) {
          std::to_string(real);
 }
 
+// Threads that must not stop for tuning (the request server's worker) use
+// the default stage variants for geometries nobody has tuned yet.
+static thread_local bool t_no_autotune = false;
+void set_thread_autotune(bool on) { t_no_autotune = !on; }
+
 // Stage variants for this geometry: cached per device, else measured on the
-// workspace (skipped while s is being captured, and when the environment sets
-// SO3GPU_AUTOTUNE=0; defaults are used then).
+// workspace (skipped while s is being captured, on threads that disabled it,
+// and when the environment sets SO3GPU_AUTOTUNE=0; defaults are used then).
 static int ensure_tuned(Device* D, const so3_parameters_t& p, int real, Resources* r, double2* W, cudaStream_t s) {
   const std::string key = tune_key(p, real);
   {
@@ -51,6 +56,7 @@ static int ensure_tuned(Device* D, const so3_parameters_t& p, int real, Resource
       return kOk;
     }
   }
+  if (t_no_autotune) return kOk;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   SO3G_CUDA(cudaStreamIsCapturing(s, &cs));
   if (cs != cudaStreamCaptureStatusNone) return kOk;
@@ -441,7 +447,8 @@ int run_forward_batch(Device* D, Workspace* wk, const so3_parameters_t& p, int r
   int rc;
   const long long wstride = (long long)(bl.wbytes / sizeof(double2));
   // forward beta stage: one tensor-core product over the whole batch where
-  // supported (complex MW), else the FP64 DFT + weight convolution per signal
+  // supported (complex MW) and its matrix table is resident, else the FP64
+  // DFT + weight convolution per signal
   const BetaTable* bt = nullptr;
   if (mixed_beta_supported(r.g) && (rc = ensure_beta_table(D, r.g, s, &bt))) return rc;
   for (int b = 0; b < nsig; b++) {

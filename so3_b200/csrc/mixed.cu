@@ -1246,11 +1246,14 @@ size_t digit_table_bytes(int L, int N) {
   return blocks * kAStage;
 }
 
-// Resident digit tables, one per (L, N, Delta recursion), built on first use
-// when it fits: at most a quarter of the device memory in total and 4 GiB
-// of free memory left after it (SO3GPU_DIGIT_TABLE=0 disables them).  Tables
-// are kept until the process exits, so streams that use one never see it
-// change.  Without a table the kernels generate the digits from Delta.
+// Resident digit tables, one per (L, N, Delta recursion), built on the
+// second split-precision call of that geometry (a geometry seen once, as in a
+// request trace of varied band limits, never pays for a table) when it fits:
+// at most a quarter of the device memory in total and 4 GiB of free memory
+// left after it (SO3GPU_DIGIT_TABLE=0 disables them, =1 builds on first
+// use).  Tables are kept until the process exits, so streams that use one
+// never see it change.  Without a table the kernels generate the digits from
+// Delta.
 int ensure_digit_table(Device* D, const Geometry& g, int method, const double* dl, cudaStream_t s,
                        const DigitTable** out) {
   *out = nullptr;
@@ -1262,6 +1265,8 @@ int ensure_digit_table(Device* D, const Geometry& g, int method, const double* d
       *out = t.get();
       return kOk;
     }
+  const long long key = ((long long)g.L << 20) ^ ((long long)g.N << 2) ^ method;
+  if (++D->digit_uses[key] < 2 && !(env && env[0] == '1')) return kOk;
   const size_t bytes = digit_table_bytes(g.L, g.N);
   size_t used = 0;
   for (const auto& t : D->digit_tables) used += t->bytes;
@@ -1403,7 +1408,10 @@ static void split_host(double r, uint8_t* q) {
   }
 }
 
-// Resident digits of R_s for this L (MW), one table per device and L.
+// Resident digits of R_s for this L (MW), one table per device and L, built
+// on the second split-precision forward call of that L (the first runs the
+// FP64 beta stage, so a band limit seen once never pays for the build);
+// SO3GPU_DIGIT_TABLE=1 builds on first use.
 int ensure_beta_table(Device* D, const Geometry& g, cudaStream_t s, const BetaTable** out) {
   *out = nullptr;
   std::lock_guard<std::mutex> lk(D->mu);
@@ -1412,6 +1420,8 @@ int ensure_beta_table(Device* D, const Geometry& g, cudaStream_t s, const BetaTa
       *out = t.get();
       return kOk;
     }
+  const char* env = getenv("SO3GPU_DIGIT_TABLE");
+  if (++D->beta_uses[g.L] < 2 && !(env && env[0] == '1')) return kOk;
   const int L = g.L, nc = nchunks(g), MT = nc;
   double* dR = nullptr;
   SO3G_CUDA(cudaMalloc(&dR, 2 * (size_t)L * L * sizeof(double)));

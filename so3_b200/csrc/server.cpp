@@ -14,8 +14,12 @@
 //  * Batching: queued split-precision requests with identical parameters and
 //    direction are admitted together (up to max_batch) and share one
 //    int8 contraction launch; everything else runs one request per slot.
-//    Results do not depend on batch companions: the split is per signal and
-//    the int32 accumulation is exact.
+//    A split-precision unit of fewer than 4 signals runs on the FP64 path
+//    (the fallback: the tensor-core operands hold 16 signals, so small
+//    batches would waste most of the products and of the operand scratch).
+//    A result depends on its companions only through that choice: within a
+//    split-precision batch the split is per signal and the int32
+//    accumulation exact, and the FP64 path is within the split tolerance.
 //  * Resident state: Wigner tables, DFT plans, index tables and tuned kernel
 //    variants are the per-device ones of the library, shared by all slots;
 //    the Delta tables are built up to max_L at creation so they never grow
@@ -110,7 +114,10 @@ class Server {
       for (int m = 0; m < 2; m++)
         if (int rc = ensure_dl(D_, max_L_, m, slots_[0]->s, &t)) return rc;
     }
-    worker_ = std::thread([this] { loop(); });
+    worker_ = std::thread([this] {
+      set_thread_autotune(false);  // never stall admission on tuning a new geometry
+      loop();
+    });
     return kOk;
   }
 
@@ -194,10 +201,20 @@ class Server {
     sv->cv_.notify_all();
   }
 
+  // Precision a unit runs in: split precision pays only for batches of at
+  // least kMinSplitBatch signals (the tensor-core operand holds 16 signals and
+  // its scratch is sized per group of 16); smaller split-precision units run
+  // on the FP64 path, the fallback (more accurate, so still within the split
+  // tolerance).
+  static constexpr int kMinSplitBatch = 4;
+  static int unit_precision(const std::vector<Req*>& b) {
+    return (b[0]->precision == kPrecMixedInt8 && (int)b.size() >= kMinSplitBatch) ? kPrecMixedInt8 : kPrecFp64;
+  }
+
   size_t unit_bytes(const std::vector<Req*>& b) const {
     const Req& r = *b[0];
     const int real = r.p.reality != 0;
-    size_t need = batch_workspace_bytes(r.p, real, (int)b.size(), r.precision);
+    size_t need = batch_workspace_bytes(r.p, real, (int)b.size(), unit_precision(b));
     if (r.kind == 2) need = ((need + 255) & ~size_t(255)) + (size_t)so3_sampling_flmn_size(&r.p) * sizeof(double2);
     return need;
   }
@@ -236,8 +253,9 @@ class Server {
           ins[i] = sl->reqs[i]->in;
           outs[i] = sl->reqs[i]->out;
         }
-        rc = r.kind == 0 ? run_inverse_batch(D_, &sl->wk, r.p, real, n, ins.data(), outs.data(), r.precision, sl->s)
-                         : run_forward_batch(D_, &sl->wk, r.p, real, n, ins.data(), outs.data(), r.precision, sl->s);
+        const int prec = unit_precision(sl->reqs);
+        rc = r.kind == 0 ? run_inverse_batch(D_, &sl->wk, r.p, real, n, ins.data(), outs.data(), prec, sl->s)
+                         : run_forward_batch(D_, &sl->wk, r.p, real, n, ins.data(), outs.data(), prec, sl->s);
       }
       cudaFreeAsync(ws, sl->s);
       sl->wk.ws = nullptr;

@@ -117,7 +117,9 @@ struct Device {
   std::map<int, double2*> conv_kernels;          // weight kernel by L (MW/MWSS identical)
   std::map<std::string, long long*> bases;       // block bases by parameter key
   std::vector<std::unique_ptr<DigitTable>> digit_tables;
+  std::map<long long, int> digit_uses;  // split-precision calls per (L, N, recursion) without a table
   std::vector<std::unique_ptr<BetaTable>> beta_tables;
+  std::map<int, int> beta_uses;  // split-precision forward calls per L without a beta table
 };
 
 // Per-stage CUDA-event timing (optional, per caller context).
@@ -245,6 +247,8 @@ int launch_mixed_forward(const Geometry& g, int n_mode, const double2* W, long l
 int mixed_take_error();
 
 // ---------------------------------------------------------------- drivers
+// Per-thread switch of the stage autotuner (default on).
+void set_thread_autotune(bool on);
 // Contraction arithmetic of a batch: FP64 (the reference-exact path) or the
 // int8 split (complex signals only; real signals always use FP64).
 enum Precision : int { kPrecFp64 = 0, kPrecMixedInt8 = 1 };

@@ -172,3 +172,74 @@ def latency_summary(res, wall):
             "p50_ms": pct(tot, 0.50), "p99_ms": pct(tot, 0.99), "queue_p50_ms": pct(q, 0.50),
             "queue_p99_ms": pct(q, 0.99), "failed": sum(1 for r in res if r.status != 0),
             "mean_batch": float(np.mean([r.batch for r in res])) if res else None}
+
+
+def replay_stream(server: Server, trace, time_scale: float = 1.0, seed: int = 5):
+    """Replays a trace of arbitrary length with bounded device memory.  The
+    inverse and forward inputs of every request are prefixes of one seeded
+    pool of U(-1,1) complex values as large as the largest input of the trace
+    (transforms read no entry outside their band limits, so any prefix is a
+    valid input); directional-convolution requests get their own buffers.
+    Every request gets its own output buffer at submission, released once it
+    has completed.  Returns (results, wall seconds)."""
+    import torch
+    need = 0
+    for r in trace:
+        if r["kind"] != "convolve":
+            p = SO3Parameters(L=r["L"], N=r["N"])
+            need = max(need, flmn_size(p) if r["kind"] == "inverse" else f_size(p))
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    pool = torch.view_as_complex((torch.rand(2 * max(need, 1), dtype=torch.float64, device="cuda", generator=g) * 2
+                                  - 1).view(-1, 2))
+    conv = {}
+    torch.cuda.synchronize()
+    live, done = {}, {}
+    ids = []
+    t0 = time.perf_counter()
+    for r in trace:
+        dt = r["t"] * time_scale - (time.perf_counter() - t0)
+        if dt > 0:
+            time.sleep(dt)
+        p = SO3Parameters(L=r["L"], N=r["N"])
+        b = None
+        if r["kind"] == "inverse":
+            a, n_out = pool[:flmn_size(p)], f_size(p)
+        elif r["kind"] == "forward":
+            a, n_out = pool[:f_size(p)], flmn_size(p)
+        else:
+            key = (r["L"], r["N"])
+            if key not in conv:
+                conv[key] = request_buffers(r)[1:3]
+            (a, b), n_out = conv[key], f_size(p)
+        out = torch.empty(n_out, dtype=torch.complex128, device="cuda")
+        rid = server.submit(r["kind"], p, a, out, r["precision"], inp2=b)
+        ids.append(rid)
+        live[rid] = out
+        for k in list(live):  # a completed poll hands over (and forgets) the record
+            d = server.poll(k)
+            if d is not None:
+                done[k] = d
+                del live[k]
+    for k in list(live):
+        done[k] = server.wait(k)
+    wall = time.perf_counter() - t0
+    live.clear()
+    return [done[i] for i in ids], wall
+
+
+def serving_run(n: int = 400, rate: float = 200.0, seed: int = 11, precision: str = "fp64",
+                budget: int = 120 << 30, max_inflight: int = 8, max_batch: int = 8, device: int = 0,
+                L_range=(16, 1024), N_max: int = 64):
+    """The serving trace workload (inverse 60 % / forward 40 %, complex MW,
+    L log-uniform, N uniform in [1, min(L, N_max)], U(-1,1) inputs, Poisson
+    arrivals at `rate`) through a Server: latency percentiles and throughput."""
+    trace = make_trace(n, rate, seed, L_range=L_range, N_max=N_max, p_inverse=0.6, precision=precision)
+    with Server(device, memory_budget=budget, max_inflight=max_inflight, max_batch=max_batch,
+                max_L=L_range[1]) as sv:
+        res, wall = replay_stream(sv, trace)
+        st = sv.stats()
+    out = latency_summary(res, wall)
+    out.update({"offered_rate_rps": rate, "precision": precision, "peak_scratch_bytes": st["peak_bytes"],
+                "units": st["units"]})
+    return out

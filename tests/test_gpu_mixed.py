@@ -15,7 +15,10 @@ TOL_MIXED = 1e-10
 
 
 @pytest.fixture(autouse=True)
-def _no_kernel_timeouts():
+def _no_kernel_timeouts(monkeypatch):
+    # resident tables on first use, so every case runs the table-fed tensor-core kernels
+    # (the default builds them on a geometry's second call; see test_tables_on_second_call)
+    monkeypatch.setenv("SO3GPU_DIGIT_TABLE", "1")
     yield
     assert so3.take_kernel_error() == 0  # no bounded wait of the tensor-core kernels gave up
 
@@ -130,7 +133,7 @@ def test_resident_digits_equal_generated_digits(L, N, nsig, kw, monkeypatch):
     fls = [torch.from_numpy(synth.gen_flmn(p, 40 + i)).cuda() for i in range(nsig)]
     f64 = ctx.inverse_batch(fls, p, "fp64")
     outs = {}
-    for mode in ("0", "1"):
+    for mode in ("1", "0"):  # "1" first: the forward beta table then exists for both runs
         monkeypatch.setenv("SO3GPU_DIGIT_TABLE", mode)
         inv = ctx.inverse_batch(fls, p, "mixed")
         fwd = ctx.forward_batch(f64, p, "mixed")
@@ -138,3 +141,30 @@ def test_resident_digits_equal_generated_digits(L, N, nsig, kw, monkeypatch):
         outs[mode] = ([x.cpu().numpy() for x in inv], [x.cpu().numpy() for x in fwd])
     for a, b in zip(outs["0"][0] + outs["0"][1], outs["1"][0] + outs["1"][1]):
         assert np.array_equal(a, b)
+
+
+def test_tables_on_second_call(monkeypatch):
+    """Default policy: the first split-precision call of a geometry generates
+    the digits from Delta and runs the FP64 forward beta stage; later calls
+    use the resident tables (tensor-core forward beta stage).  Every call is
+    within the split-precision tolerance of the FP64 path."""
+    import torch
+    monkeypatch.delenv("SO3GPU_DIGIT_TABLE", raising=False)
+    p = params(77, 5)  # a geometry no other test uses
+    ctx = so3.Context(0)
+    fls = [torch.from_numpy(synth.gen_flmn(p, 60 + i)).cuda() for i in range(3)]
+    f64 = ctx.inverse_batch(fls, p, "fp64")
+    b64 = [x.cpu().numpy() for x in ctx.forward_batch(f64, p, "fp64")]
+    runs = []
+    for _ in range(3):
+        inv = ctx.inverse_batch(fls, p, "mixed")
+        fwd = ctx.forward_batch(f64, p, "mixed")
+        torch.cuda.synchronize()
+        runs.append(([x.cpu().numpy() for x in inv], [x.cpu().numpy() for x in fwd]))
+    f64n = [x.cpu().numpy() for x in f64]
+    for inv, fwd in runs:
+        for i in range(3):
+            assert rel_err(inv[i], f64n[i]) < TOL_MIXED
+            assert rel_err(fwd[i], b64[i]) < TOL_MIXED
+    for i in range(3):  # second and third calls: same (table) path
+        assert np.array_equal(runs[1][1][i], runs[2][1][i])

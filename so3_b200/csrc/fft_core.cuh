@@ -30,6 +30,11 @@ struct FftPlan {
   const double2* chirp;      // e^{-i pi k^2/n}, k < n     (Bluestein)
   const double2* kern;       // FFT_m(conj chirp) / m      (Bluestein)
   const double2* half;       // e^{-i pi k/n}, k < n       (half-step roots: the MW beta phases)
+  // Rader tables (n = 127 only, else null): the prime-length DFT as a cyclic
+  // convolution of length n-1 with primitive root 3
+  const double2* rroots;     // e^{-2 pi i k/(n-1)}, k < n-1
+  const double2* rkern;      // FFT_{n-1}(e^{-2 pi i 3^{-m}/n}) / (n-1)
+  const int* rperm;          // [0, n-1): 3^a mod n (gather); [n-1, 2n-2): 3^{-b} mod n (scatter)
   int ld() const { return blue ? m : n; }
   // any radix above 8 (needs the large-radix kernel instances)
   bool big() const {

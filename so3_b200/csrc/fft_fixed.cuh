@@ -245,5 +245,52 @@ struct P127 {
   }
 };
 
+// 127 (prime) by Rader's algorithm: with the primitive root 3,
+//   X[3^{-b}] = x[0] + sum_{a < 126} x[3^a] w^{3^{a-b}},   X[0] = sum_n x[n],
+// a cyclic convolution of length 126 = 7 * 3 * 3 * 2 evaluated as
+// conj(FFT(conj(FFT(u) * V))) with V = FFT(v) / 126 precomputed.  About half
+// the arithmetic of Bluestein over 256 and half its shared memory.
+// Input x in a (entries 0..126); returns the buffer holding X.
+template <int T, int LD, int NT>
+struct P127R {
+  static constexpr bool sk = false;
+  static constexpr int n = 127, ld = extent<sk>(127);
+  static __device__ __forceinline__ void fft126(double2* b, double2* a, const double2* roots) {
+    pass<126, 7, 1, T, LD, NT, 1, sk>(b, a, roots);
+    __syncthreads();
+    pass<126, 3, 7, T, LD, NT, 1, sk>(a, b, roots);
+    __syncthreads();
+    pass<126, 3, 21, T, LD, NT, 1, sk>(b, a, roots);
+    __syncthreads();
+    pass<126, 2, 63, T, LD, NT, 1, sk>(a, b, roots);
+    __syncthreads();
+  }
+  static __device__ __forceinline__ double2* run(double2* a, double2* b, const FftPlan& P) {
+    __shared__ double2 x0[T], X0[T];
+    for (int w = threadIdx.x; w < T * 126; w += NT) {  // t fastest: lanes of one a share the index load
+      const int t = w % T, ai = w / T;
+      b[t * LD + ai] = a[t * LD + __ldg(P.rperm + ai)];
+    }
+    for (int t = threadIdx.x; t < T; t += NT) x0[t] = a[t * LD];
+    __syncthreads();
+    fft126(b, a, P.rroots);  // U in b
+    for (int w = threadIdx.x; w < T * 126; w += NT) {
+      const int t = w % T, k = w / T;
+      const double2 u = b[t * LD + k];
+      if (k == 0) X0[t] = cadd(x0[t], u);
+      b[t * LD + k] = cconj(cmul(u, __ldg(P.rkern + k)));
+    }
+    __syncthreads();
+    fft126(b, a, P.rroots);  // conj of the cyclic convolution in b
+    for (int w = threadIdx.x; w < T * 126; w += NT) {
+      const int t = w % T, bi = w / T;
+      a[t * LD + __ldg(P.rperm + 126 + bi)] = cadd(x0[t], cconj(b[t * LD + bi]));
+    }
+    for (int t = threadIdx.x; t < T; t += NT) a[t * LD] = X0[t];
+    __syncthreads();
+    return a;
+  }
+};
+
 }  // namespace fx
 }  // namespace so3g

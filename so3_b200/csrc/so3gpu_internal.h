@@ -88,7 +88,8 @@ __host__ __device__ inline long long dl_plane_offset(int l) {
 
 struct DevPlan {
   FftPlan plan{};
-  double2* mem = nullptr;  // owns roots/mroots/chirp/kern
+  double2* mem = nullptr;  // owns roots/mroots/chirp/kern/half/rroots/rkern
+  int* imem = nullptr;     // owns rperm
 };
 
 // Resident int8 digits of the split-precision contractions' Delta products

@@ -107,6 +107,9 @@ using E1023c = Fix<fx::P1023, fx::P1023, 2, 128, 3>;
 using E127a = Fix<fx::P127, fx::P127, 4, 128, 4>;
 using E127b = Fix<fx::P127, fx::P127, 8, 128, 3>;
 using E127c = Fix<fx::P127, fx::P127, 2, 64, 8>;
+using E127ra = Fix<fx::P127R, fx::P127R, 8, 128, 4>;
+using E127rb = Fix<fx::P127R, fx::P127R, 16, 256, 2>;
+using E127rc = Fix<fx::P127R, fx::P127R, 4, 64, 8>;
 using EConv1023a = Fix<fx::P1023, fx::P2048, 1, 128, 3>;
 using EConv1023b = Fix<fx::P1023, fx::P2048, 1, 256, 2>;
 
@@ -353,9 +356,10 @@ __global__ void __launch_bounds__(E::NT, E::MINB) fwd_beta_conv_kernel(Geometry 
 // ------------------------------------------------------------------ launchers
 namespace {
 
-enum class Eng { kGenSmall, kGenBig, k1023, k127 };
+enum class Eng { kGenSmall, kGenBig, k1023, k127, k127r };
 Eng pick(const FftPlan& p) {
   if (!p.blue && p.n == 1023) return Eng::k1023;
+  if (p.blue && p.n == 127 && p.rkern) return Eng::k127r;
   if (p.blue && p.n == 127 && p.m == 256) return Eng::k127;
   return p.big() ? Eng::kGenBig : Eng::kGenSmall;
 }
@@ -439,6 +443,9 @@ int launch_inv_beta(const Geometry& g, const FftPlan& p, double2* W, cudaStream_
     case Eng::k127:
       rc = v == 1 ? inv_beta<E127b>(g, p, W, s) : v == 2 ? inv_beta<E127c>(g, p, W, s) : inv_beta<E127a>(g, p, W, s);
       break;
+    case Eng::k127r:
+      rc = v == 1 ? inv_beta<E127rb>(g, p, W, s) : v == 2 ? inv_beta<E127rc>(g, p, W, s) : inv_beta<E127ra>(g, p, W, s);
+      break;
     case Eng::kGenBig: rc = inv_beta<Gen<true>>(g, p, W, s); break;
     default: rc = inv_beta<Gen<false>>(g, p, W, s); break;
   }
@@ -455,6 +462,10 @@ int launch_inv_alpha(const Geometry& g, const FftPlan& p, double2* W, cudaStream
       break;
     case Eng::k127:
       rc = v == 1 ? inv_alpha<E127b>(g, p, W, s) : v == 2 ? inv_alpha<E127c>(g, p, W, s) : inv_alpha<E127a>(g, p, W, s);
+      break;
+    case Eng::k127r:
+      rc = v == 1 ? inv_alpha<E127rb>(g, p, W, s) : v == 2 ? inv_alpha<E127rc>(g, p, W, s)
+                                                             : inv_alpha<E127ra>(g, p, W, s);
       break;
     case Eng::kGenBig: rc = inv_alpha<Gen<true>>(g, p, W, s); break;
     default: rc = inv_alpha<Gen<false>>(g, p, W, s); break;
@@ -476,6 +487,10 @@ int launch_inv_gamma(const Geometry& g, const FftPlan& p, const double2* W, void
     rc = v == 1   ? inv_gamma<false, E127b>(g, p, W, f, s, row_lo, row_hi)
          : v == 2 ? inv_gamma<false, E127c>(g, p, W, f, s, row_lo, row_hi)
                   : inv_gamma<false, E127a>(g, p, W, f, s, row_lo, row_hi);
+  } else if (e == Eng::k127r) {
+    rc = v == 1   ? inv_gamma<false, E127rb>(g, p, W, f, s, row_lo, row_hi)
+         : v == 2 ? inv_gamma<false, E127rc>(g, p, W, f, s, row_lo, row_hi)
+                  : inv_gamma<false, E127ra>(g, p, W, f, s, row_lo, row_hi);
   } else {
     rc = e == Eng::kGenBig ? inv_gamma<false, Gen<true>>(g, p, W, f, s, row_lo, row_hi)
                            : inv_gamma<false, Gen<false>>(g, p, W, f, s, row_lo, row_hi);
@@ -497,6 +512,10 @@ int launch_fwd_gamma(const Geometry& g, const FftPlan& p, const void* f, double2
     rc = v == 1   ? fwd_gamma<false, E127b>(g, p, f, W, s, row_lo, row_hi)
          : v == 2 ? fwd_gamma<false, E127c>(g, p, f, W, s, row_lo, row_hi)
                   : fwd_gamma<false, E127a>(g, p, f, W, s, row_lo, row_hi);
+  } else if (e == Eng::k127r) {
+    rc = v == 1   ? fwd_gamma<false, E127rb>(g, p, f, W, s, row_lo, row_hi)
+         : v == 2 ? fwd_gamma<false, E127rc>(g, p, f, W, s, row_lo, row_hi)
+                  : fwd_gamma<false, E127ra>(g, p, f, W, s, row_lo, row_hi);
   } else {
     rc = e == Eng::kGenBig ? fwd_gamma<false, Gen<true>>(g, p, f, W, s, row_lo, row_hi)
                            : fwd_gamma<false, Gen<false>>(g, p, f, W, s, row_lo, row_hi);
@@ -514,6 +533,10 @@ int launch_fwd_alpha(const Geometry& g, const FftPlan& p, double2* W, cudaStream
       break;
     case Eng::k127:
       rc = v == 1 ? fwd_alpha<E127b>(g, p, W, s) : v == 2 ? fwd_alpha<E127c>(g, p, W, s) : fwd_alpha<E127a>(g, p, W, s);
+      break;
+    case Eng::k127r:
+      rc = v == 1 ? fwd_alpha<E127rb>(g, p, W, s) : v == 2 ? fwd_alpha<E127rc>(g, p, W, s)
+                                                             : fwd_alpha<E127ra>(g, p, W, s);
       break;
     case Eng::kGenBig: rc = fwd_alpha<Gen<true>>(g, p, W, s); break;
     default: rc = fwd_alpha<Gen<false>>(g, p, W, s); break;
@@ -543,9 +566,9 @@ int stage_variants(const Geometry& g, const FftPlan& pP, const FftPlan& pg, cons
   switch (stage) {
     case kStInvBeta:
     case kStInvAlpha:
-    case kStFwdAlpha: return (pick(pP) == Eng::k1023 || pick(pP) == Eng::k127) ? 3 : 1;
+    case kStFwdAlpha: return (pick(pP) == Eng::k1023 || pick(pP) == Eng::k127 || pick(pP) == Eng::k127r) ? 3 : 1;
     case kStInvGamma:
-    case kStFwdGamma: return (!g.real && pick(pg) == Eng::k127) ? 3 : 1;
+    case kStFwdGamma: return (!g.real && (pick(pg) == Eng::k127 || pick(pg) == Eng::k127r)) ? 3 : 1;
     case kStFwdBetaConv: return conv_fixed(pP, pc) ? 2 : 1;
     default: return 1;
   }

@@ -318,11 +318,51 @@ int ensure_fft(Device* D, int n, FftPlan* out) {
     cld r = root_l(k, 2LL * n);  // e^{-i pi k/n}
     host[half_at + k] = make_double2((double)r.real(), (double)r.imag());
   }
+  // Rader's algorithm for the prime 127 (gamma length at N = 64): X[3^{-b}] =
+  // x[0] + sum_a x[3^a] w^{3^{a-b}}, a cyclic convolution of length 126
+  const bool rader = n == 127;
+  size_t rader_at = host.size();
+  std::vector<int> perm;
+  if (rader) {
+    const int q = n - 1;
+    host.resize(rader_at + 2 * (size_t)q);
+    for (int k = 0; k < q; k++) {
+      cld r = root_l(k, q);
+      host[rader_at + k] = make_double2((double)r.real(), (double)r.imag());
+    }
+    perm.resize(2 * (size_t)q);
+    std::vector<int> pw(q);  // 3^a mod n
+    long long v = 1;
+    for (int a = 0; a < q; a++) {
+      pw[a] = (int)v;
+      v = v * 3 % n;
+    }
+    for (int a = 0; a < q; a++) {
+      perm[a] = pw[a];
+      perm[q + a] = pw[(q - a) % q];  // 3^{-a} = 3^{q-a}
+    }
+    // kernel: FFT_q of v[m] = w^{3^{-m}}, divided by q (direct long-double DFT)
+    for (int k = 0; k < q; k++) {
+      cld acc(0, 0);
+      for (int m = 0; m < q; m++) acc += root_l(perm[q + m], n) * root_l((long long)m * k % q, q);
+      acc /= (long double)q;
+      host[rader_at + q + k] = make_double2((double)acc.real(), (double)acc.imag());
+    }
+  }
   cudaError_t e = cudaMalloc(&dp->mem, host.size() * sizeof(double2));
   if (e != cudaSuccess) return fail(kOutOfMemory, "FFT table allocation failed");
   e = cudaMemcpy(dp->mem, host.data(), host.size() * sizeof(double2), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return fail(kCudaError, std::string("FFT table upload: ") + cudaGetErrorString(e));
   P.half = dp->mem + half_at;
+  if (rader) {
+    P.rroots = dp->mem + rader_at;
+    P.rkern = dp->mem + rader_at + (n - 1);
+    e = cudaMalloc(&dp->imem, perm.size() * sizeof(int));
+    if (e != cudaSuccess) return fail(kOutOfMemory, "FFT table allocation failed");
+    e = cudaMemcpy(dp->imem, perm.data(), perm.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fail(kCudaError, std::string("FFT table upload: ") + cudaGetErrorString(e));
+    P.rperm = dp->imem;
+  }
   if (!P.blue) {
     P.roots = dp->mem;
   } else {

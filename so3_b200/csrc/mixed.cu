@@ -514,8 +514,8 @@ __global__ void __launch_bounds__(256) slice_kernel(SliceArgs a) {
 // Single-pass slicing: a CTA stages its columns (complex, all reduction
 // entries) in shared memory with coalesced loads, finds each column's scale
 // with a warp reduction, then writes 16-entry digit slots.
-constexpr int kSliceCols = 16;  // complex columns per slicing CTA
-constexpr int kSliceSmemMax = 200 * 1024;  // staged columns fit (L <= 768)
+constexpr int kSliceCols = 8;  // complex columns per slicing CTA (4 sign combinations x 2)
+constexpr int kSliceSmemMax = 100 * 1024;  // staged columns fit (L <= 768)
 
 // Digits of the staged columns: thread <-> (real column c of the CTA's 32,
 // block of 16 entries); c_base: first row of the stage image.
@@ -523,7 +523,7 @@ __device__ __forceinline__ void slice_from_smem(const double2* __restrict__ col,
                                                 uint8_t* pb, int c_base) {
   const int nblk = Lp / 16;
   for (int w = threadIdx.x; w < 2 * kSliceCols * nblk; w += blockDim.x) {
-    const int c = w & 31, kb = w >> 5, cc = c >> 1, part = c & 1;
+    const int c = w % (2 * kSliceCols), kb = w / (2 * kSliceCols), cc = c >> 1, part = c & 1;
     const double inv = 1.0 / scl[c];
     uint32_t d[4][kS];
 #pragma unroll
@@ -545,9 +545,10 @@ __device__ __forceinline__ void slice_from_smem(const double2* __restrict__ col,
 
 // Largest magnitude of the real and imaginary parts of each staged column
 // (warp w handles columns w, w + 8); scales into scl[2 cc + part].
+template <int NC>
 __device__ __forceinline__ void column_scales(const double2* __restrict__ col, int Lp, double* scl) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int cc = warp; cc < kSliceCols; cc += nw) {
+  for (int cc = warp; cc < NC; cc += nw) {
     double mr = 0.0, mi = 0.0;
     for (int k = lane; k < Lp; k += 32) {
       const double2 x = col[(size_t)cc * Lp + k];
@@ -563,21 +564,23 @@ __device__ __forceinline__ void column_scales(const double2* __restrict__ col, i
   }
 }
 
-// Inverse.  One CTA per (nu, block of 4 mu, signal): its 16 complex columns
-// (4 mu x combos (+-m, +-nu)) are the rows 8 * (signal % 16) .. +7 of the
-// stage images of the 4 pairs.  Staging: warp <-> (n = +-nu, l), lanes <->
-// (mu, sign of m): two runs of 4 consecutive m (64 bytes) per (n, l).
-// Entries l < max(mu, nu, L0) are zero.
+// Inverse.  One CTA per (nu, block of kMuPer mu, signal): its complex
+// columns (kMuPer mu x combos (+-m, +-nu)) are the rows 8 * (signal % 16)
+// .. +7 of the stage images of its pairs.  Staging: lanes <-> (mu, combo),
+// runs of kMuPer consecutive m per (n, l).  Entries l < max(mu, nu, L0) are
+// zero.
+constexpr int kMuPer = 4;  // 16 staged columns: 64-byte runs of m per (n, l)
 __global__ void __launch_bounds__(256) slice_inv_kernel(SliceArgs a) {
-  extern __shared__ __align__(16) double2 colbuf[];  // [4 mu][4 combos][Lp]
-  __shared__ double scl[4][2 * 4];
+  extern __shared__ __align__(16) double2 colbuf[];  // [kMuPer mu][4 combos][Lp]
+  __shared__ double scl[kMuPer][2 * 4];
   const int Lp = a.nchunk * kKC, L = a.L;
-  const int nu = blockIdx.x % a.N, mu0 = (blockIdx.x / a.N) * 4, sig = blockIdx.y;
+  const int nu = blockIdx.x % a.N, mu0 = (blockIdx.x / a.N) * kMuPer, sig = blockIdx.y;
   const int grp = sig / kSig, b = sig % kSig;
   {
     // thread <-> (j, combo) fixed (m fastest across lanes), l = l0 + 16 i;
     // 8 loads in flight per thread
-    const int j = threadIdx.x & 3, combo = (threadIdx.x >> 2) & 3, l0 = threadIdx.x >> 4;
+    const int j = threadIdx.x % kMuPer, combo = (threadIdx.x / kMuPer) & 3, l0 = threadIdx.x / (4 * kMuPer);
+    constexpr int LSTEP = 256 / (4 * kMuPer);  // l-lanes
     const int mu = mu0 + j, ms = (combo & 1) ? -1 : 1, ns = (combo & 2) ? -1 : 1;
     const int m = ms * mu, n = ns * nu;
     const bool act = mu < L && sig < a.nsig && !(ms < 0 && mu == 0) && !(ns < 0 && nu == 0) &&
@@ -586,16 +589,16 @@ __global__ void __launch_bounds__(256) slice_inv_kernel(SliceArgs a) {
     const bool flip = ms * ns < 0;
     const double2* src = act ? a.flmn[sig] + a.base[a.plane0 + n] + m : nullptr;
     double2* dst = colbuf + (size_t)(j * 4 + combo) * Lp;
-    for (int l1 = l0; l1 < Lp; l1 += 16 * 8) {
+    for (int l1 = l0; l1 < Lp; l1 += LSTEP * 8) {
       double2 x[8];
 #pragma unroll
       for (int u = 0; u < 8; u++) {
-        const int l = l1 + 16 * u;
+        const int l = l1 + LSTEP * u;
         x[u] = (act && l < L && l >= lmin) ? __ldg(src + (long long)l * l + l) : make_double2(0.0, 0.0);
       }
 #pragma unroll
       for (int u = 0; u < 8; u++) {
-        const int l = l1 + 16 * u;
+        const int l = l1 + LSTEP * u;
         if (l >= Lp) break;
         double f = (2.0 * l + 1.0) * kInv8Pi2;
         if (flip && (l & 1)) f = -f;
@@ -605,17 +608,17 @@ __global__ void __launch_bounds__(256) slice_inv_kernel(SliceArgs a) {
   }
   __syncthreads();
   // scales: column (j, combo) -> scl[j][2 combo + part]
-  column_scales(colbuf, Lp, &scl[0][0]);
+  column_scales<4 * kMuPer>(colbuf, Lp, &scl[0][0]);
   __syncthreads();
-  for (int j = 0; j < 4; j++) {
+  for (int j = 0; j < kMuPer; j++) {
     const int mu = mu0 + j;
     if (mu >= L) break;
     const size_t gp = (size_t)grp * a.npairs + (size_t)mu * a.N + nu;
     if (threadIdx.x < 8) a.xscale[gp * kM + 8 * b + threadIdx.x] = scl[j][threadIdx.x];
   }
-  // digits: pairs handled one after another (8 real columns each)
-  for (int w = threadIdx.x; w < 4 * 8 * (Lp / 16); w += blockDim.x) {
-    const int c = w & 7, j = (w >> 3) & 3, kb = w >> 5;
+  // digits: 8 real columns per pair
+  for (int w = threadIdx.x; w < kMuPer * 8 * (Lp / 16); w += blockDim.x) {
+    const int c = w & 7, j = (w >> 3) % kMuPer, kb = w / (8 * kMuPer);
     const int mu = mu0 + j;
     if (mu >= L) continue;
     const int combo = c >> 1, part = c & 1;
@@ -641,19 +644,21 @@ __global__ void __launch_bounds__(256) slice_inv_kernel(SliceArgs a) {
   }
 }
 
-// Forward.  One CTA per (pair, 4 signals): complex columns cc = 4 * signal +
-// combo (rows 32 q .. 32 q + 31 of the pair's stage image for signals
-// 4q .. 4q+3 of the group); warp <-> column, lanes along m' (512-byte runs).
+// Forward.  One CTA per (pair, kSigPer signals): complex columns cc = 4 *
+// signal + combo (rows 8 kSigPer q .. of the pair's stage image for the
+// q-th set of kSigPer signals of the group); warp <-> column, lanes along m'
+// (512-byte runs).
+constexpr int kSigPer = kSliceCols / 4;
 __global__ void __launch_bounds__(256) slice_fwd_kernel(SliceArgs a) {
-  extern __shared__ __align__(16) double2 colbuf[];  // [16 columns][Lp]
+  extern __shared__ __align__(16) double2 colbuf[];  // [kSliceCols columns][Lp]
   __shared__ double scl[2 * kSliceCols];
   const int Lp = a.nchunk * kKC, L = a.L;
-  const int pair = blockIdx.x, q4 = blockIdx.y;  // q4: quarter of all signals (4 each)
+  const int pair = blockIdx.x, q4 = blockIdx.y;  // q4: set of kSigPer signals
   const int nu = pair % a.N, mu = pair / a.N;
-  const int grp = (4 * q4) / kSig, qin = q4 % (kSig / 4);
+  const int grp = (kSigPer * q4) / kSig, qin = q4 % (kSig / kSigPer);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int cc = warp; cc < kSliceCols; cc += 8) {
-    const int sig = 4 * q4 + (cc >> 2), combo = cc & 3;
+    const int sig = kSigPer * q4 + (cc >> 2), combo = cc & 3;
     const int ms = (combo & 1) ? -1 : 1, ns = (combo & 2) ? -1 : 1;
     const int m = ms * mu, n = ns * nu;
     const bool act = sig < a.nsig && !(ms < 0 && mu == 0) && !(ns < 0 && nu == 0) && !plane_skipped(a.n_mode, a.N, n);
@@ -677,11 +682,11 @@ __global__ void __launch_bounds__(256) slice_fwd_kernel(SliceArgs a) {
     }
   }
   __syncthreads();
-  column_scales(colbuf, Lp, scl);
+  column_scales<kSliceCols>(colbuf, Lp, scl);
   __syncthreads();
   const size_t gp = (size_t)grp * a.npairs + pair;
-  if (threadIdx.x < 2 * kSliceCols) a.xscale[gp * kM + 32 * qin + threadIdx.x] = scl[threadIdx.x];
-  slice_from_smem(colbuf, Lp, scl, a.xs + gp * (size_t)a.nchunk * kXStage, 32 * qin);
+  if (threadIdx.x < 2 * kSliceCols) a.xscale[gp * kM + 2 * kSliceCols * qin + threadIdx.x] = scl[threadIdx.x];
+  slice_from_smem(colbuf, Lp, scl, a.xs + gp * (size_t)a.nchunk * kXStage, 2 * kSliceCols * qin);
 }
 
 // ---------------------------------------------------------------- persistent form
@@ -1337,12 +1342,12 @@ int launch_mixed_inverse(const Geometry& g, int n_mode, const double2* const* fl
   if (int rc = mixed_args(g, n_mode, nsig, scratch, &m, &sa)) return rc;
   sa.flmn = flmn_dev;
   sa.base = bases;
-  const int slice_smem = 16 * (int)sizeof(double2) * nchunks(g) * kKC;  // 16 columns x Lp entries
-  if (slice_smem <= kSliceSmemMax) {
+  const int slice_smem = 4 * kMuPer * (int)sizeof(double2) * nchunks(g) * kKC;  // staged columns x Lp entries
+  if (slice_smem <= 2 * kSliceSmemMax) {
     SO3G_CUDA(cudaFuncSetAttribute(slice_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, slice_smem));
     // every signal of the last group (zeros past nsig), so the group's stage images are complete
-    slice_inv_kernel<<<dim3((unsigned)(g.N * ((g.L + 3) / 4)), (unsigned)(((nsig + kSig - 1) / kSig) * kSig)), 256,
-                       slice_smem, s>>>(sa);
+    slice_inv_kernel<<<dim3((unsigned)(g.N * ((g.L + kMuPer - 1) / kMuPer)), (unsigned)(((nsig + kSig - 1) / kSig) * kSig)),
+                       256, slice_smem, s>>>(sa);
   } else {
     slice_kernel<false><<<dim3((unsigned)sa.npairs, (nsig + kSig - 1) / kSig), 256, 0, s>>>(sa);
   }
@@ -1366,10 +1371,10 @@ int launch_mixed_forward(const Geometry& g, int n_mode, const double2* W, long l
   sa.W = W + g.QOFF;
   sa.wstride = wstride;
   sa.base = bases;
-  const int slice_smem = 16 * (int)sizeof(double2) * nchunks(g) * kKC;
+  const int slice_smem = kSliceCols * (int)sizeof(double2) * nchunks(g) * kKC;
   if (slice_smem <= kSliceSmemMax) {
     SO3G_CUDA(cudaFuncSetAttribute(slice_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, slice_smem));
-    slice_fwd_kernel<<<dim3((unsigned)sa.npairs, (unsigned)(((nsig + kSig - 1) / kSig) * (kSig / 4))), 256,
+    slice_fwd_kernel<<<dim3((unsigned)sa.npairs, (unsigned)(((nsig + kSig - 1) / kSig) * (kSig / kSigPer))), 256,
                        slice_smem, s>>>(sa);
   } else {
     slice_kernel<true><<<dim3((unsigned)sa.npairs, (nsig + kSig - 1) / kSig), 256, 0, s>>>(sa);

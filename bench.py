@@ -52,6 +52,9 @@ def args_():
     ap.add_argument("--serve", type=int, default=400,
                     help="requests of the serving-trace sample (0: skip the serving leg)")
     ap.add_argument("--serve-rate", type=float, default=60.0, help="offered request rate of the serving leg (1/s)")
+    ap.add_argument("--profile-region", action="store_true",
+                    help="bracket the split-precision leg's timed steps with cudaProfilerStart/Stop "
+                         "(for ncu --profile-from-start off)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
@@ -277,7 +280,7 @@ def beta_tc_macs(L, N):
     return tiles * nc * nc * 2 * 28 * 128 * 64 * 32
 
 
-def timed_steps(step, steps, warmup, stream, ctx, so3, sdist, local, world):
+def timed_steps(step, steps, warmup, stream, ctx, so3, sdist, local, world, profile=False):
     import torch
     for _ in range(warmup):
         step()
@@ -290,11 +293,15 @@ def timed_steps(step, steps, warmup, stream, ctx, so3, sdist, local, world):
     launches0 = so3.launch_count()
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
+        if profile:
+            torch.cuda.profiler.start()
         evs[0].record(stream)
         for i in range(steps):
             step()
             evs[i + 1].record(stream)
         torch.cuda.synchronize()
+        if profile:
+            torch.cuda.profiler.stop()
     launches = so3.launch_count() - launches0
     stages = ctx.stage_times()
     ctx.stage_timing(False)
@@ -358,7 +365,7 @@ def run_ours(a):
             ctx.inverse_batch(fls, p, "mixed", outs=fs)
             ctx.forward_batch(fs, p, "mixed", outs=backs)
 
-        rmx = timed_steps(stepmx, a.steps, a.warmup, stream, ctx, so3, sdist, local, world)
+        rmx = timed_steps(stepmx, a.steps, a.warmup, stream, ctx, so3, sdist, local, world, a.profile_region)
         mixed_value = sdist.job_throughput(world * a.steps * B, rmx["total_ms"] / 1e3)
         # error of the split path against the FP64 path on the same inputs
         err_f = err_fl = err_rt = 0.0

@@ -113,6 +113,12 @@ __device__ __forceinline__ double int_to_double(int x) {
   return __hiloint2double(0x43300000, x ^ (int)0x80000000) - 4503601774854144.0;
 }
 
+// Exact int64 -> FP64 for |x| < 2^51 on the FP64 pipe: adding x to the bits
+// of 1.5 * 2^52 gives the double 1.5 * 2^52 + x; one subtraction leaves x.
+__device__ __forceinline__ double ll_to_double(long long x) {
+  return __longlong_as_double(0x4338000000000000LL + x) - 6755399441055744.0;
+}
+
 __device__ __forceinline__ double2 ipow(double2 v, int k) {  // v * i^k
   switch (k & 3) {
     case 0: return v;
@@ -780,13 +786,15 @@ __device__ __forceinline__ void drain8(uint32_t taddr, double w0, double (&v)[8]
 #pragma unroll
   for (int e = 0; e < 8; e++) v[e] = 0.0;
   if (PAIRED) {
-    const double w1 = w0 * 0.00006103515625;  // 2^{-14}: pair (1, 2) in units of diagonal 2
+    // exact integer sums: hi = acc0 2^14 + (128 acc1 + acc2) (|hi| < 2^39),
+    // lo = (128 acc3 + acc4) 2^14 + (128 acc5 + acc6) (|lo| < 2^46); value =
+    // w0 (hi 2^{-14} + lo 2^{-42}): two conversions and two FP64 operations
+    const double whi = w0 * 0.00006103515625, wlo = w0 * 2.2737367544323206e-13;  // 2^{-14}, 2^{-42}
 #pragma unroll
     for (int e = 0; e < 8; e++) {
-      v[e] = fma(int_to_double(acc[0][e]), w0, v[e]);
-      v[e] = fma(int_to_double(acc[1][e] * 128 + acc[2][e]), w1, v[e]);
-      v[e] = fma(int_to_double(acc[3][e] * 128 + acc[4][e]), w1 * 0.00006103515625, v[e]);
-      v[e] = fma(int_to_double(acc[5][e] * 128 + acc[6][e]), w1 * 0.0000000037252902984619140625, v[e]);
+      const long long hi = (long long)acc[0][e] * 16384 + (acc[1][e] * 128 + acc[2][e]);
+      const long long lo = (long long)(acc[3][e] * 128 + acc[4][e]) * 16384 + (acc[5][e] * 128 + acc[6][e]);
+      v[e] = fma(ll_to_double(hi), whi, ll_to_double(lo) * wlo);
     }
   } else {
     double wd = w0;

@@ -437,6 +437,15 @@ def run_ours(a):
                             f"complex MW, 120 GB budget, 8 slots, batches of up to 8"}
         for prec in ("fp64", "mixed"):
             serving[prec] = sserve.serving_run(a.serve, a.serve_rate, seed=rank + 11, precision=prec, device=local)
+        # recurring geometries offered as a burst: split-precision requests batch (up to 8 per launch)
+        shapes = [(512, 16), (256, 32), (128, 64)]
+        serving["recurring"] = {"trace": f"256 requests, (L, N) uniform over {shapes}, 60% inverse / 40% forward, "
+                                         f"Poisson 1000/s offered, batches of up to 8; measured after one untimed "
+                                         f"pass of the same trace (resident tables built)"}
+        for prec in ("fp64", "mixed"):
+            sserve.serving_run(256, 1000.0, seed=rank + 21, precision=prec, device=local, shapes=shapes)  # warm-up
+            serving["recurring"][prec] = sserve.serving_run(256, 1000.0, seed=rank + 21, precision=prec,
+                                                            device=local, shapes=shapes)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:

@@ -96,18 +96,22 @@ class Server:
 
 # --------------------------------------------------------------------- traces
 def make_trace(n: int, rate: float, seed: int, L_range=(16, 1024), N_max: int = 64, p_inverse: float = 0.6,
-               p_convolve: float = 0.0, precision: str = "fp64"):
+               p_convolve: float = 0.0, precision: str = "fp64", shapes=None):
     """Seeded request trace: Poisson arrivals at `rate` per second; inverse
     with probability p_inverse, directional convolution with p_convolve, else
     forward; complex MW, L log-uniform in L_range (rounded), N uniform in
-    [1, min(L, N_max)]."""
+    [1, min(L, N_max)] -- or, when `shapes` lists (L, N) pairs, one of those
+    uniformly (recurring geometries, which split-precision requests batch)."""
     rng = np.random.default_rng(seed)
     t = np.cumsum(rng.exponential(1.0 / rate, n))
     lo, hi = math.log(L_range[0]), math.log(L_range[1])
     out = []
     for i in range(n):
-        L = int(round(math.exp(rng.uniform(lo, hi))))
-        N = int(rng.integers(1, min(L, N_max) + 1))
+        if shapes:
+            L, N = shapes[int(rng.integers(len(shapes)))]
+        else:
+            L = int(round(math.exp(rng.uniform(lo, hi))))
+            N = int(rng.integers(1, min(L, N_max) + 1))
         u = rng.uniform()
         kind = "inverse" if u < p_inverse else ("convolve" if u < p_inverse + p_convolve else "forward")
         out.append({"t": float(t[i]), "kind": kind, "L": L, "N": N, "seed": int(rng.integers(1 << 31)),
@@ -230,13 +234,16 @@ def replay_stream(server: Server, trace, time_scale: float = 1.0, seed: int = 5)
 
 def serving_run(n: int = 400, rate: float = 200.0, seed: int = 11, precision: str = "fp64",
                 budget: int = 120 << 30, max_inflight: int = 8, max_batch: int = 8, device: int = 0,
-                L_range=(16, 1024), N_max: int = 64):
+                L_range=(16, 1024), N_max: int = 64, shapes=None):
     """The serving trace workload (inverse 60 % / forward 40 %, complex MW,
-    L log-uniform, N uniform in [1, min(L, N_max)], U(-1,1) inputs, Poisson
-    arrivals at `rate`) through a Server: latency percentiles and throughput."""
-    trace = make_trace(n, rate, seed, L_range=L_range, N_max=N_max, p_inverse=0.6, precision=precision)
+    L log-uniform, N uniform in [1, min(L, N_max)] or drawn from `shapes`,
+    U(-1,1) inputs, Poisson arrivals at `rate`) through a Server: latency
+    percentiles and throughput."""
+    trace = make_trace(n, rate, seed, L_range=L_range, N_max=N_max, p_inverse=0.6, precision=precision,
+                       shapes=shapes)
+    max_L = max(L for L, _ in shapes) if shapes else L_range[1]
     with Server(device, memory_budget=budget, max_inflight=max_inflight, max_batch=max_batch,
-                max_L=L_range[1]) as sv:
+                max_L=max_L) as sv:
         res, wall = replay_stream(sv, trace)
         st = sv.stats()
     out = latency_summary(res, wall)

@@ -163,6 +163,35 @@ __device__ __forceinline__ void pass(const double2* __restrict__ src, double2* _
   }
 }
 
+// A whole-butterfly pass (NG = 1) of the same structure as pass(), with the
+// load and the store of each element given as functors: in(t, i) returns
+// element i of sequence t of the source, out(t, i, v) stores output i.  Lets
+// a permutation or a pointwise factor ride on a pass instead of costing a
+// shared-memory round trip of its own.
+template <int N, int R, int NS, int T, int NT, class In, class Out>
+__device__ __forceinline__ void pass_io(const In& in, const Out& out, const double2* __restrict__ roots) {
+  constexpr int M = N / R;
+  constexpr int TSTEP = N / (NS * R);
+  constexpr bool TW = NS > 1;
+  for (int u = threadIdx.x; u < T * M; u += NT) {
+    const int t = u % T;
+    const int j = u / T;
+    const int k = j % NS;
+    const int o = (j / NS) * NS * R + k;
+    double2 v[R];
+    v[0] = in(t, j);
+#pragma unroll
+    for (int r = 1; r < R; r++) {
+      double2 x = in(t, j + r * M);
+      if constexpr (TW) x = cmul(x, __ldg(roots + r * k * TSTEP));
+      v[r] = x;
+    }
+    bfly_any<R>(v);
+#pragma unroll
+    for (int q = 0; q < R; q++) out(t, o + q * NS, v[q]);
+  }
+}
+
 // ---------------------------------------------------------------- plans
 // Each plan: static constexpr n (length), ld (buffer extent per sequence,
 // padded by phys), and run(a, b, P) -> buffer holding the result (a and b:
@@ -249,43 +278,60 @@ struct P127 {
 //   X[3^{-b}] = x[0] + sum_{a < 126} x[3^a] w^{3^{a-b}},   X[0] = sum_n x[n],
 // a cyclic convolution of length 126 = 7 * 3 * 3 * 2 evaluated as
 // conj(FFT(conj(FFT(u) * V))) with V = FFT(v) / 126 precomputed.  About half
-// the arithmetic of Bluestein over 256 and half its shared memory.
-// Input x in a (entries 0..126); returns the buffer holding X.
+// the arithmetic of Bluestein over 256 and half its shared memory.  The
+// gather x[3^a] rides on the first pass of the first FFT, the product with V
+// (and the conjugation) on its last pass, the scatter to X[3^{-b}] on the
+// last pass of the second FFT: eight passes, no separate shared-memory
+// sweeps.  Input x in a (entries 0..126); returns the buffer holding X.
 template <int T, int LD, int NT>
 struct P127R {
   static constexpr bool sk = false;
   static constexpr int n = 127, ld = extent<sk>(127);
-  static __device__ __forceinline__ void fft126(double2* b, double2* a, const double2* roots) {
-    pass<126, 7, 1, T, LD, NT, 1, sk>(b, a, roots);
+  struct Plain {
+    double2* p;
+    __device__ double2 operator()(int t, int i) const { return p[t * LD + i]; }
+    __device__ void operator()(int t, int i, double2 v) const { p[t * LD + i] = v; }
+  };
+  struct Gather {  // element a of the convolution input: x[3^a]
+    const double2* p;
+    const int* perm;
+    __device__ double2 operator()(int t, int i) const { return p[t * LD + __ldg(perm + i)]; }
+  };
+  struct Kernel {  // conj(U[k] V[k]); X[0] = x[0] + U[0]
+    double2* p;
+    const double2* kern;
+    const double2* x0;
+    double2* X0;
+    __device__ void operator()(int t, int k, double2 u) const {
+      if (k == 0) X0[t] = cadd(x0[t], u);
+      p[t * LD + k] = cconj(cmul(u, __ldg(kern + k)));
+    }
+  };
+  struct Scatter {  // X[3^{-b}] = x[0] + conj(second FFT)[b]
+    double2* p;
+    const int* perm;
+    const double2* x0;
+    __device__ void operator()(int t, int b, double2 v) const { p[t * LD + __ldg(perm + b)] = cadd(x0[t], cconj(v)); }
+  };
+  template <class In, class Out>
+  static __device__ __forceinline__ void fft126(const In& in, double2* a, double2* b, const Out& out,
+                                                const double2* roots) {
+    pass_io<126, 7, 1, T, NT>(in, Plain{b}, roots);
     __syncthreads();
-    pass<126, 3, 7, T, LD, NT, 1, sk>(a, b, roots);
+    pass_io<126, 3, 7, T, NT>(Plain{b}, Plain{a}, roots);
     __syncthreads();
-    pass<126, 3, 21, T, LD, NT, 1, sk>(b, a, roots);
+    pass_io<126, 3, 21, T, NT>(Plain{a}, Plain{b}, roots);
     __syncthreads();
-    pass<126, 2, 63, T, LD, NT, 1, sk>(a, b, roots);
-    __syncthreads();
+    pass_io<126, 2, 63, T, NT>(Plain{b}, out, roots);
   }
   static __device__ __forceinline__ double2* run(double2* a, double2* b, const FftPlan& P) {
     __shared__ double2 x0[T], X0[T];
-    for (int w = threadIdx.x; w < T * 126; w += NT) {  // t fastest: lanes of one a share the index load
-      const int t = w % T, ai = w / T;
-      b[t * LD + ai] = a[t * LD + __ldg(P.rperm + ai)];
-    }
     for (int t = threadIdx.x; t < T; t += NT) x0[t] = a[t * LD];
+    // each FFT: source -> b -> a -> b -> a; x[0] is read from a before the
+    // second pass overwrites it (barrier after the first pass)
+    fft126(Gather{a, P.rperm}, a, b, Kernel{a, P.rkern, x0, X0}, P.rroots);
     __syncthreads();
-    fft126(b, a, P.rroots);  // U in b
-    for (int w = threadIdx.x; w < T * 126; w += NT) {
-      const int t = w % T, k = w / T;
-      const double2 u = b[t * LD + k];
-      if (k == 0) X0[t] = cadd(x0[t], u);
-      b[t * LD + k] = cconj(cmul(u, __ldg(P.rkern + k)));
-    }
-    __syncthreads();
-    fft126(b, a, P.rroots);  // conj of the cyclic convolution in b
-    for (int w = threadIdx.x; w < T * 126; w += NT) {
-      const int t = w % T, bi = w / T;
-      a[t * LD + __ldg(P.rperm + 126 + bi)] = cadd(x0[t], cconj(b[t * LD + bi]));
-    }
+    fft126(Plain{a}, a, b, Scatter{a, P.rperm + 126, x0}, P.rroots);
     for (int t = threadIdx.x; t < T; t += NT) a[t * LD] = X0[t];
     __syncthreads();
     return a;

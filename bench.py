@@ -53,8 +53,8 @@ def args_():
                     help="requests of the serving-trace sample (0: skip the serving leg)")
     ap.add_argument("--serve-rate", type=float, default=60.0, help="offered request rate of the serving leg (1/s)")
     ap.add_argument("--profile-region", action="store_true",
-                    help="bracket the split-precision leg's timed steps with cudaProfilerStart/Stop "
-                         "(for ncu --profile-from-start off)")
+                    help="bracket the split-precision leg's timed steps (the FP64 leg's with --batch 0) "
+                         "with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
@@ -347,7 +347,7 @@ def run_ours(a):
         ctx.inverse(d_flmn, p, out=d_f)
         ctx.forward(d_f, p, out=d_back)
 
-    r64 = timed_steps(step64, a.steps, a.warmup, stream, ctx, so3, sdist, local, world)
+    r64 = timed_steps(step64, a.steps, a.warmup, stream, ctx, so3, sdist, local, world, a.profile_region and B == 0)
     fp64_value = sdist.job_throughput(world * a.steps, r64["total_ms"] / 1e3)
     rt_err = float(((d_back - d_flmn).abs().max() / d_flmn.abs().max()).item())
     del d_back

@@ -572,49 +572,87 @@ __device__ __forceinline__ void column_scales(const double2* __restrict__ col, i
 
 // Inverse.  One CTA per (nu, block of kMuPer mu, signal): its complex
 // columns (kMuPer mu x combos (+-m, +-nu)) are the rows 8 * (signal % 16)
-// .. +7 of the stage images of its pairs.  Staging: lanes <-> (mu, combo),
-// runs of kMuPer consecutive m per (n, l).  Entries l < max(mu, nu, L0) are
-// zero.
-constexpr int kMuPer = 4;  // 16 staged columns: 64-byte runs of m per (n, l)
-__global__ void __launch_bounds__(256) slice_inv_kernel(SliceArgs a) {
-  extern __shared__ __align__(16) double2 colbuf[];  // [kMuPer mu][4 combos][Lp]
+// .. +7 of the stage images of its pairs.  Entries l < max(mu, nu, L0) are
+// zero.  Two passes over the CTA's flmn entries (runs of kMuPer consecutive
+// m per (n, l)): the first finds the column scales, the second (served
+// mostly by L2, a CTA's entries being a few hundred KB) writes the digits.
+// Nothing is staged in shared memory, so several CTAs per SM keep loads in
+// flight.
+constexpr int kMuPer = 4;  // 64-byte runs of m per (n, l)
+
+struct InvColumn {
+  const double2* src;  // entry l at src[l * l + l]
+  int lmin;
+  bool act, flip;
+};
+__device__ __forceinline__ InvColumn inv_column(const SliceArgs& a, int sig, int mu, int nu, int combo) {
+  const int ms = (combo & 1) ? -1 : 1, ns = (combo & 2) ? -1 : 1;
+  const int m = ms * mu, n = ns * nu;
+  InvColumn c;
+  c.act = mu < a.L && sig < a.nsig && !(ms < 0 && mu == 0) && !(ns < 0 && nu == 0) &&
+          !plane_skipped(a.n_mode, a.N, n);
+  c.lmin = max(max(mu, nu), a.L0);
+  c.flip = ms * ns < 0;
+  c.src = c.act ? a.flmn[sig] + a.base[a.plane0 + n] + m : nullptr;
+  return c;
+}
+// Weighted entry l of the column, (2l+1)/(8 pi^2) (-1)^l on flipped columns.
+__device__ __forceinline__ double inv_entry(const InvColumn& c, int L, int l, int part) {
+  const double x = (c.act && l < L && l >= c.lmin) ? __ldg(reinterpret_cast<const double*>(c.src + (long long)l * l + l) + part)
+                                                  : 0.0;
+  double f = (2.0 * l + 1.0) * kInv8Pi2;
+  if (c.flip && (l & 1)) f = -f;
+  return x * f;
+}
+
+__global__ void __launch_bounds__(256, 3) slice_inv_kernel(SliceArgs a) {
+  __shared__ double wmax[8][2 * 4 * kMuPer];  // [warp][2 (4 j + combo) + part]
   __shared__ double scl[kMuPer][2 * 4];
   const int Lp = a.nchunk * kKC, L = a.L;
   const int nu = blockIdx.x % a.N, mu0 = (blockIdx.x / a.N) * kMuPer, sig = blockIdx.y;
   const int grp = sig / kSig, b = sig % kSig;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   {
     // thread <-> (j, combo) fixed (m fastest across lanes), l = l0 + 16 i;
     // 8 loads in flight per thread
     const int j = threadIdx.x % kMuPer, combo = (threadIdx.x / kMuPer) & 3, l0 = threadIdx.x / (4 * kMuPer);
     constexpr int LSTEP = 256 / (4 * kMuPer);  // l-lanes
-    const int mu = mu0 + j, ms = (combo & 1) ? -1 : 1, ns = (combo & 2) ? -1 : 1;
-    const int m = ms * mu, n = ns * nu;
-    const bool act = mu < L && sig < a.nsig && !(ms < 0 && mu == 0) && !(ns < 0 && nu == 0) &&
-                     !plane_skipped(a.n_mode, a.N, n);
-    const int lmin = max(max(mu, nu), a.L0);
-    const bool flip = ms * ns < 0;
-    const double2* src = act ? a.flmn[sig] + a.base[a.plane0 + n] + m : nullptr;
-    double2* dst = colbuf + (size_t)(j * 4 + combo) * Lp;
-    for (int l1 = l0; l1 < Lp; l1 += LSTEP * 8) {
-      double2 x[8];
+    const InvColumn col = inv_column(a, sig, mu0 + j, nu, combo);
+    double mr = 0.0, mi = 0.0;
+    if (col.act) {
+      for (int l1 = l0; l1 < L; l1 += LSTEP * 8) {
+        double2 x[8];
 #pragma unroll
-      for (int u = 0; u < 8; u++) {
-        const int l = l1 + LSTEP * u;
-        x[u] = (act && l < L && l >= lmin) ? __ldg(src + (long long)l * l + l) : make_double2(0.0, 0.0);
-      }
+        for (int u = 0; u < 8; u++) {
+          const int l = l1 + LSTEP * u;
+          x[u] = (l < L && l >= col.lmin) ? __ldg(col.src + (long long)l * l + l) : make_double2(0.0, 0.0);
+        }
 #pragma unroll
-      for (int u = 0; u < 8; u++) {
-        const int l = l1 + LSTEP * u;
-        if (l >= Lp) break;
-        double f = (2.0 * l + 1.0) * kInv8Pi2;
-        if (flip && (l & 1)) f = -f;
-        dst[l] = make_double2(x[u].x * f, x[u].y * f);
+        for (int u = 0; u < 8; u++) {
+          const int l = l1 + LSTEP * u;
+          double f = (2.0 * l + 1.0) * kInv8Pi2;
+          if (col.flip && (l & 1)) f = -f;
+          mr = fmax(mr, fabs(x[u].x * f));
+          mi = fmax(mi, fabs(x[u].y * f));
+        }
       }
+    }
+    // lanes l and l + 16 of a warp hold the same column
+    mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, 16));
+    mi = fmax(mi, __shfl_xor_sync(0xffffffffu, mi, 16));
+    if (lane < 16) {
+      wmax[warp][2 * (j * 4 + combo)] = mr;
+      wmax[warp][2 * (j * 4 + combo) + 1] = mi;
     }
   }
   __syncthreads();
-  // scales: column (j, combo) -> scl[j][2 combo + part]
-  column_scales<4 * kMuPer>(colbuf, Lp, &scl[0][0]);
+  if (threadIdx.x < 2 * 4 * kMuPer) {
+    double mx = 0.0;
+#pragma unroll
+    for (int w = 0; w < 8; w++) mx = fmax(mx, wmax[w][threadIdx.x]);
+    const int jc = threadIdx.x >> 1, part = threadIdx.x & 1;
+    scl[jc >> 2][2 * (jc & 3) + part] = scale_of(mx);
+  }
   __syncthreads();
   for (int j = 0; j < kMuPer; j++) {
     const int mu = mu0 + j;
@@ -622,23 +660,20 @@ __global__ void __launch_bounds__(256) slice_inv_kernel(SliceArgs a) {
     const size_t gp = (size_t)grp * a.npairs + (size_t)mu * a.N + nu;
     if (threadIdx.x < 8) a.xscale[gp * kM + 8 * b + threadIdx.x] = scl[j][threadIdx.x];
   }
-  // digits: 8 real columns per pair
+  // digits: 8 real columns per pair, 16 entries per work item
   for (int w = threadIdx.x; w < kMuPer * 8 * (Lp / 16); w += blockDim.x) {
     const int c = w & 7, j = (w >> 3) % kMuPer, kb = w / (8 * kMuPer);
     const int mu = mu0 + j;
     if (mu >= L) continue;
     const int combo = c >> 1, part = c & 1;
     const double inv = 1.0 / scl[j][c];
-    const double2* col = colbuf + (size_t)(j * 4 + combo) * Lp;
+    const InvColumn col = inv_column(a, sig, mu, nu, combo);
     uint32_t d[4][kS];
 #pragma unroll
     for (int qd = 0; qd < 4; qd++) {
       double r[4];
 #pragma unroll
-      for (int e = 0; e < 4; e++) {
-        const double2 x = col[16 * kb + 4 * qd + e];
-        r[e] = (part ? x.y : x.x) * inv;
-      }
+      for (int e = 0; e < 4; e++) r[e] = inv_entry(col, L, 16 * kb + 4 * qd + e, part) * inv;
       split_pack4(r, d[qd]);
     }
     const size_t gp = (size_t)grp * a.npairs + (size_t)mu * a.N + nu;
@@ -1350,15 +1385,9 @@ int launch_mixed_inverse(const Geometry& g, int n_mode, const double2* const* fl
   if (int rc = mixed_args(g, n_mode, nsig, scratch, &m, &sa)) return rc;
   sa.flmn = flmn_dev;
   sa.base = bases;
-  const int slice_smem = 4 * kMuPer * (int)sizeof(double2) * nchunks(g) * kKC;  // staged columns x Lp entries
-  if (slice_smem <= 2 * kSliceSmemMax) {
-    SO3G_CUDA(cudaFuncSetAttribute(slice_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, slice_smem));
-    // every signal of the last group (zeros past nsig), so the group's stage images are complete
-    slice_inv_kernel<<<dim3((unsigned)(g.N * ((g.L + kMuPer - 1) / kMuPer)), (unsigned)(((nsig + kSig - 1) / kSig) * kSig)),
-                       256, slice_smem, s>>>(sa);
-  } else {
-    slice_kernel<false><<<dim3((unsigned)sa.npairs, (nsig + kSig - 1) / kSig), 256, 0, s>>>(sa);
-  }
+  // every signal of the last group (zeros past nsig), so the group's stage images are complete
+  slice_inv_kernel<<<dim3((unsigned)(g.N * ((g.L + kMuPer - 1) / kMuPer)), (unsigned)(((nsig + kSig - 1) / kSig) * kSig)),
+                     256, 0, s>>>(sa);
   SO3G_LAUNCHED();
   SO3G_CUDA(cudaGetLastError());
   m.dl = dl;

@@ -153,9 +153,10 @@ __device__ __forceinline__ void pass(const double2* __restrict__ src, double2* _
       const int tws = k * TSTEP;
       if (g == 0) {
         odd_group<R, 1, QS, true, M, NS, TW, SK>(s, j, d, o, roots, tws);
-      } else if (NG == 2 || g == 1) {
-        constexpr int B = NG == 2 ? H : 2 * QS;
-        odd_group<R, QS + 1, B, false, M, NS, TW, SK>(s, j, d, o, roots, tws);
+      } else if constexpr (NG == 2) {
+        odd_group<R, QS + 1, H, false, M, NS, TW, SK>(s, j, d, o, roots, tws);
+      } else if (g == 1) {
+        odd_group<R, QS + 1, 2 * QS, false, M, NS, TW, SK>(s, j, d, o, roots, tws);
       } else {
         odd_group<R, 2 * QS + 1, H, false, M, NS, TW, SK>(s, j, d, o, roots, tws);
       }
@@ -197,13 +198,16 @@ __device__ __forceinline__ void pass_io(const In& in, const Out& out, const doub
 // padded by phys), and run(a, b, P) -> buffer holding the result (a and b:
 // T * LD entries; element i of sequence t at t * LD + phys<sk>(i)).
 
-// 1023 = 31 * 11 * 3 (the MW alpha / extended-beta length at L = 512).
-template <int T, int LD, int NT>
-struct P1023 {
+// 1023 = 31 * 11 * 3 (the MW alpha / extended-beta length at L = 512).  The
+// radix-31 butterflies run as NG output groups (each group reads all 31
+// inputs; fewer groups read shared memory less and need more registers);
+// every output is accumulated in the same order for any NG.
+template <int NG, int T, int LD, int NT>
+struct P1023G {
   static constexpr bool sk = false;
   static constexpr int n = 1023, ld = extent<sk>(1023);
   static __device__ __forceinline__ double2* run(double2* a, double2* b, const FftPlan& P) {
-    pass<1023, 31, 1, T, LD, NT, 3, sk>(a, b, P.roots);
+    pass<1023, 31, 1, T, LD, NT, NG, sk>(a, b, P.roots);
     __syncthreads();
     pass<1023, 11, 31, T, LD, NT, 1, sk>(b, a, P.roots);
     __syncthreads();
@@ -212,6 +216,8 @@ struct P1023 {
     return b;
   }
 };
+template <int T, int LD, int NT>
+using P1023 = P1023G<3, T, LD, NT>;
 
 // 2048 = 8 * 8 * 8 * 4 (the quadrature-weight convolution length at L = 512).
 template <int T, int LD, int NT>

@@ -16,6 +16,8 @@
 //          phase e^{-i m'' pi/(2L-1)} (MW), convolve with the quadrature
 //          weights through a power-of-two oversampled product, and fold
 //          G[m'] + (-1)^{m+n} G[-m'] onto m' >= 0.
+#include <algorithm>
+
 #include "fft_fixed.cuh"
 #include "so3gpu_internal.h"
 
@@ -65,7 +67,7 @@ int set_smem(K kernel, size_t bytes) {
 template <bool BIG>
 struct Gen {
   static constexpr bool fixed = false;
-  static constexpr int NT = kThreads, MINB = BIG ? 1 : 2, T = 0, LD = 0;
+  static constexpr int NT = kThreads, MINB = BIG ? 1 : 2, T = 0, LD = 0, nP = 0;
   static __device__ __forceinline__ int at(int k) { return k; }
   static __device__ __forceinline__ int atC(int k) { return k; }
   static __device__ __forceinline__ double2* runP(double2* a, double2* b, int T_, int ld, const FftPlan& P) {
@@ -81,6 +83,7 @@ struct Fix {
   static constexpr bool fixed = true;
   static constexpr int NT = NT_, MINB = MINB_, T = T_;
   static constexpr int ldP = PP<1, 1, 1>::ld, ldC = PC<1, 1, 1>::ld;
+  static constexpr int nP = PP<1, 1, 1>::n;  // runP length
   static constexpr int ldmax = ldP > ldC ? ldP : ldC;
   // pitch = 8/T (mod 8) 16-byte slots: the T sequences of one index, which
   // consecutive threads handle, fall into distinct banks
@@ -104,6 +107,7 @@ struct Fix {
 using E1023a = Fix<fx::P1023, fx::P1023, 1, 128, 4>;
 using E1023b = Fix<fx::P1023, fx::P1023, 1, 64, 8>;
 using E1023c = Fix<fx::P1023, fx::P1023, 2, 128, 3>;
+using E1023p = Fix<fx::P1023, fx::P1023, 1, 128, 3>;  // persistent inverse alpha (prefetch registers)
 using E127a = Fix<fx::P127, fx::P127, 4, 128, 4>;
 using E127b = Fix<fx::P127, fx::P127, 8, 128, 3>;
 using E127c = Fix<fx::P127, fx::P127, 2, 64, 8>;
@@ -116,6 +120,14 @@ using EConv1023b = Fix<fx::P1023, fx::P2048, 1, 256, 2>;
 __device__ __forceinline__ int wrapi(int k, int P) {
   k %= P;
   return k < 0 ? k + P : k;
+}
+// k mod P for -P < k < P (a signed plane or frequency index)
+__device__ __forceinline__ int wrap1(int k, int P) { return k < 0 ? k + P : k; }
+
+// Offset of row `row` (plane-major over the nb beta rows) of the row-major
+// part of the scratch.
+__device__ __forceinline__ long long row_off(const Geometry& g, int row) {
+  return (long long)(row / g.nb) * g.PS + (long long)(row % g.nb) * g.RS;
 }
 }  // namespace
 
@@ -133,8 +145,8 @@ __global__ void __launch_bounds__(E::NT, E::MINB) inv_beta_kernel(Geometry g, Ff
   const double2* cbase = W + g.QOFF + (long long)plane * g.QS;        // column-major input
   if (!g.mw)
     for (int t = threadIdx.x; t < T; t += E::NT) a[t * ld + E::at(L)] = make_double2(0.0, 0.0);
-  for (int idx = threadIdx.x; idx < L * T; idx += E::NT) {
-    const int mp = idx % L, t = idx / L, c = c0 + t;  // m' fastest: whole columns read contiguously
+  auto load = [&](int t, int mp) {  // m' fastest: whole columns read contiguously
+    const int c = c0 + t;
     double2 v = c < ncols ? cbase[(long long)c * g.CS + mp] : make_double2(0.0, 0.0);
     const int m = c - (L - 1);
     const double sg = ((m + n) & 1) ? -1.0 : 1.0;
@@ -146,6 +158,12 @@ __global__ void __launch_bounds__(E::NT, E::MINB) inv_beta_kernel(Geometry g, Ff
     }
     a[t * ld + E::at(mp)] = cconj(xp);
     if (mp > 0) a[t * ld + E::at(Pn - mp)] = cconj(xn);
+  };
+  if constexpr (E::fixed) {  // no index division per element
+    for (int t = 0; t < E::T; t++)
+      for (int mp = threadIdx.x; mp < L; mp += E::NT) load(t, mp);
+  } else {
+    for (int idx = threadIdx.x; idx < L * T; idx += E::NT) load(idx / L, idx % L);
   }
   __syncthreads();
   double2* r = E::runP(a, b, T, ld, P);
@@ -164,25 +182,38 @@ __global__ void __launch_bounds__(E::NT, E::MINB) inv_alpha_kernel(Geometry g, F
   double2* b = sm + (size_t)T * ld;
   const int L = g.L, Pn = g.P, nrows = g.nplanes * g.nb;
   const int r0 = blockIdx.x * T;
-  for (int idx = threadIdx.x; idx < T * Pn; idx += E::NT) {
-    const int j = idx / Pn, k = idx - j * Pn, row = r0 + j;
+  auto load = [&](int j, int k, long long off, bool ok) {
     double2 v = make_double2(0.0, 0.0);
-    if (row < nrows) {
-      const int m = k <= L - 1 ? k : k - Pn;
-      if (m >= -(L - 1)) {  // MWSS Nyquist index k = L stays zero
-        const long long off = (long long)(row / g.nb) * g.PS + (long long)(row % g.nb) * g.RS;
-        v = W[off + m + L - 1];
-      }
-    }
+    const int m = k <= L - 1 ? k : k - Pn;
+    if (ok && m >= -(L - 1)) v = W[off + m + L - 1];  // MWSS Nyquist index k = L stays zero
     a[j * ld + E::at(k)] = cconj(v);
+  };
+  if constexpr (E::fixed) {  // row offsets once per sequence, no index division per element
+    for (int j = 0; j < E::T; j++) {
+      const int row = r0 + j;
+      const bool ok = row < nrows;
+      const long long off = ok ? row_off(g, row) : 0;
+      for (int k = threadIdx.x; k < E::nP; k += E::NT) load(j, k, off, ok);
+    }
+  } else {
+    for (int idx = threadIdx.x; idx < T * Pn; idx += E::NT) {
+      const int j = idx / Pn, row = r0 + j;
+      load(j, idx - j * Pn, row < nrows ? row_off(g, row) : 0, row < nrows);
+    }
   }
   __syncthreads();
   double2* r = E::runP(a, b, T, ld, P);
-  for (int idx = threadIdx.x; idx < T * g.na; idx += E::NT) {
-    const int j = idx / g.na, k = idx - j * g.na, row = r0 + j;
-    if (row < nrows) {
-      const long long off = (long long)(row / g.nb) * g.PS + (long long)(row % g.nb) * g.RS;
-      W[off + k] = cconj(r[j * ld + E::at(k)]);
+  if constexpr (E::fixed) {
+    for (int j = 0; j < E::T; j++) {
+      const int row = r0 + j;
+      if (row >= nrows) break;
+      double2* dst = W + row_off(g, row);
+      for (int k = threadIdx.x; k < g.na; k += E::NT) dst[k] = cconj(r[j * ld + E::at(k)]);
+    }
+  } else {
+    for (int idx = threadIdx.x; idx < T * g.na; idx += E::NT) {
+      const int j = idx / g.na, k = idx - j * g.na, row = r0 + j;
+      if (row < nrows) W[row_off(g, row) + k] = cconj(r[j * ld + E::at(k)]);
     }
   }
 }
@@ -199,7 +230,7 @@ __global__ void __launch_bounds__(E::NT, E::MINB) inv_gamma_kernel(Geometry g, F
     const int t = idx % T, p = idx / T, al = a0 + t;
     double2 v = al < g.na ? W[(long long)p * g.PS + (long long)row * g.RS + al] : make_double2(0.0, 0.0);
     if (!REAL) {
-      const int k = wrapi(p - g.plane0, ng);
+      const int k = wrap1(p - g.plane0, ng);
       a[t * ld + E::at(k)] = cconj(v);
     } else {
       // Hermitian completion of planes n = 0..N-1, Im of n = 0 ignored
@@ -223,6 +254,92 @@ __global__ void __launch_bounds__(E::NT, E::MINB) inv_gamma_kernel(Geometry g, F
       static_cast<double*>(fout)[o] = y.x;
     else
       static_cast<double2*>(fout)[o] = cconj(y);
+  }
+}
+
+// Persistent variants of the 1023-point stages (one sequence per CTA): a CTA
+// walks the sequences blockIdx.x, + gridDim.x, ... and issues the next
+// sequence's global loads into registers before the current sequence's
+// passes, so the load latency hides behind the DFT.  Same element
+// arithmetic as inv_beta_kernel / inv_alpha_kernel / fwd_alpha_kernel.
+template <class E>
+__global__ void __launch_bounds__(E::NT, E::MINB) inv_beta_pf_kernel(Geometry g, FftPlan P, double2* __restrict__ W) {
+  static_assert(E::fixed && E::T == 1, "one sequence per CTA");
+  extern __shared__ double2 sm[];
+  constexpr int NT = E::NT, Pn = E::nP, NPT = ((Pn + 1) / 2 + NT - 1) / NT;  // L = (Pn + 1) / 2 (MW)
+  double2* a = sm;
+  double2* b = sm + E::LD;
+  const int L = g.L, ncols = 2 * L - 1, ntiles = ncols * g.nplanes;
+  double2 pre[NPT];
+  auto fetch = [&](int tile) {
+    const int plane = tile / ncols, c = tile - plane * ncols;
+    const double2* cbase = W + g.QOFF + (long long)plane * g.QS + (long long)c * g.CS;
+#pragma unroll
+    for (int i = 0; i < NPT; i++) {
+      const int mp = threadIdx.x + i * NT;
+      pre[i] = mp < L ? cbase[mp] : make_double2(0.0, 0.0);
+    }
+  };
+  int tile = blockIdx.x;
+  if (tile < ntiles) fetch(tile);
+  for (; tile < ntiles; tile += gridDim.x) {
+    const int plane = tile / ncols, c = tile - plane * ncols, n = plane - g.plane0;
+    const int m = c - (L - 1);
+    const double sg = ((m + n) & 1) ? -1.0 : 1.0;
+    if (!g.mw && threadIdx.x == 0) a[E::at(L)] = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int i = 0; i < NPT; i++) {
+      const int mp = threadIdx.x + i * NT;
+      if (mp >= L) break;
+      const double2 v = pre[i];
+      double2 xp = v, xn = make_double2(sg * v.x, sg * v.y);
+      if (g.mw) {
+        const double2 e = cconj(__ldg(P.half + mp));  // e^{i pi m'/(2L-1)}
+        xp = cmul(xp, e);
+        xn = cmul(xn, cconj(e));
+      }
+      a[E::at(mp)] = cconj(xp);
+      if (mp > 0) a[E::at(Pn - mp)] = cconj(xn);
+    }
+    __syncthreads();
+    if (tile + gridDim.x < ntiles) fetch(tile + gridDim.x);
+    double2* r = E::runP(a, b, 1, E::LD, P);
+    double2* base = W + (long long)plane * g.PS + c;
+    for (int row = threadIdx.x; row < g.nb; row += NT) base[(long long)row * g.RS] = cconj(r[E::at(row)]);
+  }
+}
+
+template <class E>
+__global__ void __launch_bounds__(E::NT, E::MINB) inv_alpha_pf_kernel(Geometry g, FftPlan P, double2* __restrict__ W) {
+  static_assert(E::fixed && E::T == 1, "one sequence per CTA");
+  extern __shared__ double2 sm[];
+  constexpr int NT = E::NT, Pn = E::nP, NPT = (Pn + NT - 1) / NT;
+  double2* a = sm;
+  double2* b = sm + E::LD;
+  const int L = g.L, nrows = g.nplanes * g.nb;
+  double2 pre[NPT];
+  auto fetch = [&](int row) {
+    const double2* src = W + row_off(g, row) + (L - 1);
+#pragma unroll
+    for (int i = 0; i < NPT; i++) {
+      const int k = threadIdx.x + i * NT;
+      const int m = k <= L - 1 ? k : k - Pn;
+      pre[i] = (k < Pn && m >= -(L - 1)) ? src[m] : make_double2(0.0, 0.0);  // MWSS Nyquist k = L stays zero
+    }
+  };
+  int row = blockIdx.x;
+  if (row < nrows) fetch(row);
+  for (; row < nrows; row += gridDim.x) {
+#pragma unroll
+    for (int i = 0; i < NPT; i++) {
+      const int k = threadIdx.x + i * NT;
+      if (k < Pn) a[E::at(k)] = cconj(pre[i]);
+    }
+    __syncthreads();
+    if (row + gridDim.x < nrows) fetch(row + gridDim.x);
+    double2* r = E::runP(a, b, 1, E::LD, P);
+    double2* dst = W + row_off(g, row);
+    for (int k = threadIdx.x; k < g.na; k += NT) dst[k] = cconj(r[E::at(k)]);
   }
 }
 
@@ -254,7 +371,7 @@ __global__ void __launch_bounds__(E::NT, E::MINB) fwd_gamma_kernel(Geometry g, F
   for (int idx = threadIdx.x; idx < g.nplanes * T; idx += E::NT) {
     const int t = idx % T, p = idx / T, al = a0 + t;
     if (al >= g.na) continue;
-    const int k = REAL ? p : wrapi(p - g.plane0, ng);
+    const int k = REAL ? p : wrap1(p - g.plane0, ng);
     W[(long long)p * g.PS + (long long)row * g.RS + al] = cscale(r[t * ld + E::at(k)], scale);
   }
 }
@@ -268,21 +385,69 @@ __global__ void __launch_bounds__(E::NT, E::MINB) fwd_alpha_kernel(Geometry g, F
   double2* b = sm + (size_t)T * ld;
   const int L = g.L, Pn = g.P, nrows = g.nplanes * g.nb, ncols = 2 * L - 1;
   const int r0 = blockIdx.x * T;
-  for (int idx = threadIdx.x; idx < T * Pn; idx += E::NT) {
-    const int j = idx / Pn, k = idx - j * Pn, row = r0 + j;
-    double2 v = make_double2(0.0, 0.0);
-    if (row < nrows) v = W[(long long)(row / g.nb) * g.PS + (long long)(row % g.nb) * g.RS + k];
-    a[j * ld + E::at(k)] = v;
+  if constexpr (E::fixed) {  // row offsets once per sequence, no index division per element
+    for (int j = 0; j < E::T; j++) {
+      const int row = r0 + j;
+      const double2* src = W + (row < nrows ? row_off(g, row) : 0);
+      for (int k = threadIdx.x; k < E::nP; k += E::NT)
+        a[j * ld + E::at(k)] = row < nrows ? src[k] : make_double2(0.0, 0.0);
+    }
+  } else {
+    for (int idx = threadIdx.x; idx < T * Pn; idx += E::NT) {
+      const int j = idx / Pn, k = idx - j * Pn, row = r0 + j;
+      a[j * ld + E::at(k)] = row < nrows ? W[row_off(g, row) + k] : make_double2(0.0, 0.0);
+    }
   }
   __syncthreads();
   double2* r = E::runP(a, b, T, ld, P);
   const double inv = 1.0 / Pn;
-  for (int idx = threadIdx.x; idx < T * ncols; idx += E::NT) {
-    const int j = idx / ncols, c = idx - j * ncols, row = r0 + j;
-    if (row < nrows) {
-      const int k = wrapi(c - (L - 1), Pn);
-      W[(long long)(row / g.nb) * g.PS + (long long)(row % g.nb) * g.RS + c] = cscale(r[j * ld + E::at(k)], inv);
+  if constexpr (E::fixed) {
+    for (int j = 0; j < E::T; j++) {
+      const int row = r0 + j;
+      if (row >= nrows) break;
+      double2* dst = W + row_off(g, row);
+      for (int c = threadIdx.x; c < ncols; c += E::NT)
+        dst[c] = cscale(r[j * ld + E::at(wrap1(c - (L - 1), Pn))], inv);
     }
+  } else {
+    for (int idx = threadIdx.x; idx < T * ncols; idx += E::NT) {
+      const int j = idx / ncols, c = idx - j * ncols, row = r0 + j;
+      if (row < nrows) W[row_off(g, row) + c] = cscale(r[j * ld + E::at(wrap1(c - (L - 1), Pn))], inv);
+    }
+  }
+}
+
+template <class E>
+__global__ void __launch_bounds__(E::NT, E::MINB) fwd_alpha_pf_kernel(Geometry g, FftPlan P, double2* __restrict__ W) {
+  static_assert(E::fixed && E::T == 1, "one sequence per CTA");
+  extern __shared__ double2 sm[];
+  constexpr int NT = E::NT, Pn = E::nP, NPT = (Pn + NT - 1) / NT;
+  double2* a = sm;
+  double2* b = sm + E::LD;
+  const int L = g.L, nrows = g.nplanes * g.nb, ncols = 2 * L - 1;
+  const double inv = 1.0 / Pn;
+  double2 pre[NPT];
+  auto fetch = [&](int row) {
+    const double2* src = W + row_off(g, row);
+#pragma unroll
+    for (int i = 0; i < NPT; i++) {
+      const int k = threadIdx.x + i * NT;
+      pre[i] = k < Pn ? src[k] : make_double2(0.0, 0.0);
+    }
+  };
+  int row = blockIdx.x;
+  if (row < nrows) fetch(row);
+  for (; row < nrows; row += gridDim.x) {
+#pragma unroll
+    for (int i = 0; i < NPT; i++) {
+      const int k = threadIdx.x + i * NT;
+      if (k < Pn) a[E::at(k)] = pre[i];
+    }
+    __syncthreads();
+    if (row + gridDim.x < nrows) fetch(row + gridDim.x);
+    double2* r = E::runP(a, b, 1, E::LD, P);
+    double2* dst = W + row_off(g, row);
+    for (int c = threadIdx.x; c < ncols; c += NT) dst[c] = cscale(r[E::at(wrap1(c - (L - 1), Pn))], inv);
   }
 }
 
@@ -379,6 +544,48 @@ int inv_beta(const Geometry& g, const FftPlan& p, double2* W, cudaStream_t s) {
   inv_beta_kernel<E><<<grid, E::NT, z.smem, s>>>(g, p, W, z.T, p.ld());
   return kOk;
 }
+// Grid of a persistent kernel: as many CTAs as fit on the device at once.
+template <typename K>
+int persistent_grid(K kernel, int nt, size_t smem, int ntiles, int* grid) {
+  int dev = 0, sms = 0, per_sm = 0;
+  SO3G_CUDA(cudaGetDevice(&dev));
+  SO3G_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  SO3G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, nt, smem));
+  *grid = std::max(1, std::min(ntiles, sms * std::max(per_sm, 1)));
+  return kOk;
+}
+
+template <class E>
+int inv_beta_pf(const Geometry& g, const FftPlan& p, double2* W, cudaStream_t s) {
+  if (g.P != 2 * g.L - 1) return fail(kUnsupported, "persistent beta stage needs MW sampling");
+  const size_t smem = 2 * (size_t)E::LD * sizeof(double2);
+  if (int rc = set_smem(inv_beta_pf_kernel<E>, smem)) return rc;
+  int grid = 0;
+  if (int rc = persistent_grid(inv_beta_pf_kernel<E>, E::NT, smem, (2 * g.L - 1) * g.nplanes, &grid)) return rc;
+  inv_beta_pf_kernel<E><<<grid, E::NT, smem, s>>>(g, p, W);
+  return kOk;
+}
+
+template <class E>
+int inv_alpha_pf(const Geometry& g, const FftPlan& p, double2* W, cudaStream_t s) {
+  const size_t smem = 2 * (size_t)E::LD * sizeof(double2);
+  if (int rc = set_smem(inv_alpha_pf_kernel<E>, smem)) return rc;
+  int grid = 0;
+  if (int rc = persistent_grid(inv_alpha_pf_kernel<E>, E::NT, smem, g.nplanes * g.nb, &grid)) return rc;
+  inv_alpha_pf_kernel<E><<<grid, E::NT, smem, s>>>(g, p, W);
+  return kOk;
+}
+
+template <class E>
+int fwd_alpha_pf(const Geometry& g, const FftPlan& p, double2* W, cudaStream_t s) {
+  const size_t smem = 2 * (size_t)E::LD * sizeof(double2);
+  if (int rc = set_smem(fwd_alpha_pf_kernel<E>, smem)) return rc;
+  int grid = 0;
+  if (int rc = persistent_grid(fwd_alpha_pf_kernel<E>, E::NT, smem, g.nplanes * g.nb, &grid)) return rc;
+  fwd_alpha_pf_kernel<E><<<grid, E::NT, smem, s>>>(g, p, W);
+  return kOk;
+}
+
 template <class E>
 int inv_alpha(const Geometry& g, const FftPlan& p, double2* W, cudaStream_t s) {
   const Sizing z = sizing<E>(p.ld(), 16);
@@ -438,7 +645,10 @@ int launch_inv_beta(const Geometry& g, const FftPlan& p, double2* W, cudaStream_
   const int v = g.var[kStInvBeta];
   switch (pick(p)) {
     case Eng::k1023:
-      rc = v == 1 ? inv_beta<E1023b>(g, p, W, s) : v == 2 ? inv_beta<E1023c>(g, p, W, s) : inv_beta<E1023a>(g, p, W, s);
+      rc = v == 1   ? inv_beta<E1023b>(g, p, W, s)
+           : v == 2 ? inv_beta<E1023c>(g, p, W, s)
+           : v == 3 ? inv_beta_pf<E1023a>(g, p, W, s)
+                    : inv_beta<E1023a>(g, p, W, s);
       break;
     case Eng::k127:
       rc = v == 1 ? inv_beta<E127b>(g, p, W, s) : v == 2 ? inv_beta<E127c>(g, p, W, s) : inv_beta<E127a>(g, p, W, s);
@@ -457,8 +667,10 @@ int launch_inv_alpha(const Geometry& g, const FftPlan& p, double2* W, cudaStream
   const int v = g.var[kStInvAlpha];
   switch (pick(p)) {
     case Eng::k1023:
-      rc = v == 1 ? inv_alpha<E1023b>(g, p, W, s) : v == 2 ? inv_alpha<E1023c>(g, p, W, s)
-                                                           : inv_alpha<E1023a>(g, p, W, s);
+      rc = v == 1   ? inv_alpha<E1023b>(g, p, W, s)
+           : v == 2 ? inv_alpha<E1023c>(g, p, W, s)
+           : v == 3 ? inv_alpha_pf<E1023p>(g, p, W, s)
+                    : inv_alpha<E1023a>(g, p, W, s);
       break;
     case Eng::k127:
       rc = v == 1 ? inv_alpha<E127b>(g, p, W, s) : v == 2 ? inv_alpha<E127c>(g, p, W, s) : inv_alpha<E127a>(g, p, W, s);
@@ -528,8 +740,10 @@ int launch_fwd_alpha(const Geometry& g, const FftPlan& p, double2* W, cudaStream
   const int v = g.var[kStFwdAlpha];
   switch (pick(p)) {
     case Eng::k1023:
-      rc = v == 1 ? fwd_alpha<E1023b>(g, p, W, s) : v == 2 ? fwd_alpha<E1023c>(g, p, W, s)
-                                                           : fwd_alpha<E1023a>(g, p, W, s);
+      rc = v == 1   ? fwd_alpha<E1023b>(g, p, W, s)
+           : v == 2 ? fwd_alpha<E1023c>(g, p, W, s)
+           : v == 3 ? fwd_alpha_pf<E1023a>(g, p, W, s)
+                    : fwd_alpha<E1023a>(g, p, W, s);
       break;
     case Eng::k127:
       rc = v == 1 ? fwd_alpha<E127b>(g, p, W, s) : v == 2 ? fwd_alpha<E127c>(g, p, W, s) : fwd_alpha<E127a>(g, p, W, s);
@@ -566,7 +780,8 @@ int stage_variants(const Geometry& g, const FftPlan& pP, const FftPlan& pg, cons
   switch (stage) {
     case kStInvBeta:
     case kStInvAlpha:
-    case kStFwdAlpha: return (pick(pP) == Eng::k1023 || pick(pP) == Eng::k127 || pick(pP) == Eng::k127r) ? 3 : 1;
+    case kStFwdAlpha:
+      return pick(pP) == Eng::k1023 ? 4 : (pick(pP) == Eng::k127 || pick(pP) == Eng::k127r) ? 3 : 1;
     case kStInvGamma:
     case kStFwdGamma: return (!g.real && (pick(pg) == Eng::k127 || pick(pg) == Eng::k127r)) ? 3 : 1;
     case kStFwdBetaConv: return conv_fixed(pP, pc) ? 2 : 1;

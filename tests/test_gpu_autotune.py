@@ -26,7 +26,7 @@ def test_every_variant_gives_identical_results(L, N):
     fl = torch.from_numpy(synth.gen_flmn(p, 21)).cuda()
     ctx = so3.Context(0)
     outs = []
-    for v in (0, 1, 2):
+    for v in (0, 1, 2, 3):
         _vars(lib, p, [v] * 8)
         f = ctx.inverse(fl, p)
         back = ctx.forward(f, p)
@@ -44,7 +44,7 @@ def test_prepare_tunes_and_records_variants():
     ctx.prepare(p)
     got = (ctypes.c_int * 8)()
     assert lib.so3gpu_get_stage_variants(0, ctypes.byref(p.to_struct()), got) == 1
-    # inverse beta / alpha and forward alpha have three 1023-point variants,
+    # inverse beta / alpha and forward alpha have four 1023-point variants,
     # forward beta two; the gamma stages (length 5) only the default
-    assert all(0 <= got[i] <= 2 for i in (1, 2, 5)) and 0 <= got[6] <= 1
+    assert all(0 <= got[i] <= 3 for i in (1, 2, 5)) and 0 <= got[6] <= 1
     assert got[3] == 0 and got[4] == 0

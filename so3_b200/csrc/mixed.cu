@@ -424,151 +424,10 @@ __device__ __forceinline__ double scale_of(double mx) {  // power of two with |x
   return mx > 0.0 ? ldexp(1.0, ex + 1) : 1.0;
 }
 
-// Two-pass slicing (band limits whose staged columns exceed shared memory):
-// one CTA per (pair, group of 16 signals), thread <-> real column c and every
-// other 16-entry block; pass 1 finds the scales, pass 2 writes the digits.
-// Column c of one pair: the source pointer and the stride between
-// consecutive reduction entries (inverse: l^2 + l + m grows by 2l + 2),
-// resolved once per thread.
-struct Column {
-  const double* src;  // real or imaginary part of entry k = 0 (inverse: of l = 0)
-  bool active, flip_odd;
-  int kmin;
-};
-
-template <bool FWD>
-__device__ __forceinline__ Column column_of(const SliceArgs& a, int sig, int mu, int nu, int combo, int part) {
-  Column col{nullptr, false, false, 0};
-  const int ms = (combo & 1) ? -1 : 1, ns = (combo & 2) ? -1 : 1;
-  if (sig >= a.nsig || (ms < 0 && mu == 0) || (ns < 0 && nu == 0)) return col;
-  const int m = ms * mu, n = ns * nu;
-  if (plane_skipped(a.n_mode, a.N, n)) return col;
-  col.active = true;
-  col.flip_odd = ms * ns < 0;
-  if (!FWD) {
-    col.kmin = max(max(mu, nu), a.L0);
-    col.src = reinterpret_cast<const double*>(a.flmn[sig] + a.base[a.plane0 + n] + m) + part;
-  } else {
-    col.src = reinterpret_cast<const double*>(a.W + (long long)sig * a.wstride + (long long)(a.plane0 + n) * a.QS +
-                                              (long long)(m + a.L - 1) * a.CS) + part;
-  }
-  return col;
-}
-
-// The 16 entries k0 .. k0+15 of a column (zero outside the band limit).
-template <bool FWD>
-__device__ __forceinline__ void column_block(const SliceArgs& a, const Column& col, int k0, double (&v)[16]) {
-#pragma unroll
-  for (int e = 0; e < 16; e++) {
-    const int k = k0 + e;
-    double x = 0.0;
-    if (col.active && k < a.L && k >= col.kmin) {
-      if (!FWD) x = __ldg(col.src + 2LL * ((long long)k * k + k)) * ((2.0 * k + 1.0) * kInv8Pi2);
-      else x = __ldg(col.src + 2LL * k);
-      if (col.flip_odd && (k & 1)) x = -x;
-    }
-    v[e] = x;
-  }
-}
-
-template <bool FWD>
-__global__ void __launch_bounds__(256) slice_kernel(SliceArgs a) {
-  __shared__ double colmax[2][kM];
-  const int c = threadIdx.x & (kM - 1), half = threadIdx.x >> 7;
-  const int pair = blockIdx.x, grp = blockIdx.y;
-  const int nu = pair % a.N, mu = pair / a.N;
-  const int b = c >> 3, combo = (c >> 1) & 3, part = c & 1, sig = grp * kSig + b;
-  const size_t gp = (size_t)grp * a.npairs + pair;
-  const int nblk = a.nchunk * (kKC / 16);
-  const Column col = column_of<FWD>(a, sig, mu, nu, combo, part);
-  double mx = 0.0;
-  for (int kb = half; kb < nblk; kb += 2) {
-    double v[16];
-    column_block<FWD>(a, col, 16 * kb, v);
-#pragma unroll
-    for (int e = 0; e < 16; e++) mx = fmax(mx, fabs(v[e]));
-  }
-  colmax[half][c] = mx;
-  __syncthreads();
-  mx = fmax(colmax[0][c], colmax[1][c]);
-  int ex = 0;
-  frexp(mx, &ex);
-  const double scale = mx > 0.0 ? ldexp(1.0, ex + 1) : 1.0;  // |x / scale| < 1/2
-  const double inv = 1.0 / scale;                              // exact (power of two)
-  if (half == 0) a.xscale[gp * kM + c] = scale;
-  uint8_t* out = a.xs + gp * (size_t)a.nchunk * kXStage;
-  for (int kb = half; kb < nblk; kb += 2) {
-    double v[16];
-    column_block<FWD>(a, col, 16 * kb, v);
-    uint32_t w[4][kS];
-#pragma unroll
-    for (int qd = 0; qd < 4; qd++) {
-      double r[4];
-#pragma unroll
-      for (int e = 0; e < 4; e++) r[e] = v[4 * qd + e] * inv;
-      split_pack4(r, w[qd]);
-    }
-    const int chunk = kb >> 2, kin = (kb & 3) * 16;
-    uint8_t* dst = out + (size_t)chunk * kXStage + tile_off(kM, c, kin);
-#pragma unroll
-    for (int i = 0; i < kS; i++)
-      *reinterpret_cast<uint4*>(dst + i * (kM * kKC)) = make_uint4(w[0][i], w[1][i], w[2][i], w[3][i]);
-  }
-}
-
-
-// Single-pass slicing: a CTA stages its columns (complex, all reduction
-// entries) in shared memory with coalesced loads, finds each column's scale
-// with a warp reduction, then writes 16-entry digit slots.
-constexpr int kSliceCols = 8;  // complex columns per slicing CTA (4 sign combinations x 2)
-constexpr int kSliceSmemMax = 100 * 1024;  // staged columns fit (L <= 768)
-
-// Digits of the staged columns: thread <-> (real column c of the CTA's 32,
-// block of 16 entries); c_base: first row of the stage image.
-__device__ __forceinline__ void slice_from_smem(const double2* __restrict__ col, int Lp, const double* scl,
-                                                uint8_t* pb, int c_base) {
-  const int nblk = Lp / 16;
-  for (int w = threadIdx.x; w < 2 * kSliceCols * nblk; w += blockDim.x) {
-    const int c = w % (2 * kSliceCols), kb = w / (2 * kSliceCols), cc = c >> 1, part = c & 1;
-    const double inv = 1.0 / scl[c];
-    uint32_t d[4][kS];
-#pragma unroll
-    for (int qd = 0; qd < 4; qd++) {
-      double r[4];
-#pragma unroll
-      for (int e = 0; e < 4; e++) {
-        const double2 x = col[(size_t)cc * Lp + 16 * kb + 4 * qd + e];
-        r[e] = (part ? x.y : x.x) * inv;
-      }
-      split_pack4(r, d[qd]);
-    }
-    uint8_t* dst = pb + (size_t)(kb >> 2) * kXStage + tile_off(kM, c_base + c, (kb & 3) * 16);
-#pragma unroll
-    for (int i = 0; i < kS; i++)
-      *reinterpret_cast<uint4*>(dst + i * (kM * kKC)) = make_uint4(d[0][i], d[1][i], d[2][i], d[3][i]);
-  }
-}
-
-// Largest magnitude of the real and imaginary parts of each staged column
-// (warp w handles columns w, w + 8); scales into scl[2 cc + part].
-template <int NC>
-__device__ __forceinline__ void column_scales(const double2* __restrict__ col, int Lp, double* scl) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int cc = warp; cc < NC; cc += nw) {
-    double mr = 0.0, mi = 0.0;
-    for (int k = lane; k < Lp; k += 32) {
-      const double2 x = col[(size_t)cc * Lp + k];
-      mr = fmax(mr, fabs(x.x));
-      mi = fmax(mi, fabs(x.y));
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, o));
-      mi = fmax(mi, __shfl_xor_sync(0xffffffffu, mi, o));
-    }
-    if (lane == 0) scl[2 * cc] = scale_of(mr), scl[2 * cc + 1] = scale_of(mi);
-  }
-}
+// Slicing: each CTA reads its columns twice (scales, then digits; the second
+// read is served mostly by L2) and writes 16-entry digit slots of the stage
+// images; nothing is staged in shared memory.
+constexpr int kSliceCols = 8;  // complex columns per forward slicing CTA (4 sign combinations x 2 signals)
 
 // Inverse.  One CTA per (nu, block of kMuPer mu, signal): its complex
 // columns (kMuPer mu x combos (+-m, +-nu)) are the rows 8 * (signal % 16)
@@ -690,8 +549,25 @@ __global__ void __launch_bounds__(256, 3) slice_inv_kernel(SliceArgs a) {
 // q-th set of kSigPer signals of the group); warp <-> column, lanes along m'
 // (512-byte runs).
 constexpr int kSigPer = kSliceCols / 4;
+struct FwdColumn {
+  const double2* src;  // entry k (m') at src[k]
+  bool act, flip;
+};
+__device__ __forceinline__ FwdColumn fwd_column(const SliceArgs& a, int sig, int mu, int nu, int combo) {
+  const int ms = (combo & 1) ? -1 : 1, ns = (combo & 2) ? -1 : 1;
+  const int m = ms * mu, n = ns * nu;
+  FwdColumn c;
+  c.act = sig < a.nsig && !(ms < 0 && mu == 0) && !(ns < 0 && nu == 0) && !plane_skipped(a.n_mode, a.N, n);
+  c.flip = ms * ns < 0;
+  c.src = c.act ? a.W + (long long)sig * a.wstride + (long long)(a.plane0 + n) * a.QS + (long long)(m + a.L - 1) * a.CS
+                : nullptr;
+  return c;
+}
+
+// Two passes over the CTA's columns (contiguous runs of m'): warp cc finds
+// the scales of column cc, then every thread writes 16-entry digit slots
+// from a second read (served mostly by L2).  No staging in shared memory.
 __global__ void __launch_bounds__(256) slice_fwd_kernel(SliceArgs a) {
-  extern __shared__ __align__(16) double2 colbuf[];  // [kSliceCols columns][Lp]
   __shared__ double scl[2 * kSliceCols];
   const int Lp = a.nchunk * kKC, L = a.L;
   const int pair = blockIdx.x, q4 = blockIdx.y;  // q4: set of kSigPer signals
@@ -699,35 +575,58 @@ __global__ void __launch_bounds__(256) slice_fwd_kernel(SliceArgs a) {
   const int grp = (kSigPer * q4) / kSig, qin = q4 % (kSig / kSigPer);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int cc = warp; cc < kSliceCols; cc += 8) {
-    const int sig = kSigPer * q4 + (cc >> 2), combo = cc & 3;
-    const int ms = (combo & 1) ? -1 : 1, ns = (combo & 2) ? -1 : 1;
-    const int m = ms * mu, n = ns * nu;
-    const bool act = sig < a.nsig && !(ms < 0 && mu == 0) && !(ns < 0 && nu == 0) && !plane_skipped(a.n_mode, a.N, n);
-    const bool flip = ms * ns < 0;
-    const double2* src =
-        act ? a.W + (long long)sig * a.wstride + (long long)(a.plane0 + n) * a.QS + (long long)(m + L - 1) * a.CS
-            : nullptr;
-    for (int k1 = lane; k1 < Lp; k1 += 32 * 8) {  // 8 loads in flight per lane
-      double2 x[8];
+    const FwdColumn col = fwd_column(a, kSigPer * q4 + (cc >> 2), mu, nu, cc & 3);
+    double mr = 0.0, mi = 0.0;
+    if (col.act) {
+      for (int k1 = lane; k1 < L; k1 += 32 * 8) {  // 8 loads in flight per lane
+        double2 x[8];
 #pragma unroll
-      for (int u = 0; u < 8; u++) {
-        const int k = k1 + 32 * u;
-        x[u] = (act && k < L) ? __ldg(src + k) : make_double2(0.0, 0.0);
-      }
+        for (int u = 0; u < 8; u++) {
+          const int k = k1 + 32 * u;
+          x[u] = k < L ? __ldg(col.src + k) : make_double2(0.0, 0.0);
+        }
 #pragma unroll
-      for (int u = 0; u < 8; u++) {
-        const int k = k1 + 32 * u;
-        if (k >= Lp) break;
-        colbuf[(size_t)cc * Lp + k] = (flip && (k & 1)) ? make_double2(-x[u].x, -x[u].y) : x[u];
+        for (int u = 0; u < 8; u++) {
+          mr = fmax(mr, fabs(x[u].x));
+          mi = fmax(mi, fabs(x[u].y));
+        }
       }
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, o));
+      mi = fmax(mi, __shfl_xor_sync(0xffffffffu, mi, o));
+    }
+    if (lane == 0) scl[2 * cc] = scale_of(mr), scl[2 * cc + 1] = scale_of(mi);
   }
-  __syncthreads();
-  column_scales<kSliceCols>(colbuf, Lp, scl);
   __syncthreads();
   const size_t gp = (size_t)grp * a.npairs + pair;
   if (threadIdx.x < 2 * kSliceCols) a.xscale[gp * kM + 2 * kSliceCols * qin + threadIdx.x] = scl[threadIdx.x];
-  slice_from_smem(colbuf, Lp, scl, a.xs + gp * (size_t)a.nchunk * kXStage, 2 * kSliceCols * qin);
+  uint8_t* pb = a.xs + gp * (size_t)a.nchunk * kXStage;
+  const int c_base = 2 * kSliceCols * qin, nblk = Lp / 16;
+  for (int w = threadIdx.x; w < 2 * kSliceCols * nblk; w += blockDim.x) {
+    const int c = w % (2 * kSliceCols), kb = w / (2 * kSliceCols), cc = c >> 1, part = c & 1;
+    const FwdColumn col = fwd_column(a, kSigPer * q4 + (cc >> 2), mu, nu, cc & 3);
+    const double inv = 1.0 / scl[c];
+    const double* src = reinterpret_cast<const double*>(col.src) + part;
+    uint32_t d[4][kS];
+#pragma unroll
+    for (int qd = 0; qd < 4; qd++) {
+      double r[4];
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const int k = 16 * kb + 4 * qd + e;
+        double x = (col.act && k < L) ? __ldg(src + 2 * k) : 0.0;
+        if (col.flip && (k & 1)) x = -x;
+        r[e] = x * inv;
+      }
+      split_pack4(r, d[qd]);
+    }
+    uint8_t* dst = pb + (size_t)(kb >> 2) * kXStage + tile_off(kM, c_base + c, (kb & 3) * 16);
+#pragma unroll
+    for (int i = 0; i < kS; i++)
+      *reinterpret_cast<uint4*>(dst + i * (kM * kKC)) = make_uint4(d[0][i], d[1][i], d[2][i], d[3][i]);
+  }
 }
 
 // ---------------------------------------------------------------- persistent form
@@ -1408,14 +1307,8 @@ int launch_mixed_forward(const Geometry& g, int n_mode, const double2* W, long l
   sa.W = W + g.QOFF;
   sa.wstride = wstride;
   sa.base = bases;
-  const int slice_smem = kSliceCols * (int)sizeof(double2) * nchunks(g) * kKC;
-  if (slice_smem <= kSliceSmemMax) {
-    SO3G_CUDA(cudaFuncSetAttribute(slice_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, slice_smem));
-    slice_fwd_kernel<<<dim3((unsigned)sa.npairs, (unsigned)(((nsig + kSig - 1) / kSig) * (kSig / kSigPer))), 256,
-                       slice_smem, s>>>(sa);
-  } else {
-    slice_kernel<true><<<dim3((unsigned)sa.npairs, (nsig + kSig - 1) / kSig), 256, 0, s>>>(sa);
-  }
+  slice_fwd_kernel<<<dim3((unsigned)sa.npairs, (unsigned)(((nsig + kSig - 1) / kSig) * (kSig / kSigPer))), 256, 0,
+                     s>>>(sa);
   SO3G_LAUNCHED();
   SO3G_CUDA(cudaGetLastError());
   m.dl = dl;

@@ -205,6 +205,7 @@ __device__ __forceinline__ void pass_io(const In& in, const Out& out, const doub
 template <int NG, int T, int LD, int NT>
 struct P1023G {
   static constexpr bool sk = false;
+  static constexpr bool io = false;  // no run_io form
   static constexpr int n = 1023, ld = extent<sk>(1023);
   static __device__ __forceinline__ double2* run(double2* a, double2* b, const FftPlan& P) {
     pass<1023, 31, 1, T, LD, NT, NG, sk>(a, b, P.roots);
@@ -223,6 +224,7 @@ using P1023 = P1023G<3, T, LD, NT>;
 template <int T, int LD, int NT>
 struct P2048 {
   static constexpr bool sk = true;
+  static constexpr bool io = false;  // no run_io form
   static constexpr int n = 2048, ld = extent<sk>(2048);
   static __device__ __forceinline__ double2* run(double2* a, double2* b, const FftPlan& P) {
     pass<2048, 8, 1, T, LD, NT, 1, sk>(a, b, P.roots);
@@ -253,6 +255,7 @@ __device__ __forceinline__ double2* fft256(double2* a, double2* b, const double2
 template <int T, int LD, int NT>
 struct P127 {
   static constexpr bool sk = true;
+  static constexpr bool io = false;  // no run_io form
   static constexpr int n = 127, ld = extent<sk>(256);
   static __device__ __forceinline__ double2* run(double2* a, double2* b, const FftPlan& P) {
     for (int w = threadIdx.x; w < T * 256; w += NT) {
@@ -282,13 +285,14 @@ struct P127 {
 
 // 127 (prime) by Rader's algorithm: with the primitive root 3,
 //   X[3^{-b}] = x[0] + sum_{a < 126} x[3^a] w^{3^{a-b}},   X[0] = sum_n x[n],
-// a cyclic convolution of length 126 = 7 * 3 * 3 * 2 evaluated as
+// a cyclic convolution of length 126 = 7 * 9 * 2 evaluated as
 // conj(FFT(conj(FFT(u) * V))) with V = FFT(v) / 126 precomputed.  About half
 // the arithmetic of Bluestein over 256 and half its shared memory.  The
 // gather x[3^a] rides on the first pass of the first FFT, the product with V
 // (and the conjugation) on its last pass, the scatter to X[3^{-b}] on the
-// last pass of the second FFT: eight passes, no separate shared-memory
-// sweeps.  Input x in a (entries 0..126); returns the buffer holding X.
+// last pass of the second FFT: six passes, no separate shared-memory sweeps
+// (the stage is bound by shared-memory traffic).  Input x in a (entries
+// 0..126); returns the buffer holding X.
 template <int T, int LD, int NT>
 struct P127R {
   static constexpr bool sk = false;
@@ -298,10 +302,11 @@ struct P127R {
     __device__ double2 operator()(int t, int i) const { return p[t * LD + i]; }
     __device__ void operator()(int t, int i, double2 v) const { p[t * LD + i] = v; }
   };
+  template <class In>
   struct Gather {  // element a of the convolution input: x[3^a]
-    const double2* p;
+    const In& in;
     const int* perm;
-    __device__ double2 operator()(int t, int i) const { return p[t * LD + __ldg(perm + i)]; }
+    __device__ double2 operator()(int t, int i) const { return in(t, __ldg(perm + i)); }
   };
   struct Kernel {  // conj(U[k] V[k]); X[0] = x[0] + U[0]
     double2* p;
@@ -313,32 +318,42 @@ struct P127R {
       p[t * LD + k] = cconj(cmul(u, __ldg(kern + k)));
     }
   };
+  template <class Out>
   struct Scatter {  // X[3^{-b}] = x[0] + conj(second FFT)[b]
-    double2* p;
+    const Out& out;
     const int* perm;
     const double2* x0;
-    __device__ void operator()(int t, int b, double2 v) const { p[t * LD + __ldg(perm + b)] = cadd(x0[t], cconj(v)); }
+    __device__ void operator()(int t, int b, double2 v) const { out(t, __ldg(perm + b), cadd(x0[t], cconj(v))); }
   };
+  // 126 = 7 * 9 * 2 in three passes: source -> t1 -> t2 -> out (the radix-9
+  // butterfly direct, which needs no twiddles between two radix-3 passes)
   template <class In, class Out>
-  static __device__ __forceinline__ void fft126(const In& in, double2* a, double2* b, const Out& out,
+  static __device__ __forceinline__ void fft126(const In& in, double2* t1, double2* t2, const Out& out,
                                                 const double2* roots) {
-    pass_io<126, 7, 1, T, NT>(in, Plain{b}, roots);
+    pass_io<126, 7, 1, T, NT>(in, Plain{t1}, roots);
     __syncthreads();
-    pass_io<126, 3, 7, T, NT>(Plain{b}, Plain{a}, roots);
+    pass_io<126, 9, 7, T, NT>(Plain{t1}, Plain{t2}, roots);
     __syncthreads();
-    pass_io<126, 3, 21, T, NT>(Plain{a}, Plain{b}, roots);
-    __syncthreads();
-    pass_io<126, 2, 63, T, NT>(Plain{b}, out, roots);
+    pass_io<126, 2, 63, T, NT>(Plain{t2}, out, roots);
   }
-  static __device__ __forceinline__ double2* run(double2* a, double2* b, const FftPlan& P) {
+  // Element k of input sequence t is in(t, k); output k goes to out(t, k, X).
+  // in -> b -> a -> conj(U V) in b -> a -> b -> out: in may read a (x[0] is
+  // read before the second pass overwrites a, behind the first pass's
+  // barrier) and out may write a.  No barrier after the last stores.
+  template <class In, class Out>
+  static __device__ __forceinline__ void run_io(const In& in, const Out& out, double2* a, double2* b,
+                                                const FftPlan& P) {
     __shared__ double2 x0[T], X0[T];
-    for (int t = threadIdx.x; t < T; t += NT) x0[t] = a[t * LD];
-    // each FFT: source -> b -> a -> b -> a; x[0] is read from a before the
-    // second pass overwrites it (barrier after the first pass)
-    fft126(Gather{a, P.rperm}, a, b, Kernel{a, P.rkern, x0, X0}, P.rroots);
+    for (int t = threadIdx.x; t < T; t += NT) x0[t] = in(t, 0);
+    fft126(Gather<In>{in, P.rperm}, b, a, Kernel{b, P.rkern, x0, X0}, P.rroots);
     __syncthreads();
-    fft126(Plain{a}, a, b, Scatter{a, P.rperm + 126, x0}, P.rroots);
-    for (int t = threadIdx.x; t < T; t += NT) a[t * LD] = X0[t];
+    fft126(Plain{b}, a, b, Scatter<Out>{out, P.rperm + 126, x0}, P.rroots);
+    for (int t = threadIdx.x; t < T; t += NT) out(t, 0, X0[t]);
+  }
+  static constexpr bool io = true;
+  static __device__ __forceinline__ double2* run(double2* a, double2* b, const FftPlan& P) {
+    const Plain pa{a};
+    run_io(pa, pa, a, b, P);
     __syncthreads();
     return a;
   }

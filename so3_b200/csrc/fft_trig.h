@@ -1,5 +1,5 @@
 // Generated by gen_fft_trig.py: cos / sin (2 pi k / R), k = 0 .. (R-1)/2, for the odd
-// prime radices of the DFT engine, at kTrigCos[TrigOff<R>::v + k].  Do not edit by hand.
+// radices of the DFT engine, at kTrigCos[TrigOff<R>::v + k].  Do not edit by hand.
 // Indexed with compile-time offsets, the values are constant-bank operands.
 #pragma once
 
@@ -47,8 +47,12 @@ template <>
 struct TrigOff<31> {
   static constexpr int v = 68;
 };
+template <>
+struct TrigOff<9> {
+  static constexpr int v = 84;
+};
 
-static __constant__ double kTrigCos[84] = {
+static __constant__ double kTrigCos[89] = {
     0x1.0000000000000p+0, -0x1.0000000000000p-1, 0x1.0000000000000p+0, 0x1.3c6ef372fe950p-2,
     -0x1.9e3779b97f4a8p-1, 0x1.0000000000000p+0, 0x1.3f3a0e28bedd1p-1, -0x1.c7b90e3024582p-3,
     -0x1.cd4bca9cb5c71p-1, 0x1.0000000000000p+0, 0x1.aeb8c8764f0bap-1, 0x1.a9628d9c712b6p-2,
@@ -70,8 +74,10 @@ static __constant__ double kTrigCos[84] = {
     0x1.60c045a2e9729p-1, 0x1.0ed45eea3b09fp-1, 0x1.63a3fcfaca412p-2, 0x1.361fc440b478fp-3,
     -0x1.9eeb01776b57dp-5, -0x1.00ab0eb2d7d94p-2, -0x1.c2f6af3928a8ep-2, -0x1.3965f49174d13p-1,
     -0x1.847bf1d5146ccp-1, -0x1.bfaa5c136b224p-1, -0x1.e884f0cc22cccp-1, -0x1.fd5f830f860f9p-1,
+    0x1.0000000000000p+0, 0x1.8836fa2cf5039p-1, 0x1.63a1a7e0b738ap-3, -0x1.0000000000000p-1,
+    -0x1.e11f642522d1cp-1,
 };
-static __constant__ double kTrigSin[84] = {
+static __constant__ double kTrigSin[89] = {
     0x0.0p+0, 0x1.bb67ae8584caap-1, 0x0.0p+0, 0x1.e6f0e134454ffp-1,
     0x1.2cf2304755a5ep-1, 0x0.0p+0, 0x1.904c37505de4bp-1, 0x1.f329c0558e969p-1,
     0x1.bc4c04d71abc1p-2, 0x0.0p+0, 0x1.14cedf8bb580bp-1, 0x1.d1bb48eee2c13p-1,
@@ -93,6 +99,8 @@ static __constant__ double kTrigSin[84] = {
     0x1.73180a4b0d300p-1, 0x1.b2818007c19dfp-1, 0x1.e0210c26a6e6fp-1, 0x1.fa18852c3e08ap-1,
     0x1.ff57c5208ccf9p-1, 0x1.efa7cddb128fap-1, 0x1.cbad095f50378p-1, 0x1.94e08eb13c451p-1,
     0x1.4d80b1ad9ccf6p-1, 0x1.f0f2ff6705becp-2, 0x1.328c3f1b322cbp-2, 0x1.9e62aca53c49fp-4,
+    0x0.0p+0, 0x1.491b7523c161dp-1, 0x1.f838b8c811c17p-1, 0x1.bb67ae8584caap-1,
+    0x1.5e3a8748a0bf5p-2,
 };
 
 }  // namespace so3g

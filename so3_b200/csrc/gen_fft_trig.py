@@ -1,5 +1,7 @@
 """Writes fft_trig.h: cos(2 pi k / R) and sin(2 pi k / R), k = 0 .. (R-1)/2, for
-the odd prime radices of the DFT engine, as correctly rounded FP64 literals.
+the odd radices of the DFT engine (the primes, and 9 for the direct radix-9
+butterfly of the 126-point Rader convolution), as correctly rounded FP64
+literals.
 
 The values come from 60-digit Taylor series in Python's decimal module (no
 floating-point library is involved); float(Decimal) rounds to nearest.  Run
@@ -7,7 +9,7 @@ it from this directory after changing RADICES:  python gen_fft_trig.py
 """
 from decimal import Decimal, getcontext
 
-RADICES = (3, 5, 7, 11, 13, 17, 19, 23, 29, 31)
+RADICES = (3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 9)
 
 getcontext().prec = 60
 
@@ -51,7 +53,7 @@ def main():
     P = pi()
     lines = [
         "// Generated by gen_fft_trig.py: cos / sin (2 pi k / R), k = 0 .. (R-1)/2, for the odd",
-        "// prime radices of the DFT engine, at kTrigCos[TrigOff<R>::v + k].  Do not edit by hand.",
+        "// radices of the DFT engine, at kTrigCos[TrigOff<R>::v + k].  Do not edit by hand.",
         "// Indexed with compile-time offsets, the values are constant-bank operands.",
         "#pragma once",
         "",

@@ -68,6 +68,9 @@ template <bool BIG>
 struct Gen {
   static constexpr bool fixed = false;
   static constexpr int NT = kThreads, MINB = BIG ? 1 : 2, T = 0, LD = 0, nP = 0;
+  static constexpr bool io = false;
+  template <class In, class Out>
+  static __device__ __forceinline__ void runIO(const In&, const Out&, double2*, double2*, const FftPlan&) {}
   static __device__ __forceinline__ int at(int k) { return k; }
   static __device__ __forceinline__ int atC(int k) { return k; }
   static __device__ __forceinline__ double2* runP(double2* a, double2* b, int T_, int ld, const FftPlan& P) {
@@ -84,6 +87,13 @@ struct Fix {
   static constexpr int NT = NT_, MINB = MINB_, T = T_;
   static constexpr int ldP = PP<1, 1, 1>::ld, ldC = PC<1, 1, 1>::ld;
   static constexpr int nP = PP<1, 1, 1>::n;  // runP length
+  // the runP plan reads its input and writes its output through callables
+  static constexpr bool io = PP<1, 1, 1>::io;
+  template <class In, class Out>
+  static __device__ __forceinline__ void runIO(const In& in, const Out& out, double2* a, double2* b,
+                                               const FftPlan& P) {
+    PP<T_, LD, NT_>::run_io(in, out, a, b, P);
+  }
   static constexpr int ldmax = ldP > ldC ? ldP : ldC;
   // pitch = 8/T (mod 8) 16-byte slots: the T sequences of one index, which
   // consecutive threads handle, fall into distinct banks
@@ -226,6 +236,24 @@ __global__ void __launch_bounds__(E::NT, E::MINB) inv_gamma_kernel(Geometry g, F
   double2* a = sm;
   double2* b = sm + (size_t)T * ld;
   const int row = row0 + blockIdx.y, a0 = blockIdx.x * T, ng = g.ng;
+  if constexpr (!REAL && E::io) {
+    // the plan reads plane (k + plane0) mod ng and writes gamma sample k
+    // straight from / to global memory (complex: nplanes == ng)
+    const long long plane_sz = (long long)g.nb * g.na;
+    double2* f = static_cast<double2*>(fout);
+    auto in = [&](int t, int k) {
+      const int al = a0 + t;
+      int p = k + g.plane0;
+      if (p >= ng) p -= ng;
+      return al < g.na ? cconj(W[(long long)p * g.PS + (long long)row * g.RS + al]) : make_double2(0.0, 0.0);
+    };
+    auto out = [&](int t, int k, double2 y) {
+      const int al = a0 + t;
+      if (al < g.na) f[(long long)k * plane_sz + (long long)row * g.na + al] = cconj(y);
+    };
+    E::runIO(in, out, a, b, P);
+    return;
+  }
   for (int idx = threadIdx.x; idx < g.nplanes * T; idx += E::NT) {
     const int t = idx % T, p = idx / T, al = a0 + t;
     double2 v = al < g.na ? W[(long long)p * g.PS + (long long)row * g.RS + al] : make_double2(0.0, 0.0);
@@ -257,55 +285,66 @@ __global__ void __launch_bounds__(E::NT, E::MINB) inv_gamma_kernel(Geometry g, F
   }
 }
 
-// Persistent variants of the 1023-point stages (one sequence per CTA): a CTA
-// walks the sequences blockIdx.x, + gridDim.x, ... and issues the next
-// sequence's global loads into registers before the current sequence's
-// passes, so the load latency hides behind the DFT.  Same element
+// Persistent variants of the 1023-point stages: a CTA walks its tiles
+// (T sequences) blockIdx.x, + gridDim.x, ... and issues the next tile's
+// global loads into registers before the current tile's passes, so the load
+// latency hides behind the DFT.  Same element
 // arithmetic as inv_beta_kernel / inv_alpha_kernel / fwd_alpha_kernel.
 template <class E>
 __global__ void __launch_bounds__(E::NT, E::MINB) inv_beta_pf_kernel(Geometry g, FftPlan P, double2* __restrict__ W) {
-  static_assert(E::fixed && E::T == 1, "one sequence per CTA");
+  static_assert(E::fixed, "compile-time plan");
   extern __shared__ double2 sm[];
-  constexpr int NT = E::NT, Pn = E::nP, NPT = ((Pn + 1) / 2 + NT - 1) / NT;  // L = (Pn + 1) / 2 (MW)
+  constexpr int NT = E::NT, T = E::T, Pn = E::nP, LD = E::LD;
+  constexpr int NPT = ((Pn + 1) / 2 + NT - 1) / NT;  // per column; L = (Pn + 1) / 2 (MW)
   double2* a = sm;
-  double2* b = sm + E::LD;
-  const int L = g.L, ncols = 2 * L - 1, ntiles = ncols * g.nplanes;
-  double2 pre[NPT];
+  double2* b = sm + T * LD;
+  const int L = g.L, ncols = 2 * L - 1, ctiles = (ncols + T - 1) / T, ntiles = ctiles * g.nplanes;
+  double2 pre[T][NPT];
   auto fetch = [&](int tile) {
-    const int plane = tile / ncols, c = tile - plane * ncols;
-    const double2* cbase = W + g.QOFF + (long long)plane * g.QS + (long long)c * g.CS;
+    const int plane = tile / ctiles, c0 = (tile - plane * ctiles) * T;
+    const double2* cbase = W + g.QOFF + (long long)plane * g.QS;
 #pragma unroll
-    for (int i = 0; i < NPT; i++) {
-      const int mp = threadIdx.x + i * NT;
-      pre[i] = mp < L ? cbase[mp] : make_double2(0.0, 0.0);
+    for (int t = 0; t < T; t++) {
+      const int c = c0 + t;
+#pragma unroll
+      for (int i = 0; i < NPT; i++) {
+        const int mp = threadIdx.x + i * NT;
+        pre[t][i] = (c < ncols && mp < L) ? cbase[(long long)c * g.CS + mp] : make_double2(0.0, 0.0);
+      }
     }
   };
   int tile = blockIdx.x;
   if (tile < ntiles) fetch(tile);
   for (; tile < ntiles; tile += gridDim.x) {
-    const int plane = tile / ncols, c = tile - plane * ncols, n = plane - g.plane0;
-    const int m = c - (L - 1);
-    const double sg = ((m + n) & 1) ? -1.0 : 1.0;
-    if (!g.mw && threadIdx.x == 0) a[E::at(L)] = make_double2(0.0, 0.0);
+    const int plane = tile / ctiles, c0 = (tile - plane * ctiles) * T, n = plane - g.plane0;
 #pragma unroll
-    for (int i = 0; i < NPT; i++) {
-      const int mp = threadIdx.x + i * NT;
-      if (mp >= L) break;
-      const double2 v = pre[i];
-      double2 xp = v, xn = make_double2(sg * v.x, sg * v.y);
-      if (g.mw) {
-        const double2 e = cconj(__ldg(P.half + mp));  // e^{i pi m'/(2L-1)}
-        xp = cmul(xp, e);
-        xn = cmul(xn, cconj(e));
+    for (int t = 0; t < T; t++) {
+      const int m = c0 + t - (L - 1);
+      const double sg = ((m + n) & 1) ? -1.0 : 1.0;
+      if (!g.mw && threadIdx.x == 0) a[t * LD + E::at(L)] = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int i = 0; i < NPT; i++) {
+        const int mp = threadIdx.x + i * NT;
+        if (mp >= L) break;
+        const double2 v = pre[t][i];
+        double2 xp = v, xn = make_double2(sg * v.x, sg * v.y);
+        if (g.mw) {
+          const double2 e = cconj(__ldg(P.half + mp));  // e^{i pi m'/(2L-1)}
+          xp = cmul(xp, e);
+          xn = cmul(xn, cconj(e));
+        }
+        a[t * LD + E::at(mp)] = cconj(xp);
+        if (mp > 0) a[t * LD + E::at(Pn - mp)] = cconj(xn);
       }
-      a[E::at(mp)] = cconj(xp);
-      if (mp > 0) a[E::at(Pn - mp)] = cconj(xn);
     }
     __syncthreads();
     if (tile + gridDim.x < ntiles) fetch(tile + gridDim.x);
-    double2* r = E::runP(a, b, 1, E::LD, P);
-    double2* base = W + (long long)plane * g.PS + c;
-    for (int row = threadIdx.x; row < g.nb; row += NT) base[(long long)row * g.RS] = cconj(r[E::at(row)]);
+    double2* r = E::runP(a, b, T, LD, P);
+    double2* base = W + (long long)plane * g.PS;
+    for (int idx = threadIdx.x; idx < g.nb * T; idx += NT) {  // T consecutive columns of a row per store run
+      const int t = idx % T, row = idx / T, c = c0 + t;
+      if (c < ncols) base[(long long)row * g.RS + c] = cconj(r[t * LD + E::at(row)]);
+    }
   }
 }
 
@@ -353,6 +392,24 @@ __global__ void __launch_bounds__(E::NT, E::MINB) fwd_gamma_kernel(Geometry g, F
   double2* b = sm + (size_t)T * ld;
   const int row = row0 + blockIdx.y, a0 = blockIdx.x * T, ng = g.ng;
   const long long plane_sz = (long long)g.nb * g.na;
+  const double scale = 2.0 * 3.141592653589793238462643383279502884 / ng;
+  if constexpr (!REAL && E::io) {
+    // the plan reads gamma sample k and writes plane (k + plane0) mod ng
+    // straight from / to global memory (complex: nplanes == ng)
+    const double2* f = static_cast<const double2*>(fin);
+    auto in = [&](int t, int k) {
+      const int al = a0 + t;
+      return al < g.na ? f[(long long)k * plane_sz + (long long)row * g.na + al] : make_double2(0.0, 0.0);
+    };
+    auto out = [&](int t, int k, double2 y) {
+      const int al = a0 + t;
+      int p = k + g.plane0;
+      if (p >= ng) p -= ng;
+      if (al < g.na) W[(long long)p * g.PS + (long long)row * g.RS + al] = cscale(y, scale);
+    };
+    E::runIO(in, out, a, b, P);
+    return;
+  }
   for (int idx = threadIdx.x; idx < ng * T; idx += E::NT) {
     const int t = idx % T, gi = idx / T, al = a0 + t;
     double2 v = make_double2(0.0, 0.0);
@@ -367,7 +424,6 @@ __global__ void __launch_bounds__(E::NT, E::MINB) fwd_gamma_kernel(Geometry g, F
   }
   __syncthreads();
   double2* r = E::runP(a, b, T, ld, P);
-  const double scale = 2.0 * 3.141592653589793238462643383279502884 / ng;
   for (int idx = threadIdx.x; idx < g.nplanes * T; idx += E::NT) {
     const int t = idx % T, p = idx / T, al = a0 + t;
     if (al >= g.na) continue;
@@ -558,10 +614,11 @@ int persistent_grid(K kernel, int nt, size_t smem, int ntiles, int* grid) {
 template <class E>
 int inv_beta_pf(const Geometry& g, const FftPlan& p, double2* W, cudaStream_t s) {
   if (g.P != 2 * g.L - 1) return fail(kUnsupported, "persistent beta stage needs MW sampling");
-  const size_t smem = 2 * (size_t)E::LD * sizeof(double2);
+  const size_t smem = 2 * (size_t)E::T * E::LD * sizeof(double2);
   if (int rc = set_smem(inv_beta_pf_kernel<E>, smem)) return rc;
   int grid = 0;
-  if (int rc = persistent_grid(inv_beta_pf_kernel<E>, E::NT, smem, (2 * g.L - 1) * g.nplanes, &grid)) return rc;
+  const int ntiles = (2 * g.L - 1 + E::T - 1) / E::T * g.nplanes;
+  if (int rc = persistent_grid(inv_beta_pf_kernel<E>, E::NT, smem, ntiles, &grid)) return rc;
   inv_beta_pf_kernel<E><<<grid, E::NT, smem, s>>>(g, p, W);
   return kOk;
 }
@@ -647,7 +704,7 @@ int launch_inv_beta(const Geometry& g, const FftPlan& p, double2* W, cudaStream_
     case Eng::k1023:
       rc = v == 1   ? inv_beta<E1023b>(g, p, W, s)
            : v == 2 ? inv_beta<E1023c>(g, p, W, s)
-           : v == 3 ? inv_beta_pf<E1023a>(g, p, W, s)
+           : v == 3 ? inv_beta_pf<E1023c>(g, p, W, s)
                     : inv_beta<E1023a>(g, p, W, s);
       break;
     case Eng::k127:

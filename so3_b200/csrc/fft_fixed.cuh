@@ -216,6 +216,23 @@ struct P1023G {
     __syncthreads();
     return b;
   }
+  // Same passes; the last one hands output k of sequence t to out(t, k, X)
+  // (straight to global memory) instead of a shared buffer.  Barrier at the
+  // end: the last pass reads a.
+  struct Seq {
+    const double2* p;
+    __device__ double2 operator()(int t, int i) const { return p[t * LD + i]; }
+  };
+  static constexpr bool has_out = true;
+  template <class Out>
+  static __device__ __forceinline__ void run_out(double2* a, double2* b, const FftPlan& P, const Out& out) {
+    pass<1023, 31, 1, T, LD, NT, NG, sk>(a, b, P.roots);
+    __syncthreads();
+    pass<1023, 11, 31, T, LD, NT, 1, sk>(b, a, P.roots);
+    __syncthreads();
+    pass_io<1023, 3, 341, T, NT>(Seq{a}, out, P.roots);
+    __syncthreads();
+  }
 };
 template <int T, int LD, int NT>
 using P1023 = P1023G<3, T, LD, NT>;

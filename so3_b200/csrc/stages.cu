@@ -68,9 +68,11 @@ template <bool BIG>
 struct Gen {
   static constexpr bool fixed = false;
   static constexpr int NT = kThreads, MINB = BIG ? 1 : 2, T = 0, LD = 0, nP = 0;
-  static constexpr bool io = false;
+  static constexpr bool io = false, has_out = false;
   template <class In, class Out>
   static __device__ __forceinline__ void runIO(const In&, const Out&, double2*, double2*, const FftPlan&) {}
+  template <class Out>
+  static __device__ __forceinline__ void runPOut(double2*, double2*, const FftPlan&, const Out&) {}
   static __device__ __forceinline__ int at(int k) { return k; }
   static __device__ __forceinline__ int atC(int k) { return k; }
   static __device__ __forceinline__ double2* runP(double2* a, double2* b, int T_, int ld, const FftPlan& P) {
@@ -93,6 +95,12 @@ struct Fix {
   static __device__ __forceinline__ void runIO(const In& in, const Out& out, double2* a, double2* b,
                                                const FftPlan& P) {
     PP<T_, LD, NT_>::run_io(in, out, a, b, P);
+  }
+  // the runP plan's last pass can store through a callable (1023 = 31*11*3)
+  static constexpr bool has_out = nP == 1023;
+  template <class Out>
+  static __device__ __forceinline__ void runPOut(double2* a, double2* b, const FftPlan& P, const Out& out) {
+    if constexpr (has_out) PP<T_, LD, NT_>::run_out(a, b, P, out);
   }
   static constexpr int ldmax = ldP > ldC ? ldP : ldC;
   // pitch = 8/T (mod 8) 16-byte slots: the T sequences of one index, which
@@ -176,6 +184,12 @@ __global__ void __launch_bounds__(E::NT, E::MINB) inv_beta_kernel(Geometry g, Ff
     for (int idx = threadIdx.x; idx < L * T; idx += E::NT) load(idx / L, idx % L);
   }
   __syncthreads();
+  if constexpr (E::has_out) {  // rows >= nb of the extended circle are never stored
+    E::runPOut(a, b, P, [&](int t, int row, double2 v) {
+      if (row < g.nb && c0 + t < ncols) base[(long long)row * g.RS + c0 + t] = cconj(v);
+    });
+    return;
+  }
   double2* r = E::runP(a, b, T, ld, P);
   for (int idx = threadIdx.x; idx < g.nb * T; idx += E::NT) {
     const int t = idx % T, row = idx / T, c = c0 + t;
@@ -339,12 +353,10 @@ __global__ void __launch_bounds__(E::NT, E::MINB) inv_beta_pf_kernel(Geometry g,
     }
     __syncthreads();
     if (tile + gridDim.x < ntiles) fetch(tile + gridDim.x);
-    double2* r = E::runP(a, b, T, LD, P);
     double2* base = W + (long long)plane * g.PS;
-    for (int idx = threadIdx.x; idx < g.nb * T; idx += NT) {  // T consecutive columns of a row per store run
-      const int t = idx % T, row = idx / T, c = c0 + t;
-      if (c < ncols) base[(long long)row * g.RS + c] = cconj(r[t * LD + E::at(row)]);
-    }
+    E::runPOut(a, b, P, [&](int t, int row, double2 v) {  // rows >= nb are never stored
+      if (row < g.nb && c0 + t < ncols) base[(long long)row * g.RS + c0 + t] = cconj(v);
+    });
   }
 }
 
@@ -376,9 +388,10 @@ __global__ void __launch_bounds__(E::NT, E::MINB) inv_alpha_pf_kernel(Geometry g
     }
     __syncthreads();
     if (row + gridDim.x < nrows) fetch(row + gridDim.x);
-    double2* r = E::runP(a, b, 1, E::LD, P);
     double2* dst = W + row_off(g, row);
-    for (int k = threadIdx.x; k < g.na; k += NT) dst[k] = cconj(r[E::at(k)]);
+    E::runPOut(a, b, P, [&](int, int k, double2 v) {
+      if (k < g.na) dst[k] = cconj(v);
+    });
   }
 }
 
@@ -501,9 +514,11 @@ __global__ void __launch_bounds__(E::NT, E::MINB) fwd_alpha_pf_kernel(Geometry g
     }
     __syncthreads();
     if (row + gridDim.x < nrows) fetch(row + gridDim.x);
-    double2* r = E::runP(a, b, 1, E::LD, P);
     double2* dst = W + row_off(g, row);
-    for (int c = threadIdx.x; c < ncols; c += NT) dst[c] = cscale(r[E::at(wrap1(c - (L - 1), Pn))], inv);
+    E::runPOut(a, b, P, [&](int, int k, double2 v) {  // frequency k -> column m + L - 1
+      const int c = k <= L - 1 ? k + L - 1 : k - Pn + L - 1;
+      if (c >= 0 && c < ncols) dst[c] = cscale(v, inv);
+    });
   }
 }
 

@@ -27,12 +27,6 @@ namespace {
 constexpr int kThreads = 256;
 constexpr size_t kSmemCap = 200 * 1024;
 
-int pick_T(int ld, int buffers_per_seq, int Tmax) {
-  int T = Tmax;
-  while (T > 1 && (size_t)buffers_per_seq * T * ld * sizeof(double2) > kSmemCap) T >>= 1;
-  return T;
-}
-
 // Sequences per CTA and dynamic shared memory for a plan of engine length ld:
 // large-radix instances may use up to kSmemCap (one CTA per SM), the others
 // stay within half of an SM's shared memory (two CTAs per SM).

@@ -49,7 +49,8 @@ def cos_sin(a):
     return c, s
 
 
-def main():
+def render():
+    """The text of fft_trig.h."""
     P = pi()
     lines = [
         "// Generated by gen_fft_trig.py: cos / sin (2 pi k / R), k = 0 .. (R-1)/2, for the odd",
@@ -81,7 +82,11 @@ def main():
 
     lines += [""] + table("kTrigCos", cs) + table("kTrigSin", sn)
     lines += ["", "}  // namespace so3g", ""]
-    open("fft_trig.h", "w").write("\n".join(lines))
+    return "\n".join(lines)
+
+
+def main():
+    open("fft_trig.h", "w").write(render())
 
 
 if __name__ == "__main__":

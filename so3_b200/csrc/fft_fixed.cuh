@@ -236,6 +236,8 @@ struct P1023G {
 };
 template <int T, int LD, int NT>
 using P1023 = P1023G<3, T, LD, NT>;
+template <int T, int LD, int NT>
+using P1023n2 = P1023G<2, T, LD, NT>;
 
 // 2048 = 8 * 8 * 8 * 4 (the quadrature-weight convolution length at L = 512).
 template <int T, int LD, int NT>

@@ -120,6 +120,7 @@ using E1023a = Fix<fx::P1023, fx::P1023, 1, 128, 4>;
 using E1023b = Fix<fx::P1023, fx::P1023, 1, 64, 8>;
 using E1023c = Fix<fx::P1023, fx::P1023, 2, 128, 3>;
 using E1023p = Fix<fx::P1023, fx::P1023, 1, 128, 3>;  // persistent inverse alpha (prefetch registers)
+using E1023c2 = Fix<fx::P1023n2, fx::P1023n2, 2, 128, 3>;  // radix-31 butterflies in two output groups
 using E127a = Fix<fx::P127, fx::P127, 4, 128, 4>;
 using E127b = Fix<fx::P127, fx::P127, 8, 128, 3>;
 using E127c = Fix<fx::P127, fx::P127, 2, 64, 8>;
@@ -293,67 +294,11 @@ __global__ void __launch_bounds__(E::NT, E::MINB) inv_gamma_kernel(Geometry g, F
   }
 }
 
-// Persistent variants of the 1023-point stages: a CTA walks its tiles
-// (T sequences) blockIdx.x, + gridDim.x, ... and issues the next tile's
-// global loads into registers before the current tile's passes, so the load
-// latency hides behind the DFT.  Same element
-// arithmetic as inv_beta_kernel / inv_alpha_kernel / fwd_alpha_kernel.
-template <class E>
-__global__ void __launch_bounds__(E::NT, E::MINB) inv_beta_pf_kernel(Geometry g, FftPlan P, double2* __restrict__ W) {
-  static_assert(E::fixed, "compile-time plan");
-  extern __shared__ double2 sm[];
-  constexpr int NT = E::NT, T = E::T, Pn = E::nP, LD = E::LD;
-  constexpr int NPT = ((Pn + 1) / 2 + NT - 1) / NT;  // per column; L = (Pn + 1) / 2 (MW)
-  double2* a = sm;
-  double2* b = sm + T * LD;
-  const int L = g.L, ncols = 2 * L - 1, ctiles = (ncols + T - 1) / T, ntiles = ctiles * g.nplanes;
-  double2 pre[T][NPT];
-  auto fetch = [&](int tile) {
-    const int plane = tile / ctiles, c0 = (tile - plane * ctiles) * T;
-    const double2* cbase = W + g.QOFF + (long long)plane * g.QS;
-#pragma unroll
-    for (int t = 0; t < T; t++) {
-      const int c = c0 + t;
-#pragma unroll
-      for (int i = 0; i < NPT; i++) {
-        const int mp = threadIdx.x + i * NT;
-        pre[t][i] = (c < ncols && mp < L) ? cbase[(long long)c * g.CS + mp] : make_double2(0.0, 0.0);
-      }
-    }
-  };
-  int tile = blockIdx.x;
-  if (tile < ntiles) fetch(tile);
-  for (; tile < ntiles; tile += gridDim.x) {
-    const int plane = tile / ctiles, c0 = (tile - plane * ctiles) * T, n = plane - g.plane0;
-#pragma unroll
-    for (int t = 0; t < T; t++) {
-      const int m = c0 + t - (L - 1);
-      const double sg = ((m + n) & 1) ? -1.0 : 1.0;
-      if (!g.mw && threadIdx.x == 0) a[t * LD + E::at(L)] = make_double2(0.0, 0.0);
-#pragma unroll
-      for (int i = 0; i < NPT; i++) {
-        const int mp = threadIdx.x + i * NT;
-        if (mp >= L) break;
-        const double2 v = pre[t][i];
-        double2 xp = v, xn = make_double2(sg * v.x, sg * v.y);
-        if (g.mw) {
-          const double2 e = cconj(__ldg(P.half + mp));  // e^{i pi m'/(2L-1)}
-          xp = cmul(xp, e);
-          xn = cmul(xn, cconj(e));
-        }
-        a[t * LD + E::at(mp)] = cconj(xp);
-        if (mp > 0) a[t * LD + E::at(Pn - mp)] = cconj(xn);
-      }
-    }
-    __syncthreads();
-    if (tile + gridDim.x < ntiles) fetch(tile + gridDim.x);
-    double2* base = W + (long long)plane * g.PS;
-    E::runPOut(a, b, P, [&](int t, int row, double2 v) {  // rows >= nb are never stored
-      if (row < g.nb && c0 + t < ncols) base[(long long)row * g.RS + c0 + t] = cconj(v);
-    });
-  }
-}
-
+// Persistent variants of the alpha stages: a CTA walks its sequences
+// blockIdx.x, + gridDim.x, ... and issues the next sequence's global loads
+// into registers before the current sequence's passes, so the load latency
+// hides behind the DFT.  Same element arithmetic as inv_alpha_kernel /
+// fwd_alpha_kernel.
 template <class E>
 __global__ void __launch_bounds__(E::NT, E::MINB) inv_alpha_pf_kernel(Geometry g, FftPlan P, double2* __restrict__ W) {
   static_assert(E::fixed && E::T == 1, "one sequence per CTA");
@@ -621,18 +566,6 @@ int persistent_grid(K kernel, int nt, size_t smem, int ntiles, int* grid) {
 }
 
 template <class E>
-int inv_beta_pf(const Geometry& g, const FftPlan& p, double2* W, cudaStream_t s) {
-  if (g.P != 2 * g.L - 1) return fail(kUnsupported, "persistent beta stage needs MW sampling");
-  const size_t smem = 2 * (size_t)E::T * E::LD * sizeof(double2);
-  if (int rc = set_smem(inv_beta_pf_kernel<E>, smem)) return rc;
-  int grid = 0;
-  const int ntiles = (2 * g.L - 1 + E::T - 1) / E::T * g.nplanes;
-  if (int rc = persistent_grid(inv_beta_pf_kernel<E>, E::NT, smem, ntiles, &grid)) return rc;
-  inv_beta_pf_kernel<E><<<grid, E::NT, smem, s>>>(g, p, W);
-  return kOk;
-}
-
-template <class E>
 int inv_alpha_pf(const Geometry& g, const FftPlan& p, double2* W, cudaStream_t s) {
   const size_t smem = 2 * (size_t)E::LD * sizeof(double2);
   if (int rc = set_smem(inv_alpha_pf_kernel<E>, smem)) return rc;
@@ -713,7 +646,7 @@ int launch_inv_beta(const Geometry& g, const FftPlan& p, double2* W, cudaStream_
     case Eng::k1023:
       rc = v == 1   ? inv_beta<E1023b>(g, p, W, s)
            : v == 2 ? inv_beta<E1023c>(g, p, W, s)
-           : v == 3 ? inv_beta_pf<E1023c>(g, p, W, s)
+           : v == 3 ? inv_beta<E1023c2>(g, p, W, s)
                     : inv_beta<E1023a>(g, p, W, s);
       break;
     case Eng::k127:

@@ -98,15 +98,22 @@ int so3gpu_set_stage_variants(int device, const so3_parameters_t *p, const int *
 
 /* Complex inverse transform (same result as so3gpu_inverse) that allocates
  * no device memory; no counterpart in the reference.  For callers that cannot
- * call cudaMalloc (code running under a foreign allocator or memory cap, or
- * loops that must not allocate after start-up).  f and flmn are device
+ * call cudaMalloc: code running under an allocator or memory cap owned by
+ * someone else, or loops that must not allocate (and so must not risk an
+ * implicit device synchronisation) after start-up.  f and flmn are device
  * pointers; stream is a cudaStream_t (NULL: legacy default stream).  Its
- * scratch, Wigner tables and FFT tables are file-scope device arrays (about
- * 34 MB, held by every GPU that loads the library until exit); transforms
- * needing more than 32 MiB of scratch, L > 64 or N > 64 return status 3.
- * The first call on a device builds the tables and waits for them: make it
- * before any stream capture.  Calls share the arrays, so calls whose GPU work
- * overlaps race: serialise them. */
+ * scratch, Wigner tables and FFT tables are file-scope device arrays of
+ * 35,089,464 bytes in total (32 MiB of them scratch), held by every GPU that
+ * loads the library until exit.  Complex, non-steerable signals only:
+ * reality != 0 or steerable != 0 return status 3 before any device work.
+ * L > 64, N > 64 or more than 32 MiB of scratch return status 3 (MW and MWSS
+ * with L <= 64, N <= 64 always fit).  The first call in a CUDA context (the
+ * runtime's primary context; again after cudaDeviceReset) builds the tables
+ * and waits for them: make it before any stream capture.  A call whose L, N,
+ * sampling, storage or n-order differ from the previous call's uploads new
+ * FFT and offset tables from host memory: make such calls outside stream
+ * capture as well.  Calls share the arrays, so calls whose GPU work overlaps
+ * race: serialise them. */
 int so3gpu_inverse_noalloc(void *f, const void *flmn, const so3_parameters_t *parameters, void *stream);
 
 /* Request server (no counterpart in the reference): inverse (kind 0),

@@ -6,19 +6,26 @@
 // cudaMalloc, cudaFree or any allocating routine: the transform scratch, the
 // Wigner Delta(pi/2) tables, the FFT tables and the block-offset table live
 // in the file-scope device arrays below, which every GPU that loads the
-// library holds until the process exits.
+// library holds until the process exits: kStaticBytes = 35,089,464 bytes
+// (33.5 MiB), of which 32 MiB are scratch.
 //
-// Limits: transform scratch of at most kScratchBytes (32 MiB; for example
-// MW sampling with L <= 64 and N <= 64), L <= kMaxL, N <= kMaxN.  Larger
-// requests are rejected with status 3 and a message.
+// Limits: complex, non-steerable signals only (reality != 0 or steerable !=
+// 0: status 3, before any device work -- a real signal's buffers are sized
+// for the real layout, which this entry point does not handle); transform
+// scratch of at most kScratchBytes (32 MiB; MW or MWSS sampling with L <= 64
+// and N <= 64 always fits), L <= kMaxL, N <= kMaxN.  Larger requests are
+// rejected with status 3 and a message.
 //
-// Set-up: the first call on a device (that device current) resolves the
-// arrays' device addresses with cudaGetSymbolAddress and builds the Delta
-// tables on the call's stream, then waits for them; make that first call
-// before any stream capture.  A later call whose band limits, storage or
-// n-order differ from the previous call's uploads new FFT and offset tables
-// from host memory with cudaMemcpyAsync; make such calls outside capture too
-// (a captured region may repeat one configuration).
+// Set-up: the first call in a CUDA context (the device's primary context, as
+// the runtime API uses it) resolves the arrays' device addresses with
+// cudaGetSymbolAddress and builds the Delta tables on the call's stream, then
+// waits for them; make that first call before any stream capture.  The set-up
+// is keyed by the context's unique id, so a call from a new context (after
+// cudaDeviceReset, or a context made with the driver API) sets up again.  A
+// later call whose band limits, storage or n-order differ from the previous
+// call's uploads new FFT and offset tables from host memory with
+// cudaMemcpyAsync; make such calls outside capture too (a captured region may
+// only repeat the configuration of the call before it).
 //
 // Every call shares the arrays and leaves the last call's contents behind;
 // each call writes every scratch entry before it reads it, so nothing needs
@@ -30,6 +37,8 @@
 #include <cstring>
 #include <mutex>
 #include <vector>
+
+#include <cuda.h>
 
 #include "so3gpu.h"
 #include "so3gpu_internal.h"
@@ -50,9 +59,13 @@ static __device__ __align__(256) double g_dl[2][kDlEntries];
 static __device__ __align__(256) double g_risbo_work[kRisboWork];
 static __device__ __align__(256) double2 g_fft[2][kFftSlot];
 static __device__ __align__(256) long long g_bases[kMaxPlanes];
+constexpr size_t kStaticBytes = kScratchBytes + sizeof(double) * (2 * (size_t)kDlEntries + kRisboWork) +
+                                sizeof(double2) * 2 * kFftSlot + sizeof(long long) * kMaxPlanes;
+static_assert(kStaticBytes == 35089464, "the documented size of the static arrays");
 
 struct NoAllocDevice {
   bool ready = false;
+  unsigned long long ctx_id = 0;  // context the set-up ran in
   double2* scratch = nullptr;
   double* dl[2] = {nullptr, nullptr};
   double* risbo_work = nullptr;
@@ -163,8 +176,41 @@ void plan_tables(int n, FftPlan* P, double2* h, const double2* dev) {
   half_table(n, P, h, dev, 2 * m + n);
 }
 
+// Unique id of the calling thread's current CUDA context, through the driver
+// entry points the runtime exposes (the library does not link libcuda).
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+int current_context_id(unsigned long long* id) {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  if (!get_current || !get_id) {
+    void* f0 = nullptr;
+    void* f1 = nullptr;
+    cudaDriverEntryPointQueryResult q0, q1;
+    SO3G_CUDA(cudaGetDriverEntryPoint("cuCtxGetCurrent", &f0, cudaEnableDefault, &q0));
+    SO3G_CUDA(cudaGetDriverEntryPoint("cuCtxGetId", &f1, cudaEnableDefault, &q1));
+    if (q0 != cudaDriverEntryPointSuccess || q1 != cudaDriverEntryPointSuccess || !f0 || !f1)
+      return fail(kCudaError, "so3gpu_inverse_noalloc: driver entry points cuCtxGetCurrent / cuCtxGetId missing");
+    get_current = reinterpret_cast<CtxGetCurrentFn>(f0);
+    get_id = reinterpret_cast<CtxGetIdFn>(f1);
+  }
+  CUcontext c = nullptr;
+  if (get_current(&c) != CUDA_SUCCESS || !c || get_id(c, id) != CUDA_SUCCESS)
+    return fail(kCudaError, "so3gpu_inverse_noalloc: no current CUDA context");
+  return kOk;
+}
+
 int setup_device(NoAllocDevice& S, cudaStream_t s) {
-  if (S.ready) return kOk;
+  // resolving a symbol makes the runtime's context current if no call has yet
+  void* probe = nullptr;
+  SO3G_CUDA(cudaGetSymbolAddress(&probe, g_scratch));
+  unsigned long long id = 0;
+  if (int rc = current_context_id(&id)) return rc;
+  if (S.ready && S.ctx_id == id) return kOk;
+  // first call in this context: nothing cached from another context is valid
+  S.ready = false;
+  S.plan_n[0] = S.plan_n[1] = 0;
+  S.bases_key[0] = 0;
   SO3G_CUDA(cudaGetSymbolAddress((void**)&S.scratch, g_scratch));
   SO3G_CUDA(cudaGetSymbolAddress((void**)&S.dl[0], g_dl));
   S.dl[1] = S.dl[0] + kDlEntries;
@@ -174,12 +220,17 @@ int setup_device(NoAllocDevice& S, cudaStream_t s) {
   if (int rc = launch_build_dl_risbo(S.dl[SSHT_DL_RISBO], kMaxL, S.risbo_work, s)) return rc;
   if (int rc = launch_build_dl_trapani(S.dl[SSHT_DL_TRAPANI], 0, kMaxL, s)) return rc;
   SO3G_CUDA(cudaStreamSynchronize(s));
+  S.ctx_id = id;
   S.ready = true;
   return kOk;
 }
 
 int run(void* f, const void* flmn, const so3_parameters_t* p, cudaStream_t s) {
   if (!p || !f || !flmn) return fail(kInvalidParameter, "null argument");
+  // checked before anything else: the buffers of a real signal are sized for
+  // the real layout, which this entry point does not handle
+  if (p->reality != 0) return fail(kUnsupported, "so3gpu_inverse_noalloc: complex signals only (reality = 0)");
+  if (p->steerable != 0) return fail(kUnsupported, "so3gpu_inverse_noalloc: steerable signals are not supported");
   if (int rc = validate(*p, 0)) return rc;
   if (p->L > kMaxL || p->N > kMaxN)
     return fail(kUnsupported, "so3gpu_inverse_noalloc: L <= 64 and N <= 64 only");

@@ -115,6 +115,7 @@ def ref():
             getattr(R, name).argtypes = [_VP, _VP, _P]
             getattr(R, name).restype = None
         R.so3_conv_harmonic_convolution.argtypes = [_VP, _P, _VP, _P, _VP, _P]
+        R.so3_conv_convolution.argtypes = [_VP, _P, _VP, _P, _VP, _P]
         R.so3_conv_s2toso3_harmonic_convolution.argtypes = [_VP, _P, _VP, _VP]
         R.so3_conv_get_parameters_of_convolved_lmn.argtypes = [_P, _P]
         R.so3_conv_get_parameters_of_convolved_lmn.restype = Params

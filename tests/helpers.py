@@ -21,3 +21,22 @@ def rel_err(x, y):
     y = np.asarray(y)
     den = np.abs(y).max()
     return float(np.abs(x - y).max() / (den if den > 0 else 1.0))
+
+
+# Floor of the elementwise relative error, as a fraction of max |y|: entries
+# smaller than this are compared against the floor instead of themselves
+# (a relative error is ill-posed at samples that cross zero).
+ELEM_FLOOR = 1e-3
+
+
+def rel_err_elem(x, y, floor=ELEM_FLOOR):
+    """max_i |x_i - y_i| / max(|y_i|, floor * max_j |y_j|): the elementwise
+    relative error with a stated floor for near-zero entries."""
+    x = np.asarray(x)
+    y = np.asarray(y)
+    ay = np.abs(y)
+    if ay.size == 0:
+        return 0.0
+    den = np.maximum(ay, floor * ay.max())
+    den = np.where(den > 0, den, 1.0)
+    return float((np.abs(x - y) / den).max())

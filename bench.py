@@ -55,7 +55,11 @@ def args_():
     ap.add_argument("--profile-region", action="store_true",
                     help="bracket the split-precision leg's timed steps (the FP64 leg's with --batch 0) "
                          "with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
+    ap.add_argument("--c3", type=int, default=512,
+                    help="signals of the L=128, N=16 batched split-precision leg (0: skip it)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-full-unit", action="store_true",
+                    help="also time one full CPU unit per process (no extrapolation; minutes at L=512, N=64)")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
 
@@ -134,14 +138,15 @@ def _cpu_sample_worker(args):
     bench's L and N restricted to n_mode=MAXIMUM (2 of the 2N-1 n-planes per
     direction), plus the gamma-axis FFT passes alone, so the full unit can be
     rebuilt as t_gamma + (2N-1)/2 * (t_sample - t_gamma)."""
-    L, N, use_ref = args
+    L, N, use_ref = args[:3]
+    full = len(args) > 3 and args[3]
     import ctypes
 
     import numpy as np
     sys.path.insert(0, ROOT)
     from oracle import oracle as O
     from so3_b200 import synth
-    p = O.params(L, N, mode=O.MAXIMUM)
+    p = O.params(L, N, mode=O.ALL if full else O.MAXIMUM)
     fl = synth.gen_flmn(p, 77, "uniform")
     R = O.ref() if use_ref else None
     f = np.zeros(O.f_size(p), np.complex128)
@@ -156,6 +161,8 @@ def _cpu_sample_worker(args):
         f = O.inverse(fl, p)
         O.forward(f, p, out=out)
     t1 = time.perf_counter()
+    if full:
+        return t1 - t0, 0.0
     # the gamma passes (one backward, one forward over all samples)
     stride = L * (2 * L - 1)
     g = np.zeros((2 * N - 1) * stride, np.complex128)
@@ -179,6 +186,20 @@ def cpu_unit_seconds(L, N, procs):
     for ts, tg in res:
         units.append(tg + (2 * N - 1) / 2.0 * max(ts - tg, 0.0))
     return statistics.median(units), statistics.median([r[0] for r in res]), use_ref
+
+
+def cpu_full_unit_seconds(L, N, procs):
+    """Per-process wall seconds of one FULL unit (all 2N-1 planes, no
+    extrapolation), procs concurrent single-threaded processes: the check of
+    the sampled estimate (minutes per process at L=512, N=64)."""
+    import multiprocessing as mp
+    from oracle import oracle as O
+    O.build()
+    use_ref = O.ref() is not None
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_cpu_sample_worker, [(L, N, use_ref, True)] * procs)
+    return statistics.median([r[0] for r in res])
 
 
 def cpu_procs(L, N):
@@ -246,6 +267,42 @@ def stage_work(L, N):
         "fwd_beta_conv": ("fp64", planes * P * (fft_flops(P) + 2 * fft_flops(Pc)),
                           f"{planes * P} x (DFT {P} + 2 DFTs {Pc}) at 5 n log2 n"),
     }
+
+
+def stage_bytes(L, N):
+    """Compulsory HBM bytes of one launch of each FP64 stage (complex MW, one
+    signal): every stage reads its input part once and writes its output part
+    once.  Samples / row-major scratch: (2N-1) L (2L-1) complex; column-major
+    spectra: (2N-1) (2L-1) L complex; coefficients: (2N-1) L^2 complex."""
+    planes = 2 * N - 1
+    part = planes * L * (2 * L - 1) * 16
+    flmn = planes * L * L * 16
+    return {"inv_contract": flmn + part, "inv_beta": 2 * part, "inv_alpha": 2 * part, "inv_gamma": 2 * part,
+            "fwd_gamma": 2 * part, "fwd_alpha": 2 * part, "fwd_beta_conv": 2 * part, "fwd_contract": part + flmn,
+            "mixed_inv_contract": flmn + part, "mixed_fwd_contract": part + flmn, "mixed_fwd_beta": 2 * part}
+
+
+def hbm_peak():
+    """HBM denominator: the measured-peaks file when present, else the
+    recipe's fallback (6650 GB/s, an earlier STREAM-style copy on this pool)."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(path))
+        for k in ("hbm_gbs", "hbm_GBs", "hbm"):
+            if k in d and float(d[k]) > 0:
+                return float(d[k]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        pass
+    return 6650.0, "fallback 6650 GB/s (no MEASURED_PEAKS.json)"
+
+
+def elem_err(x, y, floor=1e-3):
+    """Elementwise relative error max_i |x_i - y_i| / max(|y_i|, floor max|y|)
+    of two device tensors (floor: a stated fraction of the largest magnitude,
+    below which a relative error is ill-posed)."""
+    ay = y.abs()
+    den = ay.clamp(min=floor * float(ay.max().item()))
+    return float(((x - y).abs() / den).max().item())
 
 
 def mixed_tc_macs(L, N, fwd):
@@ -334,8 +391,9 @@ def run_ours(a):
     stream = torch.cuda.current_stream()
     ctx = so3.Context(local, stream=stream)
     ctx.prepare(p)
-    fp64_peak = so3.measure_fp64_peak(local)
-    int8_peak = so3.measure_int8_mma_peak(local)
+    from so3_b200 import peaks
+    fp64_peak = peaks.fp64_tflops(local)
+    int8_peak = peaks.int8_mma_tops(local)
 
     # ---- plain FP64 path, one signal per step
     fl_host = synth.gen_flmn(p, sdist.signal_seed(1000, rank, 0), "uniform")
@@ -368,21 +426,28 @@ def run_ours(a):
         rmx = timed_steps(stepmx, a.steps, a.warmup, stream, ctx, so3, sdist, local, world, a.profile_region)
         mixed_value = sdist.job_throughput(world * a.steps * B, rmx["total_ms"] / 1e3)
         # error of the split path against the FP64 path on the same inputs
-        err_f = err_fl = err_rt = 0.0
+        err_f = err_fl = err_rt = ee_f = ee_fl = 0.0
         for i in range(B):
             ctx.inverse(fls[i], p, out=d_f)
             torch.cuda.synchronize()
             err_f = max(err_f, float(((fs[i] - d_f).abs().max() / d_f.abs().max()).item()))
+            ee_f = max(ee_f, elem_err(fs[i], d_f))
             ref = ctx.forward(fs[i], p)
             torch.cuda.synchronize()
             err_fl = max(err_fl, float(((backs[i] - ref).abs().max() / ref.abs().max()).item()))
+            ee_fl = max(ee_fl, elem_err(backs[i], ref))
             err_rt = max(err_rt, float(((backs[i] - fls[i]).abs().max() / fls[i].abs().max()).item()))
             del ref
         del fls, fs, backs  # release the batch before the end-to-end and serving legs
         torch.cuda.empty_cache()
         mixed = {"value": mixed_value, "unit": UNIT, "batch": B, "ms_per_step": rmx["total_ms"] / a.steps,
                  "over_fp64": mixed_value / fp64_value,
-                 "rel_err_vs_fp64": {"samples": err_f, "coefficients": err_fl, "max": max(err_f, err_fl)},
+                 "rel_err_vs_fp64": {"samples": err_f, "coefficients": err_fl, "max": max(err_f, err_fl),
+                                     "definition": "normwise max|x-y| / max|y| over each signal, max over signals"},
+                 "elementwise_rel_err_vs_fp64": {
+                     "samples": ee_f, "coefficients": ee_fl, "max": max(ee_f, ee_fl),
+                     "definition": "max_i |x_i-y_i| / max(|y_i|, 1e-3 max|y|): elementwise, floor 1e-3 of the "
+                                   "largest magnitude"},
                  "roundtrip_rel_err": err_rt}
         headline = {"value": mixed_value, "run": rmx, "units_per_step": B, "precision": "mixed"}
 
@@ -406,7 +471,7 @@ def run_ours(a):
         roof = {"kernel": dom, "bound": "tensor", "achieved": achieved, "peak": int8_peak, "unit": "TOP/s",
                 "frac": achieved / int8_peak,
                 "peak_source": "tcgen05.mma kind::i8 128x256x32 back-to-back on this GPU "
-                               "(so3gpu_measure_int8_mma_peak); nominal int8 dense peak 4500 TOP/s",
+                               "(so3_b200/peaks: tcgen05 probe); nominal int8 dense peak 4500 TOP/s",
                 "algorithmic": f"{macs:.4g} int8 MACs per launch (28 digit products, batch {B}, "
                                f"stage = slicing kernel + tensor-core kernel; int8 peak measured with tcgen05)"}
     else:
@@ -414,10 +479,47 @@ def run_ours(a):
         achieved = amount / t_launch / 1e12
         roof = {"kernel": dom, "bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                 "frac": achieved / fp64_peak,
-                "peak_source": "FP64 FMA-chain microbenchmark on this GPU (so3gpu_measure_fp64_peak); the "
+                "peak_source": "FP64 FMA-chain microbenchmark on this GPU (so3_b200/peaks); the "
                                "measured-peaks file has no FP64 figure", "algorithmic": desc + " per launch"}
     roof["traffic"] = traffic_from_profiles(dom, L, N)
+    roof["traffic_source"] = "profiles/dram_traffic.txt (ncu dram__bytes_read.sum + dram__bytes_write.sum)"
     roof["avg_ms"] = per_launch[dom]
+    if dom.startswith("mixed"):
+        # FP64-equivalent: the flops of the FP64 algorithm the int8 products replace
+        if dom == "mixed_fwd_beta":
+            planes = 2 * N - 1
+            fl64 = 2.0 * planes * (2 * L - 1) * 2 * L * L * B  # dense real map R_s on re/im of every column
+            what = "dense beta map R_s: 2 flops x (2N-1)(2L-1) columns x re/im x L x L, per signal"
+        else:
+            fl64 = 4.0 * contraction_macs(L, N) * B
+            what = "4 flops x complex-by-real MACs of the contraction, per signal"
+        roof["fp64_equivalent"] = {"achieved": fl64 / t_launch / 1e12, "unit": "TFLOP/s",
+                                   "fp64_peak": fp64_peak, "frac_of_fp64_peak": fl64 / t_launch / 1e12 / fp64_peak,
+                                   "algorithmic": what}
+
+    # per-stage HBM roofline of every stage of the headline step and of the FP64 step
+    hbm, hbm_src = hbm_peak()
+    sb = stage_bytes(L, N)
+
+    def stage_roof(stg, units):
+        out = {}
+        for k, (tot, cnt) in stg.items():
+            if k not in sb or cnt == 0:
+                continue
+            ms = tot / cnt
+            by = sb[k] * units(k)
+            out[k] = {"ms_per_launch": round(ms, 4), "bytes_per_launch": by,
+                      "gbs": round(by / (ms * 1e-3) / 1e9, 1), "frac_hbm": round(by / (ms * 1e-3) / 1e9 / hbm, 3)}
+        return out
+
+    hbm_stages = {"peak_gbs": hbm, "peak_source": hbm_src, "fp64_step": stage_roof(r64["stages"], lambda k: 1)}
+    if mixed:
+        hbm_stages["split_step"] = stage_roof(run["stages"], lambda k: B if k.startswith("mixed") else 1)
+
+    # ---- config C3: 512 signals, L=128, N=16, Gaussian (l+1)^-2, split vs FP64
+    c3 = None
+    if a.c3 > 0 and B > 0:
+        c3 = run_c3(so3, synth, a.c3, rank, dev, a.steps, a.warmup, stream, sdist, local, world)
 
     # ---- end to end through the drop-in C ABI with host buffers
     e2e = None
@@ -458,6 +560,12 @@ def run_ours(a):
                              f"n-planes per direction, {samp_s:.1f} s) plus the gamma FFT passes, scaled to all "
                              f"planes; {procs} concurrent single-threaded processes",
                    "seconds_per_unit_per_process": unit_s}
+            if a.cpu_full_unit:
+                full_s = cpu_full_unit_seconds(L, N, procs)
+                cpu["full_unit_check"] = {"seconds_per_unit_per_process": full_s, "value": procs / full_s,
+                                          "estimate_over_full": unit_s / full_s,
+                                          "what": "one full inverse+forward (all planes) per process, no "
+                                                  "extrapolation, same processes"}
         except Exception as ex:  # the CPU baseline never blocks the GPU line
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {ex}"}
 
@@ -465,7 +573,9 @@ def run_ours(a):
         lat = run["lat"]
         line = {"metric": METRIC, "value": headline["value"], "unit": UNIT, "n_gpus": world, "steps": a.steps,
                 "warmup": a.warmup, "ms_per_step": run["total_ms"] / a.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "int8 Ozaki split (7 x 7-bit digits, 49-bit fixed point, exact int32 sums) + f64"
+                if mixed else "f64", "data": "synthetic",
                 "config": dict(workload(L, N), batch=B if mixed else 1,
                                step=f"inverse_batch + forward_batch of {B} signals, split-precision contractions"
                                if mixed else "one inverse + one forward, FP64"),
@@ -477,11 +587,61 @@ def run_ours(a):
                          "latency_ms": {"p50": statistics.median(r64["lat"]), "p99": pct(r64["lat"], 0.99)}},
                 "latency_ms": {"p50": statistics.median(lat), "p99": pct(lat, 0.99)},
                 "stage_ms_per_transform": {k: round(v, 4) for k, v in per_signal.items()},
-                "gpu_launches": int(run["launches"]), "roofline": roof, "e2e": e2e, "cpu_baseline": cpu,
+                "gpu_launches": int(run["launches"]), "roofline": roof, "stage_hbm": hbm_stages,
+                "c3": c3, "e2e": e2e, "cpu_baseline": cpu,
                 "serving": serving,
                 "clocks": run["clocks"]}
         print(json.dumps(line), flush=True)
     sdist.finalize()
+
+
+def run_c3(so3, synth, nsig, rank, dev, steps, warmup, stream, sdist, local, world):
+    """Batched split precision at its stated size: nsig complex signals at
+    L=128, N=16, MW, padded, Risbo, complex Gaussian coefficients with variance
+    (l+1)^-2; one step = inverse + forward of every signal, split precision
+    (one batch call per direction) against FP64 (signal by signal), with the
+    split path's error against FP64 on every signal."""
+    import torch
+    L, N = 128, 16
+    p = so3.SO3Parameters(L=L, N=N, L0=0, sampling_scheme=0, n_order=1, storage=0, n_mode=0, dl_method=0)
+    ctx = so3.Context(local, stream=stream)
+    fls = [torch.from_numpy(synth.gen_flmn(p, sdist.signal_seed(5000, rank, i), "gauss")).to(dev)
+           for i in range(nsig)]
+    fs = [torch.empty(so3.f_size(p), dtype=torch.complex128, device=dev) for _ in range(nsig)]
+    backs = [torch.zeros(so3.flmn_size(p), dtype=torch.complex128, device=dev) for _ in range(nsig)]
+    f64 = [torch.empty_like(fs[0]) for _ in range(nsig)]
+    b64 = [torch.zeros_like(backs[0]) for _ in range(nsig)]
+
+    def step_mx():
+        ctx.inverse_batch(fls, p, "mixed", outs=fs)
+        ctx.forward_batch(fs, p, "mixed", outs=backs)
+
+    def step_64():
+        ctx.inverse_batch(fls, p, "fp64", outs=f64)
+        ctx.forward_batch(f64, p, "fp64", outs=b64)
+
+    r64 = timed_steps(step_64, steps, warmup, stream, ctx, so3, sdist, local, world)
+    rmx = timed_steps(step_mx, steps, warmup, stream, ctx, so3, sdist, local, world)
+    v64 = sdist.job_throughput(world * steps * nsig, r64["total_ms"] / 1e3)
+    vmx = sdist.job_throughput(world * steps * nsig, rmx["total_ms"] / 1e3)
+    # split forward on the FP64 samples, so each direction's error is its own
+    ctx.forward_batch(f64, p, "mixed", outs=backs)
+    torch.cuda.synchronize()
+    en_f = en_b = ee_f = ee_b = 0.0
+    for i in range(nsig):
+        en_f = max(en_f, float(((fs[i] - f64[i]).abs().max() / f64[i].abs().max()).item()))
+        ee_f = max(ee_f, elem_err(fs[i], f64[i]))
+        en_b = max(en_b, float(((backs[i] - b64[i]).abs().max() / b64[i].abs().max()).item()))
+        ee_b = max(ee_b, elem_err(backs[i], b64[i]))
+    out = {"workload": f"{nsig} complex signals, L={L}, N={N}, MW, padded, Risbo, Gaussian (l+1)^-2",
+           "mixed": vmx, "fp64": v64, "unit": UNIT, "over_fp64": vmx / v64,
+           "ms_per_step": {"mixed": rmx["total_ms"] / steps, "fp64": r64["total_ms"] / steps},
+           "rel_err_vs_fp64": {"samples": en_f, "coefficients": en_b},
+           "elementwise_rel_err_vs_fp64": {"samples": ee_f, "coefficients": ee_b, "floor": 1e-3}}
+    del fls, fs, backs, f64, b64
+    ctx.close()
+    torch.cuda.empty_cache()
+    return out
 
 
 def run_e2e(so3, p, fl_host, steps, local, world, dist):

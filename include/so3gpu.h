@@ -79,14 +79,6 @@ int so3gpu_harmonic_convolution(so3gpu_context *ctx, void *hlmn, const so3_param
  * inverse / forward contraction of a batch) and resets them. */
 int so3gpu_stage_timing(so3gpu_context *ctx, int enable);
 int so3gpu_stage_times(so3gpu_context *ctx, double *total_ms, long long *counts, int n);
-/* Measured FP64 fused multiply-add throughput of the device in TFLOP/s
- * (2 flops per FMA), from a register-resident FMA chain kernel. */
-double so3gpu_measure_fp64_peak(int device);
-/* Measured int8 tensor-core throughput in TOP/s (2 ops per multiply-add) of
- * tcgen05.mma kind::i8 (M=128, N=256, K=32, shared-memory operands, tensor-
- * memory accumulators), the instruction of the split-precision contractions. */
-double so3gpu_measure_int8_mma_peak(int device);
-
 /* Kernel variants of the DFT stages for the geometry of p (L, N, sampling,
  * reality) on a device: 8 entries indexed like so3gpu_stage_times (only the
  * FFT stages have more than one variant).  The autotuner fills them on the

@@ -84,8 +84,6 @@ SIGNATURES = {
     "so3gpu_harmonic_convolution": (_I, [_VP, _VP, _P, _VP, _P, _VP, _P]),
     "so3gpu_stage_timing": (_I, [_VP, _I]),
     "so3gpu_stage_times": (_I, [_VP, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong), _I]),
-    "so3gpu_measure_fp64_peak": (ctypes.c_double, [_I]),
-    "so3gpu_measure_int8_mma_peak": (ctypes.c_double, [_I]),
     "so3gpu_get_stage_variants": (_I, [_I, _P, _VP]),
     "so3gpu_inverse_batch": (_I, [_VP, _VP, _VP, _I, _P, _I]),
     "so3gpu_server_create": (_VP, [_I, ctypes.c_size_t, _I, _I, _I]),

@@ -353,20 +353,6 @@ STAGES = ["inv_contract", "inv_beta", "inv_alpha", "inv_gamma", "fwd_gamma", "fw
 PRECISIONS = {"fp64": 0, "mixed": 1}
 
 
-def measure_fp64_peak(device: int = 0) -> float:
-    """Measured FP64 FMA throughput (TFLOP/s) of the device."""
-    v = _lib.load().so3gpu_measure_fp64_peak(device)
-    _lib.check("measure_fp64_peak")
-    return v
-
-
-def measure_int8_mma_peak(device: int = 0) -> float:
-    """Measured int8 mma.sync (m16n8k32) throughput in TOP/s."""
-    v = _lib.load().so3gpu_measure_int8_mma_peak(device)
-    _lib.check("measure_int8_mma_peak")
-    return v
-
-
 def workspace_size(p) -> int:
     return _lib.load().so3gpu_workspace_size(ctypes.byref(_s(p)))
 

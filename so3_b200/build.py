@@ -19,6 +19,8 @@ CSRC = os.path.join(PKG, "csrc")
 OUT_DIR = os.path.join(PKG, "lib")
 OBJ_DIR = os.path.join(PKG, "_build")
 LIB = os.path.join(OUT_DIR, "libso3gpu.so")
+PEAKS_SRC = os.path.join(PKG, "peaks", "peaks.cu")
+PEAKS_LIB = os.path.join(OUT_DIR, "libso3peaks.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
@@ -56,7 +58,24 @@ def _compile(src: str, verbose: bool) -> str:
     return obj
 
 
+def build_peaks(force: bool = False) -> str:
+    """The benchmark's throughput probes (not part of the product library)."""
+    deps = [PEAKS_SRC, os.path.join(CSRC, "tc_sm100.cuh"), __file__]
+    if not force and os.path.exists(PEAKS_LIB) and all(
+            os.path.getmtime(d) <= os.path.getmtime(PEAKS_LIB) for d in deps):
+        return PEAKS_LIB
+    os.makedirs(OUT_DIR, exist_ok=True)
+    tmp = PEAKS_LIB + ".tmp"
+    cmd = [NVCC] + ARCH + FLAGS + ["-shared", "-cudart", "static", PEAKS_SRC, "-o", tmp]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {PEAKS_SRC}:\n{r.stdout}\n{r.stderr}")
+    os.replace(tmp, PEAKS_LIB)
+    return PEAKS_LIB
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
+    build_peaks(force)
     if not force and up_to_date():
         return LIB
     os.makedirs(OUT_DIR, exist_ok=True)

@@ -516,28 +516,6 @@ int so3gpu_stage_times(so3gpu_context* c, double* total_ms, long long* counts, i
   return t_status = 0;
 }
 
-double so3gpu_measure_fp64_peak(int device) {
-  DeviceScope ds(device);
-  double tf = 0.0;
-  if (so3g::measure_fp64_fma_rate(&tf)) {
-    t_status = so3g::kCudaError;
-    return 0.0;
-  }
-  t_status = 0;
-  return tf;
-}
-
-double so3gpu_measure_int8_mma_peak(int device) {
-  DeviceScope ds(device);
-  double tops = 0.0;
-  if (so3g::measure_int8_mma_rate(&tops)) {
-    t_status = so3g::kCudaError;
-    return 0.0;
-  }
-  t_status = 0;
-  return tops;
-}
-
 int so3gpu_get_stage_variants(int device, const so3_parameters_t* p, int* var) {
   if (!p || !var) return t_status = so3g::fail(so3g::kInvalidParameter, "null argument"), 0;
   t_status = 0;

@@ -218,8 +218,6 @@ int autotune_stages(Geometry* g, const FftPlan& pP, const FftPlan& pg, const Fft
                     double2* W, cudaStream_t s, int reps);
 // Number of kernel variants the tuner can choose from for a stage.
 int stage_variants(const Geometry& g, const FftPlan& pP, const FftPlan& pg, const FftPlan& pc, int stage);
-int measure_fp64_fma_rate(double* tflops);
-int measure_int8_mma_rate(double* tops);
 
 // Split-precision (int8 tensor-core) contractions of a batch of complex
 // signals sharing one parameter set.  flmn_dev / W: per-signal coefficient

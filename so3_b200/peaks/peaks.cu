@@ -1,13 +1,23 @@
-// Throughput probes: the denominators the contraction kernels are reported
-// against (the measured peaks file of this pool carries HBM and BF16 figures
-// only).  FP64: each thread runs 8 independent FMA chains in registers.
-// int8 tensor cores: back-to-back tcgen05.mma kind::i8 products from shared
-// memory into tensor memory (the instruction the split-precision contractions
-// issue).
-#include "so3gpu_internal.h"
+// Throughput probes of the benchmark (not part of libso3gpu): the
+// denominators the contraction kernels are reported against, built into
+// so3_b200/lib/libso3peaks.so and loaded by bench.py only.  FP64: each
+// thread runs 8 independent FMA chains in registers.  int8 tensor cores:
+// back-to-back tcgen05.mma kind::i8 products from shared memory into tensor
+// memory (the instruction the split-precision contractions issue).  HBM: a
+// device-to-device copy of a buffer far larger than L2.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
 #include "tc_sm100.cuh"
 
-namespace so3g {
+namespace {
+using namespace so3g;
+
+#define PK_CUDA(call)                            \
+  do {                                           \
+    if ((call) != cudaSuccess) return -1.0;      \
+  } while (0)
 
 __global__ void fp64_fma_chain(double* out, int iters, double a, double b) {
   double x[8];
@@ -67,24 +77,22 @@ __global__ void __launch_bounds__(128, 1) int8_tc_chain(int iters, int* flag) {
   }
 }
 
-int measure_int8_mma_rate(double* tops) {
+double int8_mma_tops() {
   int dev = 0, sms = 0;
-  SO3G_CUDA(cudaGetDevice(&dev));
-  SO3G_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  PK_CUDA(cudaGetDevice(&dev));
+  PK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   int* flag = nullptr;
-  SO3G_CUDA(cudaMalloc(&flag, sizeof(int)));
-  SO3G_CUDA(cudaMemset(flag, 0, sizeof(int)));
+  PK_CUDA(cudaMalloc(&flag, sizeof(int)));
+  PK_CUDA(cudaMemset(flag, 0, sizeof(int)));
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   const int blocks = sms, iters = 256;
   int8_tc_chain<<<blocks, 128>>>(iters, flag);  // warm-up
-  SO3G_LAUNCHED();
   float best = 1e30f;
   for (int r = 0; r < 5; r++) {
     cudaEventRecord(e0);
     int8_tc_chain<<<blocks, 128>>>(iters, flag);
-    SO3G_LAUNCHED();
     cudaEventRecord(e1);
     cudaEventSynchronize(e1);
     float ms = 0;
@@ -96,30 +104,27 @@ int measure_int8_mma_rate(double* tops) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaFree(flag);
-  SO3G_CUDA(cudaGetLastError());
-  if (h) return fail(kCudaError, "int8 tensor-core probe: a wait timed out");
+  PK_CUDA(cudaGetLastError());
+  if (h) return -1.0;  // a bounded wait gave up
   const double ops = 2.0 * 128 * 256 * 32 * 64.0 * iters * (double)blocks;
-  *tops = ops / (best * 1e-3) / 1e12;
-  return kOk;
+  return ops / (best * 1e-3) / 1e12;
 }
 
-int measure_fp64_fma_rate(double* tflops) {
+double fp64_tflops() {
   int dev = 0, sms = 0;
-  SO3G_CUDA(cudaGetDevice(&dev));
-  SO3G_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  PK_CUDA(cudaGetDevice(&dev));
+  PK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   double* out = nullptr;
-  SO3G_CUDA(cudaMalloc(&out, sizeof(double)));
+  PK_CUDA(cudaMalloc(&out, sizeof(double)));
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   const int blocks = sms * 8, threads = 256, iters = 4096;
   fp64_fma_chain<<<blocks, threads>>>(out, iters, 0.999999, 1e-7);  // warm-up
-  SO3G_LAUNCHED();
   float best = 1e30f;
   for (int r = 0; r < 5; r++) {
     cudaEventRecord(e0);
     fp64_fma_chain<<<blocks, threads>>>(out, iters, 0.999999, 1e-7);
-    SO3G_LAUNCHED();
     cudaEventRecord(e1);
     cudaEventSynchronize(e1);
     float ms = 0;
@@ -129,10 +134,57 @@ int measure_fp64_fma_rate(double* tflops) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaFree(out);
-  SO3G_CUDA(cudaGetLastError());
+  PK_CUDA(cudaGetLastError());
   const double flops = 2.0 * 8.0 * iters * (double)blocks * threads;
-  *tflops = flops / (best * 1e-3) / 1e12;
-  return kOk;
+  return flops / (best * 1e-3) / 1e12;
 }
 
-}  // namespace so3g
+// Device-to-device copy of 4 GiB (read + write counted), best of 5.
+double hbm_copy_gbs() {
+  const size_t bytes = size_t(4) << 30;
+  void *a = nullptr, *b = nullptr;
+  PK_CUDA(cudaMalloc(&a, bytes));
+  if (cudaMalloc(&b, bytes) != cudaSuccess) {
+    cudaFree(a);
+    return -1.0;
+  }
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaMemset(a, 1, bytes);
+  cudaMemcpyAsync(b, a, bytes, cudaMemcpyDeviceToDevice, 0);  // warm-up
+  float best = 1e30f;
+  for (int r = 0; r < 5; r++) {
+    cudaEventRecord(e0);
+    cudaMemcpyAsync(b, a, bytes, cudaMemcpyDeviceToDevice, 0);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best) best = ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(a);
+  cudaFree(b);
+  PK_CUDA(cudaGetLastError());
+  return 2.0 * (double)bytes / (best * 1e-3) / 1e9;
+}
+
+}  // namespace
+
+// Each returns the measured rate on `device`, or a negative value on a CUDA
+// error.  FP64: TFLOP/s (2 flops per FMA); int8 tcgen05.mma M=128, N=256:
+// TOP/s (2 ops per multiply-add); HBM: GB/s of a device-to-device copy.
+extern "C" double so3peaks_fp64_tflops(int device) {
+  if (cudaSetDevice(device) != cudaSuccess) return -1.0;
+  return fp64_tflops();
+}
+extern "C" double so3peaks_int8_mma_tops(int device) {
+  if (cudaSetDevice(device) != cudaSuccess) return -1.0;
+  return int8_mma_tops();
+}
+extern "C" double so3peaks_hbm_copy_gbs(int device) {
+  if (cudaSetDevice(device) != cudaSuccess) return -1.0;
+  return hbm_copy_gbs();
+}

@@ -259,13 +259,13 @@ def stage_work(L, N):
     return {
         "inv_contract": ("fp64", 4.0 * macs, f"4 flops x {macs:.4g} complex-by-real MACs"),
         "fwd_contract": ("fp64", 4.0 * macs, f"4 flops x {macs:.4g} complex-by-real MACs"),
-        "inv_beta": ("fp64", planes * P * fft_flops(P), f"{planes * P} DFTs of {P} at 5 n log2 n"),
+        "inv_beta": ("fp64", planes * L * fft_flops(P), f"{planes * L} DFTs of {P} (column pairs) at 5 n log2 n"),
         "inv_alpha": ("fp64", planes * nb * fft_flops(P), f"{planes * nb} DFTs of {P} at 5 n log2 n"),
         "fwd_alpha": ("fp64", planes * nb * fft_flops(P), f"{planes * nb} DFTs of {P} at 5 n log2 n"),
         "inv_gamma": ("fp64", nb * P * fft_flops(ng), f"{nb * P} DFTs of {ng} at 5 n log2 n"),
         "fwd_gamma": ("fp64", nb * P * fft_flops(ng), f"{nb * P} DFTs of {ng} at 5 n log2 n"),
-        "fwd_beta_conv": ("fp64", planes * P * (fft_flops(P) + 2 * fft_flops(Pc)),
-                          f"{planes * P} x (DFT {P} + 2 DFTs {Pc}) at 5 n log2 n"),
+        "fwd_beta_conv": ("fp64", planes * L * (fft_flops(P) + 2 * fft_flops(Pc)),
+                          f"{planes * L} column pairs x (DFT {P} + 2 DFTs {Pc}) at 5 n log2 n"),
     }
 
 

@@ -1077,8 +1077,10 @@ __global__ void __launch_bounds__(256) beta_slice_kernel(BetaArgs a) {
   }
 }
 
-// Persistent: one CTA per SM walks the items (column tile, 64-row tile of
-// m', signal), column tiles fastest; D_d[c, m'] over the L beta samples in
+// Persistent: one CTA per SM walks the items (64-row tile t of m', column
+// tile, signal), t fastest: the MT items of one column tile run on
+// neighbouring CTAs at the same time, so its digits come from HBM once and
+// from L2 for the other output tiles.  D_d[c, m'] over the L beta samples in
 // chunks of 64, both operands streamed by bulk copies.
 __global__ void __launch_bounds__(kThreads, 1) beta_tc_kernel(BetaArgs a, int ntiles, int nitems) {
   extern __shared__ __align__(1024) unsigned char smraw[];
@@ -1101,7 +1103,7 @@ __global__ void __launch_bounds__(kThreads, 1) beta_tc_kernel(BetaArgs a, int nt
     if (lane == 0) {
       int G = 0;
       for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
-        const int tile = item % ntiles, rest = item / ntiles, t = rest % a.MT, sig = rest / a.MT;
+        const int t = item % a.MT, rest = item / a.MT, tile = rest % ntiles, sig = rest / ntiles;
         const int sc = (tile / a.ct) & 1;
         const size_t gt = (size_t)sig * ntiles + tile;
         const uint8_t* xs = a.xs + gt * (size_t)nk * kXStage;
@@ -1114,7 +1116,7 @@ __global__ void __launch_bounds__(kThreads, 1) beta_tc_kernel(BetaArgs a, int nt
     const int c = 32 * lq + lane, j = c >> 1, part = c & 1;
     int ia = 0;
     for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
-      const int tile = item % ntiles, rest = item / ntiles, t = rest % a.MT, sig = rest / a.MT;
+      const int t = item % a.MT, rest = item / a.MT, tile = rest % ntiles, sig = rest / ntiles;
       const int ct = tile % a.ct, sc = (tile / a.ct) & 1, p = tile / (2 * a.ct);
       const int n = p - a.plane0, r0 = t * kN;
       const int m = beta_first_m(L, n, sc) + 2 * (64 * ct + j);

@@ -115,7 +115,7 @@ struct Device {
   std::map<std::string, std::vector<signed char>> tuned;  // stage variants by geometry key
   DlTable dl[2];                                 // per dl_method
   std::map<int, std::unique_ptr<DevPlan>> ffts;  // by length
-  std::map<int, double2*> conv_kernels;          // weight kernel by L (MW/MWSS identical)
+  std::map<int, double2*> conv_kernels;          // forward-beta weight tables by 2L + (MW)
   std::map<std::string, long long*> bases;       // block bases by parameter key
   std::vector<std::unique_ptr<DigitTable>> digit_tables;
   std::map<long long, int> digit_uses;  // split-precision calls per (L, N, recursion) without a table

@@ -145,32 +145,54 @@ __device__ __forceinline__ long long row_off(const Geometry& g, int row) {
 }  // namespace
 
 // ------------------------------------------------------------------ inverse
+// Inverse beta stage, two columns per DFT.  Column m of plane n is the
+// mirror-symmetric sequence x(m') = e^{i m' theta} F(m'), x(-m') = s e^{-i m'
+// theta} F(m') with s = (-1)^{m+n} (theta = pi/P for MW, 0 for MWSS), so its
+// synthesis y(k) = F(0) + sum_{m'>0} F(m') (e^{i m' b_k} + s e^{-i m' b_k}),
+// b_k = (2k+1) pi / P (MW) or 2 k pi / P (MWSS), is a cosine (s = +1) or sine
+// (s = -1) transform.  Adjacent columns have opposite s: with A the s = +1
+// and B the s = -1 column of a pair, one DFT of
+//   z(m') = e^{i m' theta} (A + B)(m'),  z(-m') = e^{-i m' theta} (A - B)(m'),
+//   z(0) = A(0) + B(0)
+// gives y_z = y_A + y_B, and since b at the mirrored row k' (P-1-k for MW,
+// P-k mod P for MWSS) is 2 pi - b_k,
+//   y_A(k) = (y_z(k) + y_z(k')) / 2 - B(0),  y_B(k) = (y_z(k) - y_z(k')) / 2 + B(0).
+// Sequence t of a CTA is column pair q = blockIdx.x * T + t (columns 2q,
+// 2q + 1; the last pair of the 2L - 1 columns has one).
 template <class E>
 __global__ void __launch_bounds__(E::NT, E::MINB) inv_beta_kernel(Geometry g, FftPlan P, double2* __restrict__ W,
                                                              int T_, int ld_) {
   extern __shared__ double2 sm[];
+  __shared__ double2 b0s[E::fixed ? E::T : 16];  // B(0) of each pair
   const int T = E::fixed ? E::T : T_, ld = E::fixed ? E::LD : ld_;
   double2* a = sm;
   double2* b = sm + (size_t)T * ld;
   const int plane = blockIdx.y, n = plane - g.plane0;
-  const int c0 = blockIdx.x * T, ncols = 2 * g.L - 1, L = g.L, Pn = g.P;
+  const int q0 = blockIdx.x * T, ncols = 2 * g.L - 1, L = g.L, Pn = g.P;
   double2* base = W + (long long)plane * g.PS;                        // row-major output
   const double2* cbase = W + g.QOFF + (long long)plane * g.QS;        // column-major input
   if (!g.mw)
     for (int t = threadIdx.x; t < T; t += E::NT) a[t * ld + E::at(L)] = make_double2(0.0, 0.0);
+  // column 2q has s = +1 when (2q - (L-1) + n) is even
+  const bool first_is_a = ((L - 1 + n) & 1) == 0;
   auto load = [&](int t, int mp) {  // m' fastest: whole columns read contiguously
-    const int c = c0 + t;
-    double2 v = c < ncols ? cbase[(long long)c * g.CS + mp] : make_double2(0.0, 0.0);
-    const int m = c - (L - 1);
-    const double sg = ((m + n) & 1) ? -1.0 : 1.0;
-    double2 xp = v, xn = make_double2(sg * v.x, sg * v.y);
+    const int c = 2 * (q0 + t);
+    const double2 v0 = c < ncols ? cbase[(long long)c * g.CS + mp] : make_double2(0.0, 0.0);
+    const double2 v1 = c + 1 < ncols ? cbase[(long long)(c + 1) * g.CS + mp] : make_double2(0.0, 0.0);
+    const double2 A = first_is_a ? v0 : v1, B = first_is_a ? v1 : v0;
+    if (mp == 0) {
+      b0s[t] = B;
+      a[t * ld + E::at(0)] = cconj(cadd(A, B));
+      return;
+    }
+    double2 xp = cadd(A, B), xn = csub(A, B);
     if (g.mw) {
       const double2 e = cconj(__ldg(P.half + mp));  // e^{i pi m'/(2L-1)}
       xp = cmul(xp, e);
       xn = cmul(xn, cconj(e));
     }
     a[t * ld + E::at(mp)] = cconj(xp);
-    if (mp > 0) a[t * ld + E::at(Pn - mp)] = cconj(xn);
+    a[t * ld + E::at(Pn - mp)] = cconj(xn);
   };
   if constexpr (E::fixed) {  // no index division per element
     for (int t = 0; t < E::T; t++)
@@ -179,16 +201,24 @@ __global__ void __launch_bounds__(E::NT, E::MINB) inv_beta_kernel(Geometry g, Ff
     for (int idx = threadIdx.x; idx < L * T; idx += E::NT) load(idx / L, idx % L);
   }
   __syncthreads();
-  if constexpr (E::has_out) {  // rows >= nb of the extended circle are never stored
-    E::runPOut(a, b, P, [&](int t, int row, double2 v) {
-      if (row < g.nb && c0 + t < ncols) base[(long long)row * g.RS + c0 + t] = cconj(v);
-    });
-    return;
-  }
   double2* r = E::runP(a, b, T, ld, P);
+  // y_z(k) = conj(r[k]); rows k < nb of both columns, written pairwise
   for (int idx = threadIdx.x; idx < g.nb * T; idx += E::NT) {
-    const int t = idx % T, row = idx / T, c = c0 + t;
-    if (c < ncols) base[(long long)row * g.RS + c] = cconj(r[t * ld + E::at(row)]);
+    const int t = idx % T, row = idx / T, c = 2 * (q0 + t);
+    if (c >= ncols) continue;
+    int mrow = g.mw ? Pn - 1 - row : Pn - row;
+    if (mrow >= Pn) mrow -= Pn;
+    const double2 y0 = cconj(r[t * ld + E::at(row)]), y1 = cconj(r[t * ld + E::at(mrow)]);
+    const double2 B0 = b0s[t];
+    const double2 yA = make_double2(0.5 * (y0.x + y1.x) - B0.x, 0.5 * (y0.y + y1.y) - B0.y);
+    const double2 yB = make_double2(0.5 * (y0.x - y1.x) + B0.x, 0.5 * (y0.y - y1.y) + B0.y);
+    double2* dst = base + (long long)row * g.RS + c;
+    if (c + 1 < ncols) {
+      dst[0] = first_is_a ? yA : yB;
+      dst[1] = first_is_a ? yB : yA;
+    } else {
+      dst[0] = first_is_a ? yA : yB;
+    }
   }
 }
 
@@ -461,28 +491,52 @@ __global__ void __launch_bounds__(E::NT, E::MINB) fwd_alpha_pf_kernel(Geometry g
   }
 }
 
+// Forward beta stage, two columns per pipeline.  Per column (plane n,
+// order m, s = (-1)^{m+n}): extend the beta samples onto the circle with
+// x(mirror(b)) = s x(b) (mirror(b) = 2L-2-b for MW, 2L-b for MWSS), DFT,
+// divide by P, MW phase e^{-i m'' pi/P}, convolve with the quadrature weights
+// w (so3_sampling.c:32-51) through a power-of-two oversampled product and
+// fold G(m') + s G(-m') onto m' >= 0.  The spectrum v of an s = +1 column is
+// even in m'', that of an s = -1 column odd, and w = w_e + w_o with w_e the
+// even weights and w_o nonzero at p = +-1 only; so for a pair A (s = +1), B
+// (s = -1) pushed through ONE extension, DFT and convolution with w_e:
+//   out_A(m') = G(m') + G(-m')   (m' >= 1),   out_A(0) = G(0)
+//   out_B(m') = G(m') - G(-m')   (m' >= 1),   out_B(0) = i pi^2 (v(1) - v(-1))
+// (the terms of w_o cancel in both folds except in out_B(0)).  This holds for
+// the antisymmetric part of B; B's samples at its self-mirror rows (MW: row
+// L-1; MWSS: rows 0 and L), which the unpaired extension keeps as they are,
+// are taken out of the pipeline and added back through the stage's response
+// to a unit sample there (the vectors h of the weight table).  Sequence t of
+// a CTA is column pair q = blockIdx.x * T + t (columns 2q, 2q+1).
 template <class E>
 __global__ void __launch_bounds__(E::NT, E::MINB) fwd_beta_conv_kernel(Geometry g, FftPlan P, FftPlan Pc,
                                                                   const double2* __restrict__ wr,
                                                                   double2* __restrict__ W, int T_, int ld_) {
   extern __shared__ double2 sm[];
+  constexpr int TS = E::fixed ? E::T : 8;
+  __shared__ double2 selfB[TS][2];  // B's samples at its self-mirror rows
+  __shared__ double2 b0[TS];        // out_B(0)
   const int T = E::fixed ? E::T : T_, ld = E::fixed ? E::LD : ld_;
   double2* a = sm;
   double2* b = sm + (size_t)T * ld;
   const int plane = blockIdx.y, n = plane - g.plane0;
-  const int c0 = blockIdx.x * T, L = g.L, ncols = 2 * L - 1, Pn = g.P, pc = g.Pc;
-  double2* base = W + (long long)plane * g.PS;
+  const int q0 = blockIdx.x * T, L = g.L, ncols = 2 * L - 1, Pn = g.P, pc = g.Pc;
+  const bool first_is_a = ((L - 1 + n) & 1) == 0;  // column 2q has m + n even
+  const int sm0 = g.mw ? L - 1 : 0, sm1 = g.mw ? -1 : L;
+  const double2* base = W + (long long)plane * g.PS;
   for (int idx = threadIdx.x; idx < g.nb * T; idx += E::NT) {
-    const int t = idx % T, row = idx / T, c = c0 + t;
-    a[t * ld + E::at(row)] = c < ncols ? base[(long long)row * g.RS + c] : make_double2(0.0, 0.0);
-  }
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < (Pn - g.nb) * T; idx += E::NT) {
-    const int t = idx % T, row = g.nb + idx / T, c = c0 + t;
-    const int m = c - (L - 1);
-    const double sg = ((m + n) & 1) ? -1.0 : 1.0;
-    const int src = g.mw ? 2 * L - 2 - row : 2 * L - row;
-    a[t * ld + E::at(row)] = cscale(a[t * ld + E::at(src)], sg);
+    const int t = idx % T, row = idx / T, c = 2 * (q0 + t);
+    const double2 v0 = c < ncols ? base[(long long)row * g.RS + c] : make_double2(0.0, 0.0);
+    const double2 v1 = c + 1 < ncols ? base[(long long)row * g.RS + c + 1] : make_double2(0.0, 0.0);
+    const double2 A = first_is_a ? v0 : v1;
+    double2 B = first_is_a ? v1 : v0;
+    if (row == sm0 || row == sm1) {
+      selfB[t][row == sm0 ? 0 : 1] = B;
+      B = make_double2(0.0, 0.0);
+    }
+    a[t * ld + E::at(row)] = cadd(A, B);
+    const int mr = g.mw ? 2 * L - 2 - row : 2 * L - row;  // mirror row on the extended circle
+    if (mr >= g.nb && mr < Pn) a[t * ld + E::at(mr)] = csub(A, B);
   }
   __syncthreads();
   double2* r = E::runP(a, b, T, ld, P);
@@ -504,27 +558,41 @@ __global__ void __launch_bounds__(E::NT, E::MINB) fwd_beta_conv_kernel(Geometry 
     o[t * ld + E::atC(wrapi(mpp, pc))] = cconj(v);
   }
   __syncthreads();
+  for (int t = threadIdx.x; t < T; t += E::NT) {
+    // i pi^2 (v(1) - v(-1)); o holds conj(v).  Read before the first pass of
+    // the convolution below overwrites o (after its first barrier).
+    double2 d = make_double2(0.0, 0.0);
+    if (L > 1) d = cconj(csub(o[t * ld + E::atC(1)], o[t * ld + E::atC(pc - 1)]));
+    const double pi2 = 9.8696044010893586188344909998761511;
+    b0[t] = make_double2(-pi2 * d.y, pi2 * d.x);
+  }
   double2* o2 = (o == a) ? b : a;
   double2* q = E::runC(o, o2, T, ld, Pc);  // conj of the inverse DFT
   for (int idx = threadIdx.x; idx < T * pc; idx += E::NT) {
     const int t = idx / pc, k = idx - t * pc;
-    q[t * ld + E::atC(k)] = cmul(cconj(q[t * ld + E::atC(k)]), __ldg(wr + k));
+    q[t * ld + E::atC(k)] = cscale(cconj(q[t * ld + E::atC(k)]), __ldg(&wr[k].x));  // real spectrum of w_e
   }
   __syncthreads();
   double2* q2 = (q == a) ? b : a;
   double2* G = E::runC(q, q2, T, ld, Pc);
   double2* cbase = W + g.QOFF + (long long)plane * g.QS;  // column-major output
+  const double2* h0 = wr + pc;
+  const double2* h1 = wr + pc + L;
   for (int idx = threadIdx.x; idx < L * T; idx += E::NT) {
-    const int mp = idx % L, t = idx / L, c = c0 + t;  // m' fastest: whole columns written contiguously
+    const int mp = idx % L, t = idx / L, c = 2 * (q0 + t);  // m' fastest: whole columns written contiguously
     if (c >= ncols) continue;
-    const int m = c - (L - 1);
-    const double sg = ((m + n) & 1) ? -1.0 : 1.0;
-    double2 v = G[t * ld + E::atC(mp)];
+    const double2 gp = G[t * ld + E::atC(mp)];
+    double2 oa = gp, ob = b0[t];
     if (mp > 0) {
-      const double2 u = G[t * ld + E::atC(pc - mp)];
-      v = make_double2(v.x + sg * u.x, v.y + sg * u.y);
+      const double2 gm = G[t * ld + E::atC(pc - mp)];
+      oa = cadd(gp, gm);
+      ob = csub(gp, gm);
     }
-    cbase[(long long)c * g.CS + mp] = v;
+    ob = cadd(ob, cmul(selfB[t][0], __ldg(h0 + mp)));
+    if (!g.mw) ob = cadd(ob, cmul(selfB[t][1], __ldg(h1 + mp)));
+    const int ca = first_is_a ? c : c + 1, cb = first_is_a ? c + 1 : c;
+    if (ca < ncols) cbase[(long long)ca * g.CS + mp] = oa;
+    if (cb < ncols) cbase[(long long)cb * g.CS + mp] = ob;
   }
 }
 
@@ -549,7 +617,7 @@ Sizing sizing(int ld, int Tmax) {
 template <class E>
 int inv_beta(const Geometry& g, const FftPlan& p, double2* W, cudaStream_t s) {
   const Sizing z = sizing<E>(p.ld(), 16);
-  dim3 grid((2 * g.L - 1 + z.T - 1) / z.T, g.nplanes);
+  dim3 grid((g.L + z.T - 1) / z.T, g.nplanes);  // L column pairs per plane
   if (int rc = set_smem(inv_beta_kernel<E>, z.smem)) return rc;
   inv_beta_kernel<E><<<grid, E::NT, z.smem, s>>>(g, p, W, z.T, p.ld());
   return kOk;
@@ -625,7 +693,7 @@ int fwd_beta_conv(const Geometry& g, const FftPlan& p, const FftPlan& pc, const 
                   cudaStream_t s) {
   const int ld = p.ld() > pc.ld() ? p.ld() : pc.ld();
   const Sizing z = sizing<E>(ld, 8);
-  dim3 grid((2 * g.L - 1 + z.T - 1) / z.T, g.nplanes);
+  dim3 grid((g.L + z.T - 1) / z.T, g.nplanes);  // L column pairs per plane
   if (int rc = set_smem(fwd_beta_conv_kernel<E>, z.smem)) return rc;
   fwd_beta_conv_kernel<E><<<grid, E::NT, z.smem, s>>>(g, p, pc, wr, W, z.T, ld);
   return kOk;

@@ -378,36 +378,64 @@ int ensure_fft(Device* D, int n, FftPlan* out) {
 // Weight-convolution kernel: wr[r] = (2 pi / Pc) sum_p w(p) e^{+2 pi i p r / Pc},
 // w(p) = int_0^pi e^{-i p theta} sin(theta) d theta (reference
 // src/c/so3_sampling.c:32-51), |p| <= 2(L-1).
+// Tables of the forward beta stage (stages.cu), per (L, sampling), Pc + 2L
+// complex entries:
+//  [0, Pc)        2 pi / Pc * DFT(w_e): the spectrum of the even part of the
+//                 quadrature weights w_e(p) = 2 / (1 - p^2) (even p, |p| <=
+//                 2(L-1)) that the paired columns are convolved with (real);
+//  [Pc, Pc + L)   h_0(m'): the stage's output for the odd (s = -1) column of
+//                 a unit sample at its first self-mirror beta row (MW: row
+//                 L-1 at beta = pi; MWSS: row 0 at beta = 0), with the full
+//                 weights w (so3_sampling.c:32-51);
+//  [Pc + L, Pc + 2L) h_1(m'): the same for MWSS row L (beta = pi); zero for MW.
+// h(m') = G(m') - G(-m') (m' >= 1), G(0), with G = 2 pi v * w and v(m'') =
+// e^{-i m'' beta} / P, m'' in [-(L-1), L-1].
 int ensure_conv_kernel(Device* D, const Geometry& g, const double2** out) {
-  auto it = D->conv_kernels.find(g.L);
+  const int key = 2 * g.L + (g.mw ? 1 : 0);
+  auto it = D->conv_kernels.find(key);
   if (it != D->conv_kernels.end()) {
     *out = it->second;
     return kOk;
   }
-  const int Pc = g.Pc, L = g.L;
+  const int Pc = g.Pc, L = g.L, P = g.P;
+  auto weight = [&](long long p) -> cld {
+    if (p > 2LL * (L - 1) || p < -2LL * (L - 1)) return cld(0, 0);
+    if (p == 1) return cld(0, -kPiL / 2);
+    if (p == -1) return cld(0, kPiL / 2);
+    if (p % 2 != 0) return cld(0, 0);
+    return cld(2.0L / (1.0L - (long double)p * p), 0);
+  };
   std::vector<cld> w(Pc, cld(0, 0));
-  for (int p = -2 * (L - 1); p <= 2 * (L - 1); p++) {
-    cld v;
-    if (p == 1)
-      v = cld(0, -kPiL / 2);
-    else if (p == -1)
-      v = cld(0, kPiL / 2);
-    else if (p % 2 == 0)
-      v = cld(2.0L / (1.0L - (long double)p * p), 0);
-    else
-      v = cld(0, 0);
-    w[((p % Pc) + Pc) % Pc] += v;
-  }
+  for (int p = -2 * (L - 1); p <= 2 * (L - 1); p += 2) w[((p % Pc) + Pc) % Pc] += weight(p);
   fft_ld(w, +1);
-  std::vector<double2> host(Pc);
+  std::vector<double2> host((size_t)Pc + 2 * (size_t)L, make_double2(0.0, 0.0));
   for (int r = 0; r < Pc; r++) {
-    cld v = w[r] * (2.0L * kPiL / (long double)Pc);
-    host[r] = make_double2((double)v.real(), (double)v.imag());
+    // w_e is real and even: its spectrum is real
+    const long double v = w[r].real() * (2.0L * kPiL / (long double)Pc);
+    host[r] = make_double2((double)v, 0.0);
+  }
+  // correction vectors: v(m'') = (+1 or (-1)^{m''}) / P
+  for (int which = 0; which < (g.mw ? 1 : 2); which++) {
+    const bool alternating = g.mw || which == 1;  // beta = pi
+    std::vector<cld> G(2 * (size_t)L - 1);
+    for (int mp = -(L - 1); mp <= L - 1; mp++) {
+      cld acc(0, 0);
+      for (int mpp = -(L - 1); mpp <= L - 1; mpp++) {
+        const long double v = ((alternating && (mpp & 1)) ? -1.0L : 1.0L) / (long double)P;
+        acc += v * weight((long long)mp - mpp);
+      }
+      G[mp + L - 1] = acc * (2.0L * kPiL);
+    }
+    for (int mp = 0; mp < L; mp++) {
+      const cld h = mp == 0 ? G[L - 1] : G[mp + L - 1] - G[L - 1 - mp];
+      host[(size_t)Pc + (size_t)which * L + mp] = make_double2((double)h.real(), (double)h.imag());
+    }
   }
   double2* d = nullptr;
-  if (cudaMalloc(&d, Pc * sizeof(double2)) != cudaSuccess) return fail(kOutOfMemory, "conv kernel allocation failed");
-  SO3G_CUDA(cudaMemcpy(d, host.data(), Pc * sizeof(double2), cudaMemcpyHostToDevice));
-  D->conv_kernels[g.L] = d;
+  if (cudaMalloc(&d, host.size() * sizeof(double2)) != cudaSuccess)
+    return fail(kOutOfMemory, "beta-stage weight table allocation failed");
+  SO3G_CUDA(cudaMemcpy(d, host.data(), host.size() * sizeof(double2), cudaMemcpyHostToDevice));
+  D->conv_kernels[key] = d;
   *out = d;
   return kOk;
 }

@@ -35,7 +35,7 @@ static int acquire(Device* D, const so3_parameters_t& p, int real, cudaStream_t 
 
 static std::string tune_key(const so3_parameters_t& p, int real) {
   return std::to_string(p.L) + "/" + std::to_string(p.N) + "/" + std::to_string((int)p.sampling_scheme) + "/" +
-         std::to_string(real);
+         std::to_string(real) + "/" + std::to_string(p.steerable ? 1 : 0);
 }
 
 // Threads that must not stop for tuning (the request server's worker) use
@@ -229,7 +229,7 @@ int copy_rows(void* dst, const void* src, const Geometry& g, int r0, int r1, cud
   const size_t es = g.real ? sizeof(double) : sizeof(double2);
   const size_t pitch = (size_t)g.nb * g.na * es, off = (size_t)r0 * g.na * es;
   SO3G_CUDA(cudaMemcpy2DAsync(static_cast<char*>(dst) + off, pitch, static_cast<const char*>(src) + off, pitch,
-                              (size_t)(r1 - r0) * g.na * es, g.ng, kind, s));
+                              (size_t)(r1 - r0) * g.na * es, g.nf, kind, s));
   return kOk;
 }
 
@@ -272,7 +272,7 @@ int run_inverse_staged(Device* D, Workspace* wk, const so3_parameters_t& p, int 
   timer_begin(T, s, &ev);
   if ((rc = launch_inv_alpha(g, r.pP, W, s))) return rc;
   timer_end(T, s, kStInvAlpha, ev);
-  const size_t out_bytes = (size_t)g.ng * g.nb * g.na * (g.real ? 8 : 16);
+  const size_t out_bytes = (size_t)g.nf * g.nb * g.na * (g.real ? 8 : 16);
   const int kr = split(g.nb, io.host_out ? out_bytes : 0, 1, rb);
   timer_begin(T, s, &ev);
   for (int k = 0; k < kr; k++) {
@@ -303,7 +303,7 @@ int run_forward_staged(Device* D, Workspace* wk, const so3_parameters_t& p, int 
   cudaEvent_t ev;
   int rc;
   int nb[kMaxChunks + 1], rb[kMaxChunks + 1];
-  const size_t in_bytes = (size_t)g.ng * g.nb * g.na * (g.real ? 8 : 16);
+  const size_t in_bytes = (size_t)g.nf * g.nb * g.na * (g.real ? 8 : 16);
   const int kr = split(g.nb, io.host_in ? in_bytes : 0, 1, rb);
   timer_begin(T, s, &ev);
   for (int k = 0; k < kr; k++) {

@@ -57,7 +57,9 @@ struct Geometry {
   int real;     // reality flag of the transform being run
   int na, nb;   // alpha / beta samples
   int P;        // DFT length over alpha and over the extended beta circle (= na)
-  int ng;       // gamma samples 2N-1
+  int ng;       // gamma DFT length: 2N-1, or 2N for steerable signals
+  int nf;       // gamma samples of the caller's f: 2N-1, or N for steerable signals
+  int steer;    // steerable signal (complex only): supersampled gamma axis
   int nplanes;  // 2N-1 (complex) or N (real)
   int plane0;
   long RS, PS;

@@ -293,6 +293,8 @@ __global__ void __launch_bounds__(E::NT, E::MINB) inv_gamma_kernel(Geometry g, F
     E::runIO(in, out, a, b, P);
     return;
   }
+  if (!REAL && g.steer)  // the 2N-point circle of a steerable signal has no plane n = N
+    for (int t = threadIdx.x; t < T; t += E::NT) a[t * ld + E::at(g.N)] = make_double2(0.0, 0.0);
   for (int idx = threadIdx.x; idx < g.nplanes * T; idx += E::NT) {
     const int t = idx % T, p = idx / T, al = a0 + t;
     double2 v = al < g.na ? W[(long long)p * g.PS + (long long)row * g.RS + al] : make_double2(0.0, 0.0);
@@ -312,7 +314,7 @@ __global__ void __launch_bounds__(E::NT, E::MINB) inv_gamma_kernel(Geometry g, F
   __syncthreads();
   double2* r = E::runP(a, b, T, ld, P);
   const long long plane_sz = (long long)g.nb * g.na;
-  for (int idx = threadIdx.x; idx < ng * T; idx += E::NT) {
+  for (int idx = threadIdx.x; idx < g.nf * T; idx += E::NT) {  // steerable: the first N of 2N samples
     const int t = idx % T, gi = idx / T, al = a0 + t;
     if (al >= g.na) continue;
     const long long o = (long long)gi * plane_sz + (long long)row * g.na + al;
@@ -374,7 +376,8 @@ __global__ void __launch_bounds__(E::NT, E::MINB) fwd_gamma_kernel(Geometry g, F
   double2* b = sm + (size_t)T * ld;
   const int row = row0 + blockIdx.y, a0 = blockIdx.x * T, ng = g.ng;
   const long long plane_sz = (long long)g.nb * g.na;
-  const double scale = 2.0 * 3.141592653589793238462643383279502884 / ng;
+  // 2 pi / (2N-1); steerable (so3_core.c:309-328): 2 pi / N over the N samples
+  const double scale = 2.0 * 3.141592653589793238462643383279502884 / g.nf;
   if constexpr (!REAL && E::io) {
     // the plan reads gamma sample k and writes plane (k + plane0) mod ng
     // straight from / to global memory (complex: nplanes == ng)
@@ -395,7 +398,7 @@ __global__ void __launch_bounds__(E::NT, E::MINB) fwd_gamma_kernel(Geometry g, F
   for (int idx = threadIdx.x; idx < ng * T; idx += E::NT) {
     const int t = idx % T, gi = idx / T, al = a0 + t;
     double2 v = make_double2(0.0, 0.0);
-    if (al < g.na) {
+    if (al < g.na && gi < g.nf) {  // steerable: samples N..2N-1 of the circle are zero
       const long long o = (long long)gi * plane_sz + (long long)row * g.na + al;
       if (REAL)
         v = make_double2(static_cast<const double*>(fin)[o], 0.0);
@@ -410,7 +413,10 @@ __global__ void __launch_bounds__(E::NT, E::MINB) fwd_gamma_kernel(Geometry g, F
     const int t = idx % T, p = idx / T, al = a0 + t;
     if (al >= g.na) continue;
     const int k = REAL ? p : wrap1(p - g.plane0, ng);
-    W[(long long)p * g.PS + (long long)row * g.RS + al] = cscale(r[t * ld + E::at(k)], scale);
+    // steerable: only n = N-1 (mod 2) is analysed (so3_core.c:315); the other planes are zero
+    const bool keep = !g.steer || (((p - g.plane0) - (g.N - 1)) & 1) == 0;
+    W[(long long)p * g.PS + (long long)row * g.RS + al] =
+        keep ? cscale(r[t * ld + E::at(k)], scale) : make_double2(0.0, 0.0);
   }
 }
 

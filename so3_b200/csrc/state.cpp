@@ -32,7 +32,9 @@ Geometry make_geometry(const so3_parameters_t& p, int real) {
   g.na = g.mw ? 2 * p.L - 1 : 2 * p.L;
   g.nb = g.mw ? p.L : p.L + 1;
   g.P = g.na;
-  g.ng = 2 * p.N - 1;
+  g.steer = p.steerable != 0;
+  g.ng = g.steer ? 2 * p.N : 2 * p.N - 1;
+  g.nf = g.steer ? p.N : 2 * p.N - 1;
   g.nplanes = real ? p.N : 2 * p.N - 1;
   g.plane0 = real ? 0 : p.N - 1;
   g.RS = ((2L * p.L + 7) / 8) * 8;
@@ -101,7 +103,10 @@ int validate(const so3_parameters_t& p, int real) {
     return fail(kInvalidParameter, "Invalid dl method");
   if (p.storage == SO3_STORAGE_COMPACT && p.N > p.L)
     return fail(kInvalidParameter, "compact storage needs N <= L");
-  if (p.steerable) return fail(kUnsupported, "steerable signals are not supported by the GPU path");
+  // the reference's real transforms ignore the flag (so3_core.c:526-547) and
+  // write 2N-1 gamma planes into a buffer sized for the N of a steerable signal
+  if (p.steerable && (p.reality || real))
+    return fail(kUnsupported, "steerable signals are supported for complex transforms only");
   if (p.L > 4096) return fail(kUnsupported, "L > 4096 is not supported");
   if (p.N > 2048) return fail(kUnsupported, "N > 2048 is not supported");
   double fsz = (double)(2 * p.L) * (p.L + 1) * (2 * p.N - 1);

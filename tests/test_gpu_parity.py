@@ -159,9 +159,9 @@ def test_invalid_parameters_return_status():
     p = params(8, 4, mode=9)
     with pytest.raises(so3.SO3Error, match="status 1"):
         so3.inverse(np.zeros(8 * 8 * 7, complex), p)
-    p = params(8, 4, steerable=1)
+    p = params(8, 4, steerable=1, reality=1)  # steerable: complex transforms only
     with pytest.raises(so3.SO3Error, match="status 3"):
-        so3.inverse(np.zeros(8 * 8 * 7, complex), p)
+        so3.inverse(np.zeros(8 * 8 * 4, complex), p)
 
 
 def test_device_api_matches_host_api():

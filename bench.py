@@ -57,6 +57,8 @@ def args_():
                          "with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     ap.add_argument("--c3", type=int, default=512,
                     help="signals of the L=128, N=16 batched split-precision leg (0: skip it)")
+    ap.add_argument("--c4", type=int, default=64,
+                    help="kernels of the L=1024 directional-convolution leg (0: skip it)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-full-unit", action="store_true",
                     help="also time one full CPU unit per process (no extrapolation; minutes at L=512, N=64)")
@@ -521,6 +523,11 @@ def run_ours(a):
     if a.c3 > 0 and B > 0:
         c3 = run_c3(so3, synth, a.c3, rank, dev, a.steps, a.warmup, stream, sdist, local, world)
 
+    # ---- config C4: one S^2 signal at L=1024 convolved with kernels (N=8), inverse to samples
+    c4 = None
+    if a.c4 > 0 and B > 0:
+        c4 = run_c4(so3, synth, a.c4, rank, dev, stream, sdist, local, world)
+
     # ---- end to end through the drop-in C ABI with host buffers
     e2e = None
     if not a.no_e2e:
@@ -588,7 +595,7 @@ def run_ours(a):
                 "latency_ms": {"p50": statistics.median(lat), "p99": pct(lat, 0.99)},
                 "stage_ms_per_transform": {k: round(v, 4) for k, v in per_signal.items()},
                 "gpu_launches": int(run["launches"]), "roofline": roof, "stage_hbm": hbm_stages,
-                "c3": c3, "e2e": e2e, "cpu_baseline": cpu,
+                "c3": c3, "c4": c4, "e2e": e2e, "cpu_baseline": cpu,
                 "serving": serving,
                 "clocks": run["clocks"]}
         print(json.dumps(line), flush=True)
@@ -639,6 +646,51 @@ def run_c3(so3, synth, nsig, rank, dev, steps, warmup, stream, sdist, local, wor
            "rel_err_vs_fp64": {"samples": en_f, "coefficients": en_b},
            "elementwise_rel_err_vs_fp64": {"samples": ee_f, "coefficients": ee_b, "floor": 1e-3}}
     del fls, fs, backs, f64, b64
+    ctx.close()
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_c4(so3, synth, nker, rank, dev, stream, sdist, local, world, chunk=16, steps=2, warmup=2):
+    """Directional convolution at L=1024: one S^2 signal flm (complex
+    Gaussian, variance (l+1)^-2) convolved with nker kernels glm (complex
+    Gaussian for |m| < 8, zero otherwise) by so3_conv_s2toso3_harmonic_
+    convolution (N=8), each result inverse-transformed to MW samples; the
+    kernels run in chunks of `chunk` (so3gpu_s2toso3_inverse_batch), FP64
+    against split precision (h built inside the contraction's operand load).
+    One step = all nker kernels; value in kernels/s."""
+    import torch
+    L, N = 1024, 8
+    hp = so3.SO3Parameters(L=L, N=N, L0=0, sampling_scheme=0, n_order=1, storage=0, n_mode=0, dl_method=0)
+    ctx = so3.Context(local, stream=stream)
+    flm = torch.from_numpy(synth.gen_flm(L, sdist.signal_seed(7000, rank, 0), "gauss")).to(dev)
+    glms = [torch.from_numpy(synth.gen_flm(L, sdist.signal_seed(7001, rank, k), "gauss", mmax=N - 1)).to(dev)
+            for k in range(nker)]
+    outs = [torch.empty(so3.f_size(hp), dtype=torch.complex128, device=dev) for _ in range(chunk)]
+    ref = [torch.empty(so3.f_size(hp), dtype=torch.complex128, device=dev) for _ in range(chunk)]
+
+    def step(prec):
+        for c0 in range(0, nker, chunk):
+            g = glms[c0:c0 + chunk]
+            ctx.s2toso3_inverse_batch(hp, flm, g, prec, outs=outs[:len(g)])
+
+    res = {}
+    for prec in ("fp64", "mixed"):
+        r = timed_steps(lambda: step(prec), steps, warmup, stream, ctx, so3, sdist, local, world)
+        res[prec] = sdist.job_throughput(world * steps * nker, r["total_ms"] / 1e3)
+    # error of split against FP64 on the first chunk
+    g = glms[:chunk]
+    ctx.s2toso3_inverse_batch(hp, flm, g, "fp64", outs=ref[:len(g)])
+    ctx.s2toso3_inverse_batch(hp, flm, g, "mixed", outs=outs[:len(g)])
+    torch.cuda.synchronize()
+    en = max(float(((o - r_).abs().max() / r_.abs().max()).item()) for o, r_ in zip(outs[:len(g)], ref))
+    ee = max(elem_err(o, r_) for o, r_ in zip(outs[:len(g)], ref))
+    out = {"workload": f"flm L={L} (Gaussian (l+1)^-2) convolved with {nker} kernels (|m| < {N}), N={N}, "
+                       f"inverse to MW samples, chunks of {chunk}",
+           "unit": "kernels/s", "fp64": res["fp64"], "mixed": res["mixed"], "over_fp64": res["mixed"] / res["fp64"],
+           "steps": steps, "warmup": warmup,
+           "rel_err_vs_fp64": en, "elementwise_rel_err_vs_fp64": ee}
+    del outs, ref, glms, flm
     ctx.close()
     torch.cuda.empty_cache()
     return out

@@ -63,6 +63,17 @@ int so3gpu_inverse_batch(so3gpu_context *ctx, void *const *f, const void *const 
 int so3gpu_forward_batch(so3gpu_context *ctx, void *const *flmn, const void *const *f, int count,
                          const so3_parameters_t *parameters, int precision);
 
+/* Directional convolutions of one S^2 signal with `count` kernels, then the
+ * inverse transform (no counterpart in the reference; the composition of
+ * so3_conv_s2toso3_harmonic_convolution, src/c/so3_conv.c:186-215, with
+ * so3_core_inverse_via_ssht): f[k] = inverse(h_k), h_k,lmn = flm_lm
+ * conj(glm[k]_ln) 8 pi^2 / (2l+1), h parameters `h_parameters` (complex).
+ * flm and glm[k] hold L*L coefficients.  SO3GPU_PRECISION_FP64 materialises
+ * each h_k in the workspace and runs the FP64 inverse; MIXED_INT8 computes h
+ * inside the split-precision contraction's operand load (never stored). */
+int so3gpu_s2toso3_inverse_batch(so3gpu_context *ctx, void *const *f, const void *flm, const void *const *glm,
+                                 int count, const so3_parameters_t *h_parameters, int precision);
+
 /* Same as so3_conv_s2toso3_harmonic_convolution / so3_conv_harmonic_convolution. */
 int so3gpu_s2toso3_harmonic_convolution(so3gpu_context *ctx, void *hlmn, const so3_parameters_t *h_parameters,
                                         const void *flm, const void *glm);

@@ -324,6 +324,24 @@ class Context:
             outs = [torch.zeros(flmn_size(q), dtype=torch.complex128, device=x.device) for x in fs]
         return self._batch(self._lib.so3gpu_forward_batch, fs, outs, q, precision, "so3gpu_forward_batch")
 
+    def s2toso3_inverse_batch(self, hp, flm, glms, precision="fp64", outs=None):
+        """Samples of the directional convolutions of flm with each kernel in
+        glms (so3_conv_s2toso3_harmonic_convolution with parameters hp, then
+        the inverse transform); precision "fp64" or "mixed"."""
+        import torch
+        q = _s(hp)
+        if precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
+        if outs is None:
+            outs = [torch.empty(f_size(q), dtype=torch.complex128, device=flm.device) for _ in glms]
+        n = len(glms)
+        pg = (ctypes.c_void_p * n)(*[t.data_ptr() for t in glms])
+        pf = (ctypes.c_void_p * n)(*[t.data_ptr() for t in outs])
+        if self._lib.so3gpu_s2toso3_inverse_batch(self._c, pf, ctypes.c_void_p(flm.data_ptr()), pg, n,
+                                                  ctypes.byref(q), PRECISIONS[precision]):
+            _lib.check("so3gpu_s2toso3_inverse_batch")
+        return outs
+
     def s2toso3(self, hp, flm, glm, out=None):
         import torch
         q = _s(hp)

@@ -463,6 +463,18 @@ int so3gpu_forward_batch(so3gpu_context* c, void* const* flmn, const void* const
   return ctx_batch(c, flmn, f, count, p, precision, false);
 }
 
+int so3gpu_s2toso3_inverse_batch(so3gpu_context* c, void* const* f, const void* flm, const void* const* glm, int count,
+                                 const so3_parameters_t* hp, int precision) {
+  if (!c || !hp || !flm || (count > 0 && (!f || !glm)))
+    return t_status = so3g::fail(so3g::kInvalidParameter, "null argument");
+  for (int i = 0; i < count; i++)
+    if (!f[i] || !glm[i]) return t_status = so3g::fail(so3g::kInvalidParameter, "null signal pointer");
+  DeviceScope ds(c->device);
+  std::lock_guard<std::mutex> lk(c->mu);
+  Device* D = so3g::device_state(c->device);
+  return t_status = so3g::run_conv_inverse_batch(D, &c->wk, *hp, count, flm, glm, f, precision, c->stream);
+}
+
 int so3gpu_s2toso3_harmonic_convolution(so3gpu_context* c, void* hlmn, const so3_parameters_t* hp, const void* flm,
                                         const void* glm) {
   if (!c || !hp) return t_status = so3g::fail(so3g::kInvalidParameter, "null argument");

@@ -6,6 +6,7 @@
 #include <utility>
 #include <vector>
 
+#include "so3/so3_sampling.h"
 #include "so3gpu_internal.h"
 
 namespace so3g {
@@ -480,6 +481,62 @@ int run_forward_batch(Device* D, Workspace* wk, const so3_parameters_t& p, int r
                             base + bl.scratch_off, s);
   if (rc) return rc;
   timer_end(T, s, kStMixFwd, ev);
+  return kOk;
+}
+
+int run_conv_inverse_batch(Device* D, Workspace* wk, const so3_parameters_t& p, int nsig, const void* flm_d,
+                           const void* const* glm_d, void* const* f_d, int precision, cudaStream_t s) {
+  if (nsig < 0) return fail(kInvalidParameter, "negative batch size");
+  if (precision != kPrecFp64 && precision != kPrecMixedInt8) return fail(kInvalidParameter, "unknown precision");
+  if (p.reality) return fail(kUnsupported, "directional convolutions produce complex signals");
+  if (nsig == 0) return kOk;
+  Resources r;
+  if (int rc = acquire(D, p, 0, s, &r, false)) return rc;
+  int rc;
+  if (precision == kPrecFp64) {
+    // hlmn of each kernel after the transform's scratch; run_inverse keeps the (larger) workspace
+    const size_t wb = (workspace_bytes(p, 0) + 255) & ~size_t(255);
+    void* ws = nullptr;
+    if ((rc = ensure_ws(wk, wb + (size_t)so3_sampling_flmn_size(&p) * sizeof(double2), &ws))) return rc;
+    double2* h = reinterpret_cast<double2*>(static_cast<char*>(ws) + wb);
+    for (int b = 0; b < nsig; b++) {
+      if ((rc = launch_s2toso3(p, r.bases, static_cast<const double2*>(flm_d), static_cast<const double2*>(glm_d[b]),
+                               h, s)))
+        return rc;
+      if ((rc = run_inverse(D, wk, p, h, f_d[b], 0, s))) return rc;
+    }
+    return kOk;
+  }
+  const BatchLayout bl = batch_layout(r.g, p, 0, nsig);
+  void* ws = nullptr;
+  if ((rc = ensure_ws(wk, bl.total, &ws))) return rc;
+  char* base = static_cast<char*>(ws);
+  double2* W = reinterpret_cast<double2*>(base);
+  if ((rc = ensure_tuned(D, p, 0, &r, W, s))) return rc;
+  if ((rc = upload_table(base + bl.table_off, glm_d, nsig, s))) return rc;
+  StageTimer* T = &wk->timer;
+  cudaEvent_t ev;
+  const long long wstride = (long long)(bl.wbytes / sizeof(double2));
+  const DigitTable* tab = nullptr;
+  if ((rc = ensure_digit_table(D, r.g, p.dl_method, r.dl, s, &tab))) return rc;
+  timer_begin(T, s, &ev);
+  rc = launch_mixed_inverse(r.g, p.n_mode, nullptr, nsig, r.bases, r.dl, tab, W, wstride, base + bl.scratch_off, s,
+                            static_cast<const double2*>(flm_d),
+                            reinterpret_cast<const double2* const*>(base + bl.table_off));
+  if (rc) return rc;
+  timer_end(T, s, kStMixInv, ev);
+  for (int b = 0; b < nsig; b++) {
+    double2* Wb = W + (size_t)b * wstride;
+    timer_begin(T, s, &ev);
+    if ((rc = launch_inv_beta(r.g, r.pP, Wb, s))) return rc;
+    timer_end(T, s, kStInvBeta, ev);
+    timer_begin(T, s, &ev);
+    if ((rc = launch_inv_alpha(r.g, r.pP, Wb, s))) return rc;
+    timer_end(T, s, kStInvAlpha, ev);
+    timer_begin(T, s, &ev);
+    if ((rc = launch_inv_gamma(r.g, r.pg, Wb, f_d[b], s))) return rc;
+    timer_end(T, s, kStInvGamma, ev);
+  }
   return kOk;
 }
 

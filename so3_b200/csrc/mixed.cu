@@ -411,6 +411,11 @@ struct SliceArgs {
   uint8_t* xs;
   double* xscale;
   const double2* const* flmn;  // inverse input, per signal
+  // directional convolution (inverse only): the coefficients are h_lmn =
+  // flm_lm conj(glm_ln) 8 pi^2 / (2l+1) of so3_conv.c:186-215, computed on
+  // load (never stored); flm shared, glm per signal
+  const double2* flm;
+  const double2* const* glm;
   const double2* W;            // forward input: column-major scratch part of signal 0, signal b at W + b * wstride
   const long long* base;
   long long wstride;
@@ -440,7 +445,8 @@ constexpr int kSliceCols = 8;  // complex columns per forward slicing CTA (4 sig
 constexpr int kMuPer = 4;  // 64-byte runs of m per (n, l)
 
 struct InvColumn {
-  const double2* src;  // entry l at src[l * l + l]
+  const double2* src;   // entry l at src[l * l + l] (the signal's flmn, or flm of a convolution)
+  const double2* gsrc;  // convolution: entry l of the kernel glm at gsrc[l * l + l] (order n)
   int lmin;
   bool act, flip;
 };
@@ -452,16 +458,30 @@ __device__ __forceinline__ InvColumn inv_column(const SliceArgs& a, int sig, int
           !plane_skipped(a.n_mode, a.N, n);
   c.lmin = max(max(mu, nu), a.L0);
   c.flip = ms * ns < 0;
-  c.src = c.act ? a.flmn[sig] + a.base[a.plane0 + n] + m : nullptr;
+  c.src = c.act ? (a.flm ? a.flm + m : a.flmn[sig] + a.base[a.plane0 + n] + m) : nullptr;
+  c.gsrc = (c.act && a.flm) ? a.glm[sig] + n : nullptr;
   return c;
 }
-// Weighted entry l of the column, (2l+1)/(8 pi^2) (-1)^l on flipped columns.
+// Weighted entry l of the column (both parts), times (-1)^l on flipped
+// columns: (2l+1)/(8 pi^2) f_lmn, or for a convolution (2l+1)/(8 pi^2) h_lmn
+// = flm_lm conj(glm_ln).
+__device__ __forceinline__ double2 inv_value(const InvColumn& c, int L, int l) {
+  if (!(c.act && l < L && l >= c.lmin)) return make_double2(0.0, 0.0);
+  const double2 x = __ldg(c.src + (long long)l * l + l);
+  double2 v;
+  if (c.gsrc) {
+    const double2 gk = __ldg(c.gsrc + (long long)l * l + l);
+    v = make_double2(fma(x.x, gk.x, x.y * gk.y), fma(x.y, gk.x, -x.x * gk.y));
+  } else {
+    const double f = (2.0 * l + 1.0) * kInv8Pi2;
+    v = make_double2(x.x * f, x.y * f);
+  }
+  if (c.flip && (l & 1)) v = make_double2(-v.x, -v.y);
+  return v;
+}
 __device__ __forceinline__ double inv_entry(const InvColumn& c, int L, int l, int part) {
-  const double x = (c.act && l < L && l >= c.lmin) ? __ldg(reinterpret_cast<const double*>(c.src + (long long)l * l + l) + part)
-                                                  : 0.0;
-  double f = (2.0 * l + 1.0) * kInv8Pi2;
-  if (c.flip && (l & 1)) f = -f;
-  return x * f;
+  const double2 v = inv_value(c, L, l);
+  return part ? v.y : v.x;
 }
 
 __global__ void __launch_bounds__(256, 3) slice_inv_kernel(SliceArgs a) {
@@ -482,17 +502,11 @@ __global__ void __launch_bounds__(256, 3) slice_inv_kernel(SliceArgs a) {
       for (int l1 = l0; l1 < L; l1 += LSTEP * 8) {
         double2 x[8];
 #pragma unroll
-        for (int u = 0; u < 8; u++) {
-          const int l = l1 + LSTEP * u;
-          x[u] = (l < L && l >= col.lmin) ? __ldg(col.src + (long long)l * l + l) : make_double2(0.0, 0.0);
-        }
+        for (int u = 0; u < 8; u++) x[u] = inv_value(col, L, l1 + LSTEP * u);
 #pragma unroll
         for (int u = 0; u < 8; u++) {
-          const int l = l1 + LSTEP * u;
-          double f = (2.0 * l + 1.0) * kInv8Pi2;
-          if (col.flip && (l & 1)) f = -f;
-          mr = fmax(mr, fabs(x[u].x * f));
-          mi = fmax(mi, fabs(x[u].y * f));
+          mr = fmax(mr, fabs(x[u].x));
+          mi = fmax(mi, fabs(x[u].y));
         }
       }
     }
@@ -1279,13 +1293,16 @@ static int launch_tc(const MixArgs& m, int nsig, cudaStream_t s) {
 
 int launch_mixed_inverse(const Geometry& g, int n_mode, const double2* const* flmn_dev, int nsig,
                          const long long* bases, const double* dl, const DigitTable* tab, double2* W,
-                         long long wstride, void* scratch, cudaStream_t s) {
+                         long long wstride, void* scratch, cudaStream_t s, const double2* conv_flm,
+                         const double2* const* conv_glm) {
   if (g.real) return fail(kUnsupported, "split-precision contractions take complex signals");
   MixArgs m;
   SliceArgs sa;
   if (int rc = mixed_args(g, n_mode, nsig, scratch, &m, &sa)) return rc;
   sa.flmn = flmn_dev;
   sa.base = bases;
+  sa.flm = conv_flm;
+  sa.glm = conv_glm;
   // every signal of the last group (zeros past nsig), so the group's stage images are complete
   slice_inv_kernel<<<dim3((unsigned)(g.N * ((g.L + kMuPer - 1) / kMuPer)), (unsigned)(((nsig + kSig - 1) / kSig) * kSig)),
                      256, 0, s>>>(sa);

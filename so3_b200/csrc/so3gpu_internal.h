@@ -237,9 +237,13 @@ int ensure_beta_table(Device* D, const Geometry& g, cudaStream_t s, const BetaTa
 int launch_mixed_fwd_beta(const Geometry& g, double2* W, long long wstride, int nsig, const BetaTable* tab,
                           void* scratch, cudaStream_t s);
 // tab: resident digits of (g.L, g.N) or null (digits generated from dl).
+// conv_flm / conv_glm (device array of nsig kernel pointers): when set, the
+// coefficients of signal b are the directional convolution h_lmn = flm_lm
+// conj(glm_b,ln) 8 pi^2/(2l+1), computed on load (flmn_dev unused).
 int launch_mixed_inverse(const Geometry& g, int n_mode, const double2* const* flmn_dev, int nsig,
                          const long long* bases, const double* dl, const DigitTable* tab, double2* W,
-                         long long wstride, void* scratch, cudaStream_t s);
+                         long long wstride, void* scratch, cudaStream_t s, const double2* conv_flm = nullptr,
+                         const double2* const* conv_glm = nullptr);
 int launch_mixed_forward(const Geometry& g, int n_mode, const double2* W, long long wstride, int nsig,
                          const long long* bases, const double* dl, const DigitTable* tab, double2* const* flmn_dev,
                          int storage_compact, void* scratch, cudaStream_t s);
@@ -273,6 +277,13 @@ int run_inverse_batch(Device* D, Workspace* wk, const so3_parameters_t& p, int r
                       const void* const* flmn_d, void* const* f_d, int precision, cudaStream_t s);
 int run_forward_batch(Device* D, Workspace* wk, const so3_parameters_t& p, int real, int nsig, const void* const* f_d,
                       void* const* flmn_d, int precision, cudaStream_t s);
+// Directional convolutions of one S^2 signal flm with nsig kernels glm_d[b]
+// (so3_conv_s2toso3_harmonic_convolution with h parameters p) followed by the
+// inverse transform into f_d[b] (complex signals).  FP64: hlmn of each kernel
+// in the workspace, then the FP64 inverse.  Split precision: h is computed in
+// the contraction's operand load and never stored.
+int run_conv_inverse_batch(Device* D, Workspace* wk, const so3_parameters_t& p, int nsig, const void* flm_d,
+                           const void* const* glm_d, void* const* f_d, int precision, cudaStream_t s);
 
 // Drop-in calls on caller buffers that may live in host memory: the
 // transform runs in chunks (|n| ranges for the contractions, beta-row ranges

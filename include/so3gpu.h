@@ -63,6 +63,19 @@ int so3gpu_inverse_batch(so3gpu_context *ctx, void *const *f, const void *const 
 int so3gpu_forward_batch(so3gpu_context *ctx, void *const *flmn, const void *const *f, int count,
                          const so3_parameters_t *parameters, int precision);
 
+/* Batches of signals of different parameters (no counterpart in the
+ * reference): signal k has its own parameters[k] (any L, N, L0, sampling,
+ * storage, n-order, n-mode, recursion).  SO3GPU_PRECISION_MIXED_INT8: the
+ * Wigner contractions of all complex signals run in one int8 tensor-core
+ * launch per Delta recursion -- signals sorted by (L, N) share 16-signal
+ * operand tiles at the tile's largest L and N -- while every DFT stage runs
+ * per signal in FP64; real signals, and precision FP64, take the FP64 path
+ * per signal.  Same error contract as so3gpu_inverse_batch. */
+int so3gpu_inverse_ragged(so3gpu_context *ctx, void *const *f, const void *const *flmn,
+                          const so3_parameters_t *parameters, int count, int precision);
+int so3gpu_forward_ragged(so3gpu_context *ctx, void *const *flmn, const void *const *f,
+                          const so3_parameters_t *parameters, int count, int precision);
+
 /* Directional convolutions of one S^2 signal with `count` kernels, then the
  * inverse transform (no counterpart in the reference; the composition of
  * so3_conv_s2toso3_harmonic_convolution, src/c/so3_conv.c:186-215, with

@@ -86,6 +86,8 @@ SIGNATURES = {
     "so3gpu_stage_times": (_I, [_VP, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong), _I]),
     "so3gpu_get_stage_variants": (_I, [_I, _P, _VP]),
     "so3gpu_inverse_batch": (_I, [_VP, _VP, _VP, _I, _P, _I]),
+    "so3gpu_inverse_ragged": (_I, [_VP, _VP, _VP, _VP, _I, _I]),
+    "so3gpu_forward_ragged": (_I, [_VP, _VP, _VP, _VP, _I, _I]),
     "so3gpu_s2toso3_inverse_batch": (_I, [_VP, _VP, _VP, _VP, _I, _P, _I]),
     "so3gpu_server_create": (_VP, [_I, ctypes.c_size_t, _I, _I, _I]),
     "so3gpu_server_destroy": (None, [_VP]),

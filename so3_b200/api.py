@@ -324,6 +324,33 @@ class Context:
             outs = [torch.zeros(flmn_size(q), dtype=torch.complex128, device=x.device) for x in fs]
         return self._batch(self._lib.so3gpu_forward_batch, fs, outs, q, precision, "so3gpu_forward_batch")
 
+    def _ragged(self, fn, ins, outs, ps, precision, name):
+        if precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
+        n = len(ins)
+        arr = (Params * n)(*[_s(p) for p in ps])
+        pin = (ctypes.c_void_p * n)(*[t.data_ptr() for t in ins])
+        pout = (ctypes.c_void_p * n)(*[t.data_ptr() for t in outs])
+        if fn(self._c, pout, pin, arr, n, PRECISIONS[precision]):
+            _lib.check(name)
+        return outs
+
+    def inverse_ragged(self, flmns, ps, precision="fp64", outs=None):
+        """Inverse transforms of signals with one parameter set each (ps[k]);
+        "mixed" runs every complex signal's contraction in one ragged
+        tensor-core launch."""
+        import torch
+        if outs is None:
+            outs = [torch.empty(f_size(p), dtype=torch.float64 if p.reality else torch.complex128, device=x.device)
+                    for x, p in zip(flmns, ps)]
+        return self._ragged(self._lib.so3gpu_inverse_ragged, flmns, outs, ps, precision, "so3gpu_inverse_ragged")
+
+    def forward_ragged(self, fs, ps, precision="fp64", outs=None):
+        import torch
+        if outs is None:
+            outs = [torch.zeros(flmn_size(p), dtype=torch.complex128, device=x.device) for x, p in zip(fs, ps)]
+        return self._ragged(self._lib.so3gpu_forward_ragged, fs, outs, ps, precision, "so3gpu_forward_ragged")
+
     def s2toso3_inverse_batch(self, hp, flm, glms, precision="fp64", outs=None):
         """Samples of the directional convolutions of flm with each kernel in
         glms (so3_conv_s2toso3_harmonic_convolution with parameters hp, then

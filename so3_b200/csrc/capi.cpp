@@ -463,6 +463,28 @@ int so3gpu_forward_batch(so3gpu_context* c, void* const* flmn, const void* const
   return ctx_batch(c, flmn, f, count, p, precision, false);
 }
 
+static int ctx_ragged(so3gpu_context* c, void* const* out, const void* const* in, const so3_parameters_t* ps,
+                      int count, int precision, bool inverse) {
+  if (!c || (count > 0 && (!out || !in || !ps))) return t_status = so3g::fail(so3g::kInvalidParameter, "null argument");
+  for (int i = 0; i < count; i++)
+    if (!out[i] || !in[i]) return t_status = so3g::fail(so3g::kInvalidParameter, "null signal pointer");
+  DeviceScope ds(c->device);
+  std::lock_guard<std::mutex> lk(c->mu);
+  Device* D = so3g::device_state(c->device);
+  int rc = inverse ? so3g::run_inverse_ragged(D, &c->wk, ps, count, in, out, precision, c->stream)
+                   : so3g::run_forward_ragged(D, &c->wk, ps, count, in, out, precision, c->stream);
+  return t_status = rc;
+}
+
+int so3gpu_inverse_ragged(so3gpu_context* c, void* const* f, const void* const* flmn, const so3_parameters_t* ps,
+                          int count, int precision) {
+  return ctx_ragged(c, f, flmn, ps, count, precision, true);
+}
+int so3gpu_forward_ragged(so3gpu_context* c, void* const* flmn, const void* const* f, const so3_parameters_t* ps,
+                          int count, int precision) {
+  return ctx_ragged(c, flmn, f, ps, count, precision, false);
+}
+
 int so3gpu_s2toso3_inverse_batch(so3gpu_context* c, void* const* f, const void* flm, const void* const* glm, int count,
                                  const so3_parameters_t* hp, int precision) {
   if (!c || !hp || !flm || (count > 0 && (!f || !glm)))

@@ -540,4 +540,186 @@ int run_conv_inverse_batch(Device* D, Workspace* wk, const so3_parameters_t& p, 
   return kOk;
 }
 
+// ------------------------------------------------------------ ragged batches
+namespace {
+
+// Per-signal state of a ragged batch.
+struct RagItem {
+  int idx;  // position in the caller's arrays
+  Resources r;
+  size_t ws_off;
+};
+
+// Signals of a ragged split-precision batch: complex ones go to the
+// tensor-core contraction (per Delta recursion), real ones to the FP64 path.
+int ragged_prepare(Device* D, const so3_parameters_t* ps, int nsig, bool conv_tables, cudaStream_t s,
+                   std::vector<RagItem>* items, std::vector<int>* fp64) {
+  int Lmax[2] = {0, 0};
+  for (int i = 0; i < nsig; i++) {
+    if (int rc = validate(ps[i], ps[i].reality != 0)) return rc;
+    if (!ps[i].reality) Lmax[ps[i].dl_method] = std::max(Lmax[ps[i].dl_method], ps[i].L);
+  }
+  {
+    // Delta tables to the largest L first, so no later call regrows them
+    std::lock_guard<std::mutex> lk(D->mu);
+    const double* t;
+    for (int m = 0; m < 2; m++)
+      if (Lmax[m] > 0)
+        if (int rc = ensure_dl(D, Lmax[m], m, s, &t)) return rc;
+  }
+  size_t off = 0;
+  for (int i = 0; i < nsig; i++) {
+    if (ps[i].reality) {
+      fp64->push_back(i);
+      continue;
+    }
+    RagItem it;
+    it.idx = i;
+    if (int rc = acquire(D, ps[i], 0, s, &it.r, conv_tables)) return rc;
+    it.ws_off = off;
+    off += (workspace_bytes(ps[i], 0) + 255) & ~size_t(255);
+    items->push_back(it);
+  }
+  return kOk;
+}
+
+size_t ragged_ws_end(const std::vector<RagItem>& items, const so3_parameters_t* ps) {
+  return items.empty() ? 0 : items.back().ws_off + ((workspace_bytes(ps[items.back().idx], 0) + 255) & ~size_t(255));
+}
+
+}  // namespace
+
+int run_inverse_ragged(Device* D, Workspace* wk, const so3_parameters_t* ps, int nsig, const void* const* flmn_d,
+                       void* const* f_d, int precision, cudaStream_t s) {
+  if (nsig < 0) return fail(kInvalidParameter, "negative batch size");
+  if (precision != kPrecFp64 && precision != kPrecMixedInt8) return fail(kInvalidParameter, "unknown precision");
+  if (precision == kPrecFp64) {
+    for (int b = 0; b < nsig; b++)
+      if (int rc = run_inverse(D, wk, ps[b], flmn_d[b], f_d[b], ps[b].reality != 0, s)) return rc;
+    return kOk;
+  }
+  std::vector<RagItem> items;
+  std::vector<int> fp64;
+  if (int rc = ragged_prepare(D, ps, nsig, false, s, &items, &fp64)) return rc;
+  for (int i : fp64)  // real signals: the FP64 path, before the batch workspace is laid out
+    if (int rc = run_inverse(D, wk, ps[i], flmn_d[i], f_d[i], 1, s)) return rc;
+  if (items.empty()) return kOk;
+  const size_t sig_end = ragged_ws_end(items, ps);
+  std::vector<RaggedSig> rs[2];
+  for (const RagItem& it : items) {
+    RaggedSig r;
+    r.flmn = flmn_d[it.idx];
+    r.Wc = nullptr;  // set once the workspace exists
+    r.base = it.r.bases;
+    r.g = it.r.g;
+    r.n_mode = ps[it.idx].n_mode;
+    r.compact = ps[it.idx].storage == SO3_STORAGE_COMPACT;
+    rs[ps[it.idx].dl_method].push_back(r);
+  }
+  const size_t rag = std::max(ragged_scratch_bytes(rs[0], false), ragged_scratch_bytes(rs[1], false));
+  void* ws = nullptr;
+  if (int rc = ensure_ws(wk, sig_end + rag, &ws)) return rc;
+  char* wsb = static_cast<char*>(ws);
+  int rc;
+  {
+    int k[2] = {0, 0};
+    for (RagItem& it : items) {
+      double2* W = reinterpret_cast<double2*>(wsb + it.ws_off);
+      if ((rc = ensure_tuned(D, ps[it.idx], 0, &it.r, W, s))) return rc;
+      rs[ps[it.idx].dl_method][k[ps[it.idx].dl_method]++].Wc = W + it.r.g.QOFF;
+    }
+  }
+  StageTimer* T = &wk->timer;
+  cudaEvent_t ev;
+  for (int m = 0; m < 2; m++) {
+    if (rs[m].empty()) continue;
+    const double* dl = nullptr;
+    {
+      std::lock_guard<std::mutex> lk(D->mu);
+      if ((rc = ensure_dl(D, 1, m, s, &dl))) return rc;  // current table (already large enough)
+    }
+    timer_begin(T, s, &ev);
+    if ((rc = launch_mixed_ragged(false, rs[m], dl, wsb + sig_end, s))) return rc;
+    timer_end(T, s, kStMixInv, ev);
+  }
+  for (const RagItem& it : items) {
+    double2* W = reinterpret_cast<double2*>(wsb + it.ws_off);
+    const Resources& r = it.r;
+    timer_begin(T, s, &ev);
+    if ((rc = launch_inv_beta(r.g, r.pP, W, s))) return rc;
+    timer_end(T, s, kStInvBeta, ev);
+    timer_begin(T, s, &ev);
+    if ((rc = launch_inv_alpha(r.g, r.pP, W, s))) return rc;
+    timer_end(T, s, kStInvAlpha, ev);
+    timer_begin(T, s, &ev);
+    if ((rc = launch_inv_gamma(r.g, r.pg, W, f_d[it.idx], s))) return rc;
+    timer_end(T, s, kStInvGamma, ev);
+  }
+  return kOk;
+}
+
+int run_forward_ragged(Device* D, Workspace* wk, const so3_parameters_t* ps, int nsig, const void* const* f_d,
+                       void* const* flmn_d, int precision, cudaStream_t s) {
+  if (nsig < 0) return fail(kInvalidParameter, "negative batch size");
+  if (precision != kPrecFp64 && precision != kPrecMixedInt8) return fail(kInvalidParameter, "unknown precision");
+  if (precision == kPrecFp64) {
+    for (int b = 0; b < nsig; b++)
+      if (int rc = run_forward(D, wk, ps[b], f_d[b], flmn_d[b], ps[b].reality != 0, s)) return rc;
+    return kOk;
+  }
+  std::vector<RagItem> items;
+  std::vector<int> fp64;
+  if (int rc = ragged_prepare(D, ps, nsig, true, s, &items, &fp64)) return rc;
+  for (int i : fp64)
+    if (int rc = run_forward(D, wk, ps[i], f_d[i], flmn_d[i], 1, s)) return rc;
+  if (items.empty()) return kOk;
+  const size_t sig_end = ragged_ws_end(items, ps);
+  std::vector<RaggedSig> rs[2];
+  for (const RagItem& it : items) {
+    RaggedSig r;
+    r.flmn = flmn_d[it.idx];
+    r.Wc = nullptr;
+    r.base = it.r.bases;
+    r.g = it.r.g;
+    r.n_mode = ps[it.idx].n_mode;
+    r.compact = ps[it.idx].storage == SO3_STORAGE_COMPACT;
+    rs[ps[it.idx].dl_method].push_back(r);
+  }
+  const size_t rag = std::max(ragged_scratch_bytes(rs[0], true), ragged_scratch_bytes(rs[1], true));
+  void* ws = nullptr;
+  if (int rc = ensure_ws(wk, sig_end + rag, &ws)) return rc;
+  char* wsb = static_cast<char*>(ws);
+  int rc;
+  StageTimer* T = &wk->timer;
+  cudaEvent_t ev;
+  int k[2] = {0, 0};
+  for (RagItem& it : items) {
+    double2* W = reinterpret_cast<double2*>(wsb + it.ws_off);
+    if ((rc = ensure_tuned(D, ps[it.idx], 0, &it.r, W, s))) return rc;
+    const Resources& r = it.r;
+    rs[ps[it.idx].dl_method][k[ps[it.idx].dl_method]++].Wc = W + r.g.QOFF;
+    timer_begin(T, s, &ev);
+    if ((rc = launch_fwd_gamma(r.g, r.pg, f_d[it.idx], W, s))) return rc;
+    timer_end(T, s, kStFwdGamma, ev);
+    timer_begin(T, s, &ev);
+    if ((rc = launch_fwd_alpha(r.g, r.pP, W, s))) return rc;
+    timer_end(T, s, kStFwdAlpha, ev);
+    timer_begin(T, s, &ev);
+    if ((rc = launch_fwd_beta_conv(r.g, r.pP, r.pc, r.wr, W, s))) return rc;
+    timer_end(T, s, kStFwdBetaConv, ev);
+  }
+  for (int m = 0; m < 2; m++) {
+    if (rs[m].empty()) continue;
+    const double* dl = nullptr;
+    {
+      std::lock_guard<std::mutex> lk(D->mu);
+      if ((rc = ensure_dl(D, 1, m, s, &dl))) return rc;
+    }
+    timer_begin(T, s, &ev);
+    if ((rc = launch_mixed_ragged(true, rs[m], dl, wsb + sig_end, s))) return rc;
+    timer_end(T, s, kStMixFwd, ev);
+  }
+  return kOk;
+}
+
 }  // namespace so3g

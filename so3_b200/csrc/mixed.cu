@@ -1166,6 +1166,423 @@ __global__ void __launch_bounds__(kThreads, 1) beta_tc_kernel(BetaArgs a, int nt
   tcp_teardown(S, warp);
 }
 
+// ---------------------------------------------------------------- ragged batches
+// Split-precision contractions of signals with different parameters (L, N,
+// L0, storage, n-order, n-mode) in one launch.  The Delta products A[m', l] =
+// Delta^l_{m' mu} Delta^l_{m' nu} do not depend on L or N, so signals of
+// different geometry share the tensor-core tiles: the host sorts the signals
+// by (recursion, L, N) and cuts them into groups of 16 (one M = 128 operand);
+// a group runs at its largest L and N, each signal's columns are zero past its
+// own L, N (and below its L0) and its outputs are written in its own layout.
+// Work items of all groups form one 1-D grid; A is generated from the FP64
+// Delta table in the producer warps (no resident digit table: the group
+// geometry changes from batch to batch).
+struct SigDesc {
+  const double2* flmn;    // inverse: coefficients in; forward: coefficients out
+  double2* Wc;            // column-major scratch part: inverse output, forward input
+  const long long* base;  // block bases of the signal's parameters
+  long long CS, QS;       // its column-major strides
+  int L, N, L0, plane0, n_mode, compact;
+};
+struct GroupDesc {
+  long long xs_off;  // byte offset of the group's stage images [pair][chunk][kXStage]
+  long long sc_off;  // offset (doubles) of its column scales [pair][kM]
+  int Lg, Ng, nc;    // largest L and N of the group, reduction chunks
+  int sig0, nsig;    // first signal (index into the descriptors) and count (<= 16)
+  int item0, slice0;  // first tensor-core item and first slicing block of the group
+};
+struct RagArgs {
+  uint8_t* xs;
+  double* xscale;
+  const SigDesc* sigs;
+  const GroupDesc* groups;
+  const double* dl;
+  int ngroups;
+};
+
+// Group of a 1-D block index (prefix offsets item0 or slice0, ascending).
+template <bool ITEMS>
+__device__ __forceinline__ int ragged_group(const RagArgs& a, int x) {
+  int g = 0;
+  while (g + 1 < a.ngroups && (ITEMS ? a.groups[g + 1].item0 : a.groups[g + 1].slice0) <= x) g++;
+  return g;
+}
+
+// Inverse slicing of a ragged group: block (slot b, nu, block of kMuPer mu),
+// the same two passes as slice_inv_kernel, columns read in the signal's own
+// layout and written into the group's stage images.
+__global__ void __launch_bounds__(256, 3) ragged_slice_inv_kernel(RagArgs a) {
+  __shared__ double wmax[8][2 * 4 * kMuPer];
+  __shared__ double scl[kMuPer][2 * 4];
+  const int gi = ragged_group<false>(a, blockIdx.x);
+  const GroupDesc G = a.groups[gi];
+  const int local = blockIdx.x - G.slice0;
+  const int b = local % kSig, rest = local / kSig;
+  const int nu = rest % G.Ng, mu0 = (rest / G.Ng) * kMuPer;
+  const int Lp = G.nc * kKC;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  SigDesc sd{};
+  const bool has = b < G.nsig;
+  if (has) sd = a.sigs[G.sig0 + b];
+  // column of slot b for (mu, nu, combo), in the signal's own layout
+  auto column = [&](int mu, int combo) {
+    InvColumn c;
+    const int ms = (combo & 1) ? -1 : 1, ns = (combo & 2) ? -1 : 1;
+    const int m = ms * mu, n = ns * nu;
+    c.act = has && mu < sd.L && nu < sd.N && !(ms < 0 && mu == 0) && !(ns < 0 && nu == 0) &&
+            !plane_skipped(sd.n_mode, sd.N, n);
+    c.lmin = max(max(mu, nu), sd.L0);
+    c.flip = ms * ns < 0;
+    c.src = c.act ? sd.flmn + sd.base[sd.plane0 + n] + m : nullptr;
+    c.gsrc = nullptr;
+    return c;
+  };
+  const int Ls = has ? sd.L : 0;
+  {
+    const int j = threadIdx.x % kMuPer, combo = (threadIdx.x / kMuPer) & 3, l0 = threadIdx.x / (4 * kMuPer);
+    constexpr int LSTEP = 256 / (4 * kMuPer);
+    const InvColumn col = column(mu0 + j, combo);
+    double mr = 0.0, mi = 0.0;
+    if (col.act) {
+      for (int l1 = l0; l1 < Ls; l1 += LSTEP * 8) {
+        double2 x[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) x[u] = inv_value(col, Ls, l1 + LSTEP * u);
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          mr = fmax(mr, fabs(x[u].x));
+          mi = fmax(mi, fabs(x[u].y));
+        }
+      }
+    }
+    mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, 16));
+    mi = fmax(mi, __shfl_xor_sync(0xffffffffu, mi, 16));
+    if (lane < 16) {
+      wmax[warp][2 * (j * 4 + combo)] = mr;
+      wmax[warp][2 * (j * 4 + combo) + 1] = mi;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 2 * 4 * kMuPer) {
+    double mx = 0.0;
+#pragma unroll
+    for (int w = 0; w < 8; w++) mx = fmax(mx, wmax[w][threadIdx.x]);
+    const int jc = threadIdx.x >> 1, part = threadIdx.x & 1;
+    scl[jc >> 2][2 * (jc & 3) + part] = scale_of(mx);
+  }
+  __syncthreads();
+  for (int j = 0; j < kMuPer; j++) {
+    const int mu = mu0 + j;
+    if (mu >= G.Lg) break;
+    const long long gp = (long long)mu * G.Ng + nu;
+    if (threadIdx.x < 8) a.xscale[G.sc_off + gp * kM + 8 * b + threadIdx.x] = scl[j][threadIdx.x];
+  }
+  for (int w = threadIdx.x; w < kMuPer * 8 * (Lp / 16); w += blockDim.x) {
+    const int c = w & 7, j = (w >> 3) % kMuPer, kb = w / (8 * kMuPer);
+    const int mu = mu0 + j;
+    if (mu >= G.Lg) continue;
+    const int combo = c >> 1, part = c & 1;
+    const double inv = 1.0 / scl[j][c];
+    const InvColumn col = column(mu, combo);
+    uint32_t d[4][kS];
+#pragma unroll
+    for (int qd = 0; qd < 4; qd++) {
+      double r[4];
+#pragma unroll
+      for (int e = 0; e < 4; e++) r[e] = inv_entry(col, Ls, 16 * kb + 4 * qd + e, part) * inv;
+      split_pack4(r, d[qd]);
+    }
+    const long long gp = (long long)mu * G.Ng + nu;
+    uint8_t* dst = a.xs + G.xs_off + gp * (long long)G.nc * kXStage + (long long)(kb >> 2) * kXStage +
+                   tile_off(kM, 8 * b + c, (kb & 3) * 16);
+#pragma unroll
+    for (int i = 0; i < kS; i++)
+      *reinterpret_cast<uint4*>(dst + i * (kM * kKC)) = make_uint4(d[0][i], d[1][i], d[2][i], d[3][i]);
+  }
+}
+
+// Forward slicing of a ragged group: block (pair, set q4 of kSigPer slots),
+// as slice_fwd_kernel, columns read from each signal's own column-major part.
+__global__ void __launch_bounds__(256) ragged_slice_fwd_kernel(RagArgs a) {
+  __shared__ double scl[2 * kSliceCols];
+  const int gi = ragged_group<false>(a, blockIdx.x);
+  const GroupDesc G = a.groups[gi];
+  const int local = blockIdx.x - G.slice0;
+  const int npairs = G.Lg * G.Ng;
+  const int pair = local % npairs, q4 = local / npairs;  // q4 < kSig / kSigPer
+  const int nu = pair % G.Ng, mu = pair / G.Ng;
+  const int Lp = G.nc * kKC;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // complex column cc (slot kSigPer q4 + cc / 4, combo cc % 4)
+  auto column = [&](int cc, int* Ls) {
+    FwdColumn c;
+    const int b = kSigPer * q4 + (cc >> 2), combo = cc & 3;
+    const int ms = (combo & 1) ? -1 : 1, ns = (combo & 2) ? -1 : 1;
+    const int m = ms * mu, n = ns * nu;
+    c.act = false;
+    c.flip = ms * ns < 0;
+    c.src = nullptr;
+    *Ls = 0;
+    if (b < G.nsig) {
+      const SigDesc& sd = a.sigs[G.sig0 + b];
+      c.act = mu < sd.L && nu < sd.N && !(ms < 0 && mu == 0) && !(ns < 0 && nu == 0) &&
+              !plane_skipped(sd.n_mode, sd.N, n);
+      if (c.act) c.src = sd.Wc + (long long)(sd.plane0 + n) * sd.QS + (long long)(m + sd.L - 1) * sd.CS;
+      *Ls = sd.L;
+    }
+    return c;
+  };
+  for (int cc = warp; cc < kSliceCols; cc += 8) {
+    int Ls;
+    const FwdColumn col = column(cc, &Ls);
+    double mr = 0.0, mi = 0.0;
+    if (col.act) {
+      for (int k1 = lane; k1 < Ls; k1 += 32 * 8) {
+        double2 x[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          const int k = k1 + 32 * u;
+          x[u] = k < Ls ? __ldg(col.src + k) : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          mr = fmax(mr, fabs(x[u].x));
+          mi = fmax(mi, fabs(x[u].y));
+        }
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, o));
+      mi = fmax(mi, __shfl_xor_sync(0xffffffffu, mi, o));
+    }
+    if (lane == 0) scl[2 * cc] = scale_of(mr), scl[2 * cc + 1] = scale_of(mi);
+  }
+  __syncthreads();
+  if (threadIdx.x < 2 * kSliceCols)
+    a.xscale[G.sc_off + (long long)pair * kM + 2 * kSliceCols * q4 + threadIdx.x] = scl[threadIdx.x];
+  uint8_t* pb = a.xs + G.xs_off + (long long)pair * G.nc * kXStage;
+  const int c_base = 2 * kSliceCols * q4, nblk = Lp / 16;
+  for (int w = threadIdx.x; w < 2 * kSliceCols * nblk; w += blockDim.x) {
+    const int c = w % (2 * kSliceCols), kb = w / (2 * kSliceCols), cc = c >> 1, part = c & 1;
+    int Ls;
+    const FwdColumn col = column(cc, &Ls);
+    const double inv = 1.0 / scl[c];
+    const double* src = reinterpret_cast<const double*>(col.src) + part;
+    uint32_t d[4][kS];
+#pragma unroll
+    for (int qd = 0; qd < 4; qd++) {
+      double r[4];
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const int k = 16 * kb + 4 * qd + e;
+        double x = (col.act && k < Ls) ? __ldg(src + 2 * k) : 0.0;
+        if (col.flip && (k & 1)) x = -x;
+        r[e] = x * inv;
+      }
+      split_pack4(r, d[qd]);
+    }
+    uint8_t* dst = pb + (long long)(kb >> 2) * kXStage + tile_off(kM, c_base + c, (kb & 3) * 16);
+#pragma unroll
+    for (int i = 0; i < kS; i++)
+      *reinterpret_cast<uint4*>(dst + i * (kM * kKC)) = make_uint4(d[0][i], d[1][i], d[2][i], d[3][i]);
+  }
+}
+
+// Tensor-core products of a ragged batch: one CTA per item (group, mu, tile,
+// nu), the producer warps generating A from Delta as mixed_tc_kernel does;
+// outputs in each signal's own layout.
+template <bool FWD>
+__global__ void __launch_bounds__(kThreads, 1) ragged_tc_kernel(RagArgs ra) {
+  extern __shared__ __align__(1024) unsigned char smraw[];
+  TcSmem& S = *reinterpret_cast<TcSmem*>(smraw);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int gi = ragged_group<true>(ra, blockIdx.x);
+  const GroupDesc G = ra.groups[gi];
+  const int MT = G.nc;
+  const int local = blockIdx.x - G.item0;
+  const int nu = local % G.Ng, rest = local / G.Ng;
+  const int t = rest % MT, mu = rest / MT;
+  const int L = G.Lg, r0 = t * kN;
+  const int lmin = max(mu, nu);  // the signals' own L0 zero their columns / outputs
+  MixArgs a{};
+  a.dl = ra.dl;
+  a.L = L;
+  a.N = G.Ng;
+  int kc0, nk;
+  if (FWD) {
+    const bool any_row = r0 + kN > lmin && r0 < L;
+    kc0 = 0;
+    nk = any_row ? (min(L, r0 + kN) + kKC - 1) / kKC : 0;
+  } else {
+    const int kstart = max(lmin, r0) & ~(kKC - 1);
+    kc0 = kstart / kKC;
+    nk = kstart < L ? (L - kstart + kKC - 1) / kKC : 0;
+  }
+  const long long gp = (long long)mu * G.Ng + nu;
+  const uint8_t* xs = ra.xs + G.xs_off + gp * (long long)G.nc * kXStage;
+  if (*reinterpret_cast<volatile int*>(&g_tc_error)) return;
+
+  const uint32_t full0 = tc::smem_u32(&S.full[0]), empty0 = tc::smem_u32(&S.empty[0]);
+  const uint32_t accum = tc::smem_u32(&S.accum);
+  if (tid == 0) {
+    for (int s = 0; s < kStages; s++) {
+      tc::mbar_init(full0 + 8 * s, kGen + 1);
+      tc::mbar_init(empty0 + 8 * s, 1);
+    }
+    tc::mbar_init(accum, 1);
+    tc::mbar_fence_init();
+  }
+  if (warp == 0) tc::tmem_alloc(tc::smem_u32(&S.tmem_base), kTmemCols);
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tbase = S.tmem_base;
+
+  if (warp == 0) {
+    if (lane == 0 && nk > 0) {
+      constexpr uint32_t idesc = tc::idesc_s8(kM, kN);
+      for (int k = 0; k < nk; k++) {
+        const int s = k & 1;
+        tc::mbar_wait(full0 + 8 * s, (k >> 1) & 1, &g_tc_error, 2);
+        tc::tc_fence_after();
+        const uint32_t xb = tc::smem_u32(&S.X[s][0]), ab = tc::smem_u32(&S.A[s][0]);
+#pragma unroll
+        for (int ks = 0; ks < kKC / 32; ks++) {
+#pragma unroll
+          for (int i = 0; i < kS; i++) {
+            const uint64_t ad = tc::smem_desc(xb + i * (kM * kKC) + ks * 2 * (kM * 16), kM * 16, 128);
+#pragma unroll
+            for (int j = 0; j + i < kND; j++) {
+              const uint64_t bd = tc::smem_desc(ab + j * (kN * kKC) + ks * 2 * (kN * 16), kN * 16, 128);
+              tc::mma_i8(tbase + (uint32_t)(kN * (i + j)), ad, bd, idesc, (k | ks | i) != 0);
+            }
+          }
+        }
+        tc::mma_commit(empty0 + 8 * s);
+      }
+      tc::mma_commit(accum);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      for (int k = 0; k < nk; k++) {
+        const int s = k & 1;
+        if (k >= kStages) tc::mbar_wait(empty0 + 8 * s, ((k >> 1) - 1) & 1, &g_tc_error, 2);
+        tc::mbar_arrive_expect_tx(full0 + 8 * s, kXStage);
+        tc::bulk_g2s(tc::smem_u32(&S.X[s][0]), xs + (long long)(kc0 + k) * kXStage, kXStage, full0 + 8 * s);
+      }
+    }
+  } else {
+    const int gw = warp - 2;
+    double xa[4][4], xb[4][4];
+    if (nk > 0) gen_load<FWD>(a, mu, nu, lmin, r0, kc0 * kKC, gw, lane, xa);
+    for (int k = 0; k < nk; k += 2) {
+      if (k + 1 < nk) gen_load<FWD>(a, mu, nu, lmin, r0, (kc0 + k + 1) * kKC, gw, lane, xb);
+      if (k >= kStages) tc::mbar_wait(empty0, ((k >> 1) - 1) & 1, &g_tc_error, 2);
+      gen_store(&S.A[0][0], gw, lane, xa);
+      tc::fence_proxy_async_smem();
+      tc::mbar_arrive(full0);
+      if (k + 1 >= nk) break;
+      if (k + 2 < nk) gen_load<FWD>(a, mu, nu, lmin, r0, (kc0 + k + 2) * kKC, gw, lane, xa);
+      if (k + 1 >= kStages) tc::mbar_wait(empty0 + 8, (((k + 1) >> 1) - 1) & 1, &g_tc_error, 2);
+      gen_store(&S.A[1][0], gw, lane, xb);
+      tc::fence_proxy_async_smem();
+      tc::mbar_arrive(full0 + 8);
+    }
+
+    // epilogue: thread <-> TMEM lane c (signal column), 32 output rows
+    const int lq = warp & 3, ch = gw >> 2;
+    const int c = 32 * lq + lane;
+    const int b = c >> 3, combo = (c >> 1) & 3, part = c & 1;
+    const int ms = (combo & 1) ? -1 : 1, ns = (combo & 2) ? -1 : 1;
+    const int m = ms * mu, n = ns * nu;
+    const bool one_neg = ms * ns < 0;
+    const double sgn_mn = ((mu + nu) & 1) ? -1.0 : 1.0;
+    const double scale = ra.xscale[G.sc_off + gp * kM + c];
+    bool live = b < G.nsig && !((ms < 0 && mu == 0) || (ns < 0 && nu == 0));
+    SigDesc sd{};
+    if (live) {
+      sd = ra.sigs[G.sig0 + b];
+      live = mu < sd.L && nu < sd.N && !(FWD && plane_skipped(sd.n_mode, sd.N, n));
+    }
+    if (nk > 0) {
+      tc::mbar_wait(accum, 0, &g_tc_error, 2);
+      tc::tc_fence_after();
+    }
+    double2* Wout = nullptr;
+    double2* F = nullptr;
+    long long blk = 0;
+    if (live) {
+      if (!FWD) {
+        Wout = sd.Wc + (long long)(sd.plane0 + n) * sd.QS + (long long)(m + sd.L - 1) * sd.CS;
+      } else {
+        F = const_cast<double2*>(sd.flmn);
+        blk = sd.base[sd.plane0 + n];
+      }
+    }
+    const int lmin_s = max(lmin, sd.L0);
+#pragma unroll 1
+    for (int g = 0; g < 4; g++) {
+      __syncwarp();
+      const int col = 32 * ch + 8 * g;
+      double v[8];
+#pragma unroll
+      for (int e = 0; e < 8; e++) v[e] = 0.0;
+      if (nk > 0) {
+        int acc[kND][8];
+#pragma unroll
+        for (int d = 0; d < kND; d++)
+          tc::tmem_ld8(tbase + ((uint32_t)(32 * lq) << 16) + (uint32_t)(kN * d + col), acc[d]);
+        tc::tmem_wait_ld();
+        double wd = 2.0 * 0.000061035156250000000;  // A scale 2, diagonal 0: 2^{-14}
+#pragma unroll
+        for (int d = 0; d < kND; d++) {
+#pragma unroll
+          for (int e = 0; e < 8; e++) v[e] = fma(int_to_double(acc[d][e]), wd, v[e]);
+          wd *= 0.0078125;
+        }
+#pragma unroll
+        for (int e = 0; e < 8; e++) v[e] *= scale;
+      }
+      double re[4], im[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const double send = part ? v[q] : v[4 + q];
+        const double recv = __shfl_xor_sync(0xffffffffu, send, 1);
+        re[q] = part ? recv : v[q];
+        im[q] = part ? v[4 + q] : recv;
+      }
+      if (!live) continue;
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int row = r0 + col + 4 * part + q;
+        if (row >= sd.L) continue;
+        const double s = (one_neg && (row & 1)) ? -sgn_mn : sgn_mn;
+        double2 val = make_double2(re[q] * s, im[q] * s);
+        if (!FWD) {
+          Wout[row] = ipow(val, n - m + 4 * sd.L);
+        } else {
+          const int lr = row;
+          if (mu > lr) continue;
+          if (sd.compact && lr < nu) continue;  // not stored
+          if (lr < lmin_s) val = make_double2(0.0, 0.0);
+          else val = ipow(val, m - n + 4 * sd.L);
+          F[blk + (long long)lr * lr + lr + m] = val;
+        }
+      }
+    }
+  }
+
+  if (warp == 0 && lane == 0 && nk > 0) tc::mbar_wait(accum, 0, &g_tc_error, 2);
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    __syncwarp();
+    tc::tc_fence_after();
+    tc::tmem_dealloc(tbase, kTmemCols);
+  }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------- host side
@@ -1434,6 +1851,108 @@ int launch_mixed_fwd_beta(const Geometry& g, double2* W, long long wstride, int 
   SO3G_CUDA(cudaFuncSetAttribute(beta_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   const int grid = (int)std::min<long long>(items, sm_count());
   beta_tc_kernel<<<grid, kThreads, smem, s>>>(a, tiles, (int)items);
+  SO3G_LAUNCHED();
+  SO3G_CUDA(cudaGetLastError());
+  return kOk;
+}
+
+// ---------------------------------------------------------------- ragged batches (host)
+namespace {
+struct RaggedPlan {
+  std::vector<SigDesc> sigs;
+  std::vector<GroupDesc> groups;
+  size_t xs_bytes = 0, sc_count = 0;
+  long long items = 0, slices = 0;
+  size_t sc_off = 0, sig_off = 0, grp_off = 0, total = 0;
+};
+
+RaggedPlan ragged_plan(const std::vector<RaggedSig>& in, bool fwd) {
+  RaggedPlan P;
+  std::vector<int> order(in.size());
+  for (size_t i = 0; i < in.size(); i++) order[i] = (int)i;
+  // similar geometries share a group: the group runs at its largest L and N
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    return in[x].g.L != in[y].g.L ? in[x].g.L > in[y].g.L : in[x].g.N > in[y].g.N;
+  });
+  for (int i : order) {
+    const RaggedSig& r = in[i];
+    SigDesc d{};
+    d.flmn = static_cast<const double2*>(r.flmn);
+    d.Wc = r.Wc;
+    d.base = r.base;
+    d.CS = r.g.CS, d.QS = r.g.QS;
+    d.L = r.g.L, d.N = r.g.N, d.L0 = r.g.L0, d.plane0 = r.g.plane0, d.n_mode = r.n_mode, d.compact = r.compact;
+    P.sigs.push_back(d);
+  }
+  for (size_t s0 = 0; s0 < P.sigs.size(); s0 += kSig) {
+    GroupDesc G{};
+    G.sig0 = (int)s0;
+    G.nsig = (int)std::min<size_t>(kSig, P.sigs.size() - s0);
+    for (int b = 0; b < G.nsig; b++) {
+      G.Lg = std::max(G.Lg, P.sigs[s0 + b].L);
+      G.Ng = std::max(G.Ng, P.sigs[s0 + b].N);
+    }
+    G.nc = (G.Lg + kKC - 1) / kKC;
+    const size_t pairs = (size_t)G.Lg * G.Ng;
+    G.xs_off = (long long)P.xs_bytes;
+    G.sc_off = (long long)P.sc_count;
+    G.item0 = (int)P.items;
+    G.slice0 = (int)P.slices;
+    P.xs_bytes += pairs * G.nc * (size_t)kXStage;
+    P.sc_count += pairs * kM;
+    P.items += (long long)pairs * G.nc;
+    P.slices += fwd ? (long long)pairs * (kSig / kSigPer) : (long long)G.Ng * ((G.Lg + kMuPer - 1) / kMuPer) * kSig;
+    P.groups.push_back(G);
+  }
+  auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+  P.sc_off = al(P.xs_bytes);
+  P.sig_off = al(P.sc_off + P.sc_count * sizeof(double));
+  P.grp_off = al(P.sig_off + P.sigs.size() * sizeof(SigDesc));
+  P.total = al(P.grp_off + P.groups.size() * sizeof(GroupDesc));
+  return P;
+}
+}  // namespace
+
+size_t ragged_scratch_bytes(const std::vector<RaggedSig>& sigs, bool fwd) {
+  return sigs.empty() ? 0 : ragged_plan(sigs, fwd).total;
+}
+
+int launch_mixed_ragged(bool fwd, const std::vector<RaggedSig>& sigs, const double* dl, void* scratch,
+                        cudaStream_t s) {
+  if (sigs.empty()) return kOk;
+  for (const auto& r : sigs)
+    if (r.g.real) return fail(kUnsupported, "split-precision contractions take complex signals");
+  const RaggedPlan P = ragged_plan(sigs, fwd);
+  if (P.items > 0x7fffffffLL || P.slices > 0x7fffffffLL)
+    return fail(kUnsupported, "split-precision ragged batch: too many work items");
+  char* base = static_cast<char*>(scratch);
+  // pageable copies: the bytes are staged by the time cudaMemcpyAsync returns
+  SO3G_CUDA(cudaMemcpyAsync(base + P.sig_off, P.sigs.data(), P.sigs.size() * sizeof(SigDesc),
+                            cudaMemcpyHostToDevice, s));
+  SO3G_CUDA(cudaMemcpyAsync(base + P.grp_off, P.groups.data(), P.groups.size() * sizeof(GroupDesc),
+                            cudaMemcpyHostToDevice, s));
+  RagArgs a{};
+  a.xs = reinterpret_cast<uint8_t*>(base);
+  a.xscale = reinterpret_cast<double*>(base + P.sc_off);
+  a.sigs = reinterpret_cast<const SigDesc*>(base + P.sig_off);
+  a.groups = reinterpret_cast<const GroupDesc*>(base + P.grp_off);
+  a.dl = dl;
+  a.ngroups = (int)P.groups.size();
+  if (fwd)
+    ragged_slice_fwd_kernel<<<(unsigned)P.slices, 256, 0, s>>>(a);
+  else
+    ragged_slice_inv_kernel<<<(unsigned)P.slices, 256, 0, s>>>(a);
+  SO3G_LAUNCHED();
+  SO3G_CUDA(cudaGetLastError());
+  if (P.items == 0) return kOk;
+  const int smem = (int)sizeof(TcSmem);
+  if (fwd) {
+    SO3G_CUDA(cudaFuncSetAttribute(ragged_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    ragged_tc_kernel<true><<<(unsigned)P.items, kThreads, smem, s>>>(a);
+  } else {
+    SO3G_CUDA(cudaFuncSetAttribute(ragged_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    ragged_tc_kernel<false><<<(unsigned)P.items, kThreads, smem, s>>>(a);
+  }
   SO3G_LAUNCHED();
   SO3G_CUDA(cudaGetLastError());
   return kOk;

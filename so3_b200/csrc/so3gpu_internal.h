@@ -247,6 +247,22 @@ int launch_mixed_inverse(const Geometry& g, int n_mode, const double2* const* fl
 int launch_mixed_forward(const Geometry& g, int n_mode, const double2* W, long long wstride, int nsig,
                          const long long* bases, const double* dl, const DigitTable* tab, double2* const* flmn_dev,
                          int storage_compact, void* scratch, cudaStream_t s);
+// One signal of a ragged split-precision batch (complex; any L, N, L0,
+// storage, n-order, n-mode; one Delta recursion per launch).
+struct RaggedSig {
+  const void* flmn;        // inverse: coefficients in; forward: coefficients out (device)
+  double2* Wc;             // column-major part of the signal's scratch (inverse out, forward in)
+  const long long* base;   // block bases of its parameters (device)
+  Geometry g;
+  int n_mode, compact;
+};
+// Scratch of a ragged contraction (stage images of the groups of 16 similar
+// signals, their column scales and the descriptor tables).
+size_t ragged_scratch_bytes(const std::vector<RaggedSig>& sigs, bool fwd);
+// Slicing and tensor-core products of every signal in two launches; dl: the
+// Delta table of the batch's recursion, covering the largest L.
+int launch_mixed_ragged(bool fwd, const std::vector<RaggedSig>& sigs, const double* dl, void* scratch,
+                        cudaStream_t s);
 // Reads and clears the flag the tensor-core kernels set when a bounded wait
 // gave up (0: none; synchronous).
 int mixed_take_error();
@@ -277,6 +293,15 @@ int run_inverse_batch(Device* D, Workspace* wk, const so3_parameters_t& p, int r
                       const void* const* flmn_d, void* const* f_d, int precision, cudaStream_t s);
 int run_forward_batch(Device* D, Workspace* wk, const so3_parameters_t& p, int real, int nsig, const void* const* f_d,
                       void* const* flmn_d, int precision, cudaStream_t s);
+// Batches of signals with one parameter set each (ps[b]; any L, N, L0,
+// sampling, storage, n-order, n-mode, recursion).  Split precision: every
+// complex signal's contraction runs in one ragged tensor-core launch per
+// Delta recursion; real signals and precision FP64 run the FP64 path per
+// signal.
+int run_inverse_ragged(Device* D, Workspace* wk, const so3_parameters_t* ps, int nsig, const void* const* flmn_d,
+                       void* const* f_d, int precision, cudaStream_t s);
+int run_forward_ragged(Device* D, Workspace* wk, const so3_parameters_t* ps, int nsig, const void* const* f_d,
+                       void* const* flmn_d, int precision, cudaStream_t s);
 // Directional convolutions of one S^2 signal flm with nsig kernels glm_d[b]
 // (so3_conv_s2toso3_harmonic_convolution with h parameters p) followed by the
 // inverse transform into f_d[b] (complex signals).  FP64: hlmn of each kernel

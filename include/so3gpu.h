@@ -138,20 +138,24 @@ int so3gpu_inverse_noalloc(void *f, const void *flmn, const so3_parameters_t *pa
  * so3_conv_s2toso3_harmonic_convolution result) requests of any parameters,
  * submitted from any host thread, run on one device with continuous
  * batching.  Up to max_inflight units run at once on separate streams;
- * queued split-precision (SO3GPU_PRECISION_MIXED_INT8) requests with
- * identical parameters and direction are admitted together, up to
- * max_batch per unit.  Each unit reserves its scratch from memory_budget
- * bytes (stream-ordered allocations) and is admitted when a slot and the
- * budget allow, first come first served; a request that alone exceeds the
- * budget completes with status 4.  max_L (> 0) builds the Wigner tables up
- * to that band limit at creation and rejects larger requests; 0 lets the
- * tables grow, which synchronises the device when it happens.  Buffers are
- * device pointers owned by the caller until the request completes.
- * submit returns the request id (>= 0) or minus a status code.  poll / wait
- * return 1 once the request is done (filling queueing and total latency in
- * microseconds, the size of the unit it ran in, and its status; the request
- * is then forgotten), poll returns 0 while it is pending, -1 for unknown ids.
- * destroy waits for every submitted request. */
+ * queued complex split-precision (SO3GPU_PRECISION_MIXED_INT8) requests of
+ * one direction are admitted together, up to max_batch per unit, whatever
+ * their parameters (companions chosen by geometry; the unit's contractions
+ * share the ragged tensor-core launch of so3gpu_inverse_ragged).  The
+ * memory_budget covers the device's resident tables, the scratch of the
+ * units in flight and the callers' buffers of those units; a unit is
+ * admitted when a slot and the budget allow, first come first served, and a
+ * request that cannot fit beside the resident tables completes with status
+ * 4.  max_L (> 0) builds the Wigner tables up to that band limit at creation
+ * and rejects larger requests; 0 lets the tables grow, which synchronises
+ * the device when it happens.  Buffers are device pointers owned by the
+ * caller until the request completes.  submit returns the request id (>= 0)
+ * or minus a status code.  poll / wait return 1 once the request is done
+ * (filling queueing and total latency in microseconds, the size of the unit
+ * it ran in, and its status; the request is then forgotten), poll returns 0
+ * while it is pending, -1 for unknown ids.  stats' peak_bytes is the largest
+ * resident + in-flight total seen.  destroy waits for every submitted
+ * request. */
 typedef struct so3gpu_server so3gpu_server;
 so3gpu_server *so3gpu_server_create(int device, size_t memory_budget, int max_inflight, int max_batch, int max_L);
 void so3gpu_server_destroy(so3gpu_server *server);

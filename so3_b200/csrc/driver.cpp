@@ -589,6 +589,19 @@ size_t ragged_ws_end(const std::vector<RagItem>& items, const so3_parameters_t* 
 
 }  // namespace
 
+size_t ragged_workspace_bytes(const so3_parameters_t* ps, int nsig, bool fwd) {
+  size_t sig = 0;
+  std::vector<RaggedSig> rs[2];
+  for (int i = 0; i < nsig; i++) {
+    if (ps[i].reality) continue;
+    sig += (workspace_bytes(ps[i], 0) + 255) & ~size_t(255);
+    RaggedSig r{};
+    r.g = make_geometry(ps[i], 0);
+    rs[ps[i].dl_method & 1].push_back(r);
+  }
+  return sig + std::max(ragged_scratch_bytes(rs[0], fwd), ragged_scratch_bytes(rs[1], fwd));
+}
+
 int run_inverse_ragged(Device* D, Workspace* wk, const so3_parameters_t* ps, int nsig, const void* const* flmn_d,
                        void* const* f_d, int precision, cudaStream_t s) {
   if (nsig < 0) return fail(kInvalidParameter, "negative batch size");

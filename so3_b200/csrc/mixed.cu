@@ -1821,7 +1821,7 @@ int ensure_beta_table(Device* D, const Geometry& g, cudaStream_t s, const BetaTa
         for (int i = 0; i < kS; i++) blk[i * (kN * kKC) + off] = q[i];
       }
   auto t = std::make_unique<BetaTable>();
-  t->L = L, t->rscale = rscale;
+  t->L = L, t->rscale = rscale, t->bytes = bytes;
   SO3G_CUDA(cudaMalloc(&t->d, bytes));
   SO3G_CUDA(cudaMemcpyAsync(t->d, host.data(), bytes, cudaMemcpyHostToDevice, s));
   SO3G_CUDA(cudaStreamSynchronize(s));  // the host image goes out of scope

@@ -6,17 +6,22 @@
 //    once, each on its own CUDA stream with its own scratch, so their kernels
 //    overlap.  A request that arrives while others run is admitted as soon as
 //    a slot and memory free up; it never waits for the running ones to end.
-//  * Memory admission: every admitted unit reserves its scratch bytes from a
-//    budget; scratch comes from the stream-ordered allocator
-//    (cudaMallocAsync / cudaFreeAsync on the slot's stream), so admitting and
-//    retiring work never synchronises the device.  A request that alone
-//    exceeds the budget fails with status 4.
-//  * Batching: queued split-precision requests with identical parameters and
-//    direction are admitted together (up to max_batch) and share one
-//    int8 contraction launch; everything else runs one request per slot.
-//    A split-precision unit of fewer than 4 signals runs on the FP64 path
-//    (the fallback: the tensor-core operands hold 16 signals, so small
-//    batches would waste most of the products and of the operand scratch).
+//  * Memory admission: the budget covers the device's resident tables (Delta,
+//    digit, beta and weight tables, plans), the scratch of the units in flight
+//    and the callers' input and output buffers of those units.  Scratch comes
+//    from the stream-ordered allocator (cudaMallocAsync / cudaFreeAsync on
+//    the slot's stream), so admitting and retiring work never synchronises
+//    the device.  A request that cannot fit beside the resident tables
+//    fails with status 4.
+//  * Batching: queued complex split-precision requests of one direction are
+//    admitted together (up to max_batch) whatever their parameters: the unit
+//    runs the ragged tensor-core contraction, where signals of different
+//    (L, N) share the operand tiles at the tiles' largest L and N (identical
+//    parameters take the uniform batch path and its resident digit tables).
+//    Companions are picked from the queue by geometry so that the padded
+//    work stays at least half useful.  A split-precision unit of fewer than 4
+//    signals runs on the FP64 path (the fallback: the tensor-core operands
+//    hold 16 signals, so small batches would waste most of the products).
 //    A result depends on its companions only through that choice: within a
 //    split-precision batch the split is per signal and the int32
 //    accumulation exact, and the FP64 path is within the split tolerance.
@@ -28,8 +33,10 @@
 //    time and wakes the worker thread, which retires the slot and admits more.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <deque>
 #include <memory>
@@ -75,11 +82,25 @@ struct Slot {
   void* owner = nullptr;
 };
 
-bool same_batch(const Req& a, const Req& b) {
+bool same_params(const Req& a, const Req& b) {
   return a.kind == b.kind && a.precision == b.precision && a.p.L == b.p.L && a.p.N == b.p.N &&
          a.p.L0 == b.p.L0 && a.p.sampling_scheme == b.p.sampling_scheme && a.p.n_order == b.p.n_order &&
          a.p.storage == b.p.storage && a.p.n_mode == b.p.n_mode && a.p.dl_method == b.p.dl_method &&
-         a.p.reality == b.p.reality;
+         a.p.reality == b.p.reality && a.p.steerable == b.p.steerable;
+}
+// Requests that may share a ragged split-precision unit.
+bool ragged_mates(const Req& a, const Req& b) {
+  return a.kind == b.kind && a.kind != 2 && a.precision == kPrecMixedInt8 && b.precision == kPrecMixedInt8 &&
+         !a.p.reality && !b.p.reality;
+}
+// Contraction work of a request, and of a tile padded to the largest L, N.
+double work_of(const so3_parameters_t& p) { return (double)p.L * p.L * p.L * p.N; }
+
+size_t buffer_bytes(const Req& r) {
+  const size_t fl = (size_t)so3_sampling_flmn_size(&r.p) * sizeof(double2);
+  const size_t f = (size_t)so3_sampling_f_size(&r.p) * (r.p.reality ? sizeof(double) : sizeof(double2));
+  if (r.kind == 2) return 2 * (size_t)r.p.L * r.p.L * sizeof(double2) + f;
+  return fl + f;
 }
 
 }  // namespace
@@ -210,13 +231,58 @@ class Server {
   static int unit_precision(const std::vector<Req*>& b) {
     return (b[0]->precision == kPrecMixedInt8 && (int)b.size() >= kMinSplitBatch) ? kPrecMixedInt8 : kPrecFp64;
   }
+  // A split-precision unit whose requests differ in parameters (ragged path).
+  static bool unit_ragged(const std::vector<Req*>& b) {
+    if (unit_precision(b) != kPrecMixedInt8) return false;
+    for (const Req* r : b)
+      if (!same_params(*r, *b[0])) return true;
+    return false;
+  }
 
   size_t unit_bytes(const std::vector<Req*>& b) const {
     const Req& r = *b[0];
     const int real = r.p.reality != 0;
-    size_t need = batch_workspace_bytes(r.p, real, (int)b.size(), unit_precision(b));
+    size_t need;
+    if (unit_ragged(b)) {
+      std::vector<so3_parameters_t> ps;
+      for (const Req* q : b) ps.push_back(q->p);
+      need = ragged_workspace_bytes(ps.data(), (int)ps.size(), r.kind == 1);
+    } else {
+      need = batch_workspace_bytes(r.p, real, (int)b.size(), unit_precision(b));
+    }
     if (r.kind == 2) need = ((need + 255) & ~size_t(255)) + (size_t)so3_sampling_flmn_size(&r.p) * sizeof(double2);
+    for (const Req* q : b) need += buffer_bytes(*q);  // the callers' buffers count against the budget
     return need;
+  }
+
+  // Companions of the oldest queued request r0 for a split-precision unit:
+  // queued requests that may share its tiles, taken in order of geometric
+  // closeness while the unit's useful work stays at least half of its padded
+  // work (sum of L^3 N over count * Lmax^3 Nmax).
+  std::vector<Req*> pick_unit() const {
+    Req* r0 = queue_.front();
+    std::vector<Req*> unit{r0};
+    if (!(r0->precision == kPrecMixedInt8 && r0->kind != 2 && !r0->p.reality)) return unit;
+    std::vector<std::pair<double, Req*>> cand;
+    const double w0 = std::log(work_of(r0->p));
+    const size_t scan = std::min<size_t>(queue_.size(), 512);
+    for (size_t i = 1; i < scan; i++)
+      if (ragged_mates(*queue_[i], *r0)) cand.push_back({std::fabs(std::log(work_of(queue_[i]->p)) - w0), queue_[i]});
+    std::stable_sort(cand.begin(), cand.end(),
+                     [](const std::pair<double, Req*>& x, const std::pair<double, Req*>& y) { return x.first < y.first; });
+    double sum = work_of(r0->p);
+    int Lm = r0->p.L, Nm = r0->p.N;
+    for (const auto& c : cand) {
+      if ((int)unit.size() >= max_batch_) break;
+      const so3_parameters_t& q = c.second->p;
+      const int L2 = std::max(Lm, q.L), N2 = std::max(Nm, q.N);
+      const double eff = (sum + work_of(q)) / ((double)(unit.size() + 1) * (double)L2 * L2 * L2 * N2);
+      if (eff < 0.5) continue;
+      unit.push_back(c.second);
+      sum += work_of(q);
+      Lm = L2, Nm = N2;
+    }
+    return unit;
   }
 
   // Enqueues the unit's work, the release of its scratch and the completion
@@ -249,13 +315,19 @@ class Server {
       } else {
         std::vector<const void*> ins(n);
         std::vector<void*> outs(n);
+        std::vector<so3_parameters_t> ps(n);
         for (int i = 0; i < n; i++) {
           ins[i] = sl->reqs[i]->in;
           outs[i] = sl->reqs[i]->out;
+          ps[i] = sl->reqs[i]->p;
         }
         const int prec = unit_precision(sl->reqs);
-        rc = r.kind == 0 ? run_inverse_batch(D_, &sl->wk, r.p, real, n, ins.data(), outs.data(), prec, sl->s)
-                         : run_forward_batch(D_, &sl->wk, r.p, real, n, ins.data(), outs.data(), prec, sl->s);
+        if (unit_ragged(sl->reqs))
+          rc = r.kind == 0 ? run_inverse_ragged(D_, &sl->wk, ps.data(), n, ins.data(), outs.data(), prec, sl->s)
+                           : run_forward_ragged(D_, &sl->wk, ps.data(), n, ins.data(), outs.data(), prec, sl->s);
+        else
+          rc = r.kind == 0 ? run_inverse_batch(D_, &sl->wk, r.p, real, n, ins.data(), outs.data(), prec, sl->s)
+                           : run_forward_batch(D_, &sl->wk, r.p, real, n, ins.data(), outs.data(), prec, sl->s);
       }
       cudaFreeAsync(ws, sl->s);
       sl->wk.ws = nullptr;
@@ -306,17 +378,15 @@ class Server {
             break;
           }
         if (!free_slot) break;
-        std::vector<Req*> unit{queue_.front()};
-        if (unit[0]->precision == kPrecMixedInt8 && unit[0]->kind != 2) {
-          for (size_t i = 1; i < queue_.size() && (int)unit.size() < max_batch_; i++)
-            if (same_batch(*queue_[i], *unit[0])) unit.push_back(queue_[i]);
-        }
+        std::vector<Req*> unit = pick_unit();
+        const size_t resident = resident_bytes(D_);
+        const size_t room = budget_ > resident ? budget_ - resident : 0;
         size_t need = unit_bytes(unit);
-        while (need > budget_ && unit.size() > 1) {  // shrink the batch to fit
+        while (need > room && unit.size() > 1) {  // shrink the batch to fit
           unit.pop_back();
           need = unit_bytes(unit);
         }
-        if (need > budget_) {  // can never run
+        if (need > room) {  // can never run beside the resident tables
           Req* r = unit[0];
           queue_.pop_front();
           r->status = fail(kOutOfMemory, "request scratch exceeds the server memory budget");
@@ -325,7 +395,7 @@ class Server {
           completed_++;
           continue;
         }
-        if (inflight_bytes_ + need > budget_) break;  // wait for memory
+        if (inflight_bytes_ + need > room) break;  // wait for memory
         for (Req* r : unit) {
           for (auto it = queue_.begin(); it != queue_.end(); ++it)
             if (*it == r) {
@@ -340,7 +410,7 @@ class Server {
         free_slot->busy = true;
         free_slot->finished.store(false);
         inflight_bytes_ += need;
-        if (inflight_bytes_ > peak_bytes_) peak_bytes_ = inflight_bytes_;
+        if (inflight_bytes_ + resident > peak_bytes_) peak_bytes_ = inflight_bytes_ + resident;
         busy_++;
         units_++;
         lk.unlock();

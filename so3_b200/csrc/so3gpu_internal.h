@@ -109,6 +109,7 @@ struct BetaTable {
   int L = 0;
   uint8_t* d = nullptr;
   double rscale = 1.0;
+  size_t bytes = 0;
 };
 
 struct Device {
@@ -167,6 +168,9 @@ int ensure_conv_kernel(Device* D, const Geometry& g, const double2** out);
 int ensure_bases(Device* D, const so3_parameters_t& p, int real, const long long** out);
 int ensure_ws(Workspace* W, size_t bytes, void** out);
 size_t workspace_bytes(const so3_parameters_t& p, int real);
+// Device bytes of the resident per-device tables (Delta tables, digit and
+// beta tables, weight tables, DFT plans, block bases).
+size_t resident_bytes(Device* D);
 
 // ---------------------------------------------------------------- launches
 int launch_build_dl_trapani(double* table, int L0cap, int Lcap, cudaStream_t s);
@@ -302,6 +306,8 @@ int run_inverse_ragged(Device* D, Workspace* wk, const so3_parameters_t* ps, int
                        void* const* f_d, int precision, cudaStream_t s);
 int run_forward_ragged(Device* D, Workspace* wk, const so3_parameters_t* ps, int nsig, const void* const* f_d,
                        void* const* flmn_d, int precision, cudaStream_t s);
+// Workspace bytes of a split-precision ragged call (complex signals).
+size_t ragged_workspace_bytes(const so3_parameters_t* ps, int nsig, bool fwd);
 // Directional convolutions of one S^2 signal flm with nsig kernels glm_d[b]
 // (so3_conv_s2toso3_harmonic_convolution with h parameters p) followed by the
 // inverse transform into f_d[b] (complex signals).  FP64: hlmn of each kernel

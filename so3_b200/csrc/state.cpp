@@ -115,6 +115,19 @@ int validate(const so3_parameters_t& p, int real) {
 }
 
 // ------------------------------------------------------------------ devices
+size_t resident_bytes(Device* D) {
+  std::lock_guard<std::mutex> lk(D->mu);
+  size_t b = 0;
+  for (const DlTable& t : D->dl)
+    if (t.d) b += (size_t)dl_plane_offset(t.Lcap) * sizeof(double);
+  for (const auto& t : D->digit_tables) b += t->bytes + (size_t)t->L * t->N * sizeof(long long);
+  for (const auto& t : D->beta_tables) b += t->bytes;
+  for (const auto& kv : D->conv_kernels) b += (size_t)(8 * (kv.first / 2) + 2 * (kv.first / 2)) * sizeof(double2);  // Pc <= 8L, plus 2L
+  for (const auto& kv : D->ffts) b += (size_t)4 * (kv.first + 256) * sizeof(double2);
+  for (const auto& kv : D->bases) b += 4096 * sizeof(long long);
+  return b;
+}
+
 static std::mutex g_dev_mu;
 static std::map<int, std::unique_ptr<Device>> g_devs;
 

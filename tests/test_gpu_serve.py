@@ -82,7 +82,9 @@ def test_budget_rejects_oversized_request_and_serves_the_rest():
     import torch
     small = {"t": 0.0, "kind": "inverse", "L": 16, "N": 4, "seed": 1, "precision": "fp64"}
     big = {"t": 0.0, "kind": "inverse", "L": 128, "N": 32, "seed": 2, "precision": "fp64"}
-    with serve.Server(0, memory_budget=8 << 20, max_inflight=2, max_batch=1, max_L=128) as sv:
+    # 24 MiB: the resident Delta tables to L=128 (11.3 MB for both recursions) plus room for
+    # the small request's scratch and buffers, not for the big one's (about 70 MB)
+    with serve.Server(0, memory_budget=24 << 20, max_inflight=2, max_batch=1, max_L=128) as sv:
         pb, ab, _, ob = serve.request_buffers(big)
         ps, as_, _, os_ = serve.request_buffers(small)
         torch.cuda.synchronize()
@@ -102,3 +104,20 @@ def test_latency_fields():
     assert s["requests"] == 20 and s["failed"] == 0
     assert 0 < s["p50_ms"] <= s["p99_ms"]
     assert all(0 <= r.queue_us <= r.total_us for r in res)
+
+
+def test_split_requests_of_different_geometries_batch():
+    """Split-precision requests of different (L, N) form ragged units (one
+    tensor-core launch); each result matches its FP64 transform."""
+    import torch
+    trace = serve.make_trace(40, rate=1e5, seed=21, L_range=(24, 40), N_max=6, p_inverse=1.0, precision="mixed")
+    with serve.Server(0, memory_budget=8 << 30, max_inflight=2, max_batch=16, max_L=64) as sv:
+        res, wall, outs = serve.replay(sv, trace, keep_outputs=True)
+    assert all(r.status == 0 for r in res)
+    assert max(r.batch for r in res) >= 4
+    ctx = so3.Context(0)
+    for req, out in zip(trace, outs):
+        p, a, b, _ = serve.request_buffers(req)
+        ref = ctx.inverse(a, p)
+        torch.cuda.synchronize()
+        assert rel_err(out.cpu().numpy(), ref.cpu().numpy()) <= TOL_MIXED

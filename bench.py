@@ -49,9 +49,13 @@ def args_():
     ap.add_argument("--N", type=int, default=64)
     ap.add_argument("--batch", type=int, default=16,
                     help="signals per split-precision step (0: time the FP64 path only)")
-    ap.add_argument("--serve", type=int, default=400,
+    ap.add_argument("--serve", type=int, default=1500,
                     help="requests of the serving-trace sample (0: skip the serving leg)")
-    ap.add_argument("--serve-rate", type=float, default=60.0, help="offered request rate of the serving leg (1/s)")
+    ap.add_argument("--serve-rates", default="60,1000",
+                    help="offered request rates of the serving leg (1/s, comma separated)")
+    ap.add_argument("--serve-sweep", default="",
+                    help="run only the serving sweep of the request trace: 20,000 requests at each of these offered "
+                         "rates (comma separated), FP64 and split precision; prints one JSON line")
     ap.add_argument("--profile-region", action="store_true",
                     help="bracket the split-precision leg's timed steps (the FP64 leg's with --batch 0) "
                          "with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
@@ -375,8 +379,35 @@ def pct(lat, q):
     return s[min(len(s) - 1, max(0, math.ceil(q * len(s)) - 1))]
 
 
+def run_serve_sweep(a):
+    """Config C5 at its stated size: 20,000 seeded requests (60 % inverse /
+    40 % forward complex MW, L log-uniform in [16, 1024], N uniform in
+    [1, min(L, 64)], U(-1,1) inputs, Poisson arrivals) at each offered rate,
+    FP64 and split precision, 120 GB admission budget: throughput, p50 / p99
+    latency, mean unit size."""
+    import torch
+
+    from so3_b200 import serve as sserve
+    torch.cuda.set_device(0)
+    rates = [float(x) for x in a.serve_sweep.split(",") if x]
+    rows = []
+    for rate in rates:
+        row = {"offered_rate_rps": rate}
+        for prec in ("fp64", "mixed"):
+            row[prec] = sserve.serving_run(20000, rate, seed=11, precision=prec, device=0, max_batch=16)
+        rows.append(row)
+        print(json.dumps({"partial": row}), file=sys.stderr, flush=True)
+    print(json.dumps({"serving_sweep": rows, "requests_per_rate": 20000,
+                      "trace": "60% inverse / 40% forward, complex MW, L log-uniform [16, 1024], "
+                               "N uniform [1, min(L, 64)], U(-1,1), Poisson, 120 GB budget, 8 slots, units <= 16"}),
+          flush=True)
+
+
 def run_ours(a):
     import torch
+    if a.serve_sweep:
+        run_serve_sweep(a)
+        return
 
     import so3_b200 as so3
     from so3_b200 import dist as sdist
@@ -541,11 +572,17 @@ def run_ours(a):
         ctx.close()  # the batch workspace
         del d_flmn, d_f
         torch.cuda.empty_cache()
-        serving = {"trace": f"{a.serve} requests, seed {rank + 11}, Poisson {a.serve_rate:g}/s offered, "
+        rates = [float(x) for x in a.serve_rates.split(",") if x]
+        serving = {"trace": f"{a.serve} requests per rate, seed {rank + 11}, Poisson arrivals at each offered rate, "
                             f"L log-uniform [16, 1024], N uniform [1, min(L, 64)], 60% inverse / 40% forward, "
-                            f"complex MW, 120 GB budget, 8 slots, batches of up to 8"}
-        for prec in ("fp64", "mixed"):
-            serving[prec] = sserve.serving_run(a.serve, a.serve_rate, seed=rank + 11, precision=prec, device=local)
+                            f"complex MW, 120 GB budget (resident tables and buffers included), 8 slots, "
+                            f"units of up to 16 (split precision across geometries)", "by_rate": []}
+        for rate in rates:
+            row = {"offered_rate_rps": rate}
+            for prec in ("fp64", "mixed"):
+                row[prec] = sserve.serving_run(a.serve, rate, seed=rank + 11, precision=prec, device=local,
+                                               max_batch=16)
+            serving["by_rate"].append(row)
         # recurring geometries offered as a burst: split-precision requests batch (up to 8 per launch)
         shapes = [(512, 16), (256, 32), (128, 64)]
         serving["recurring"] = {"trace": f"256 requests, (L, N) uniform over {shapes}, 60% inverse / 40% forward, "

@@ -6,4 +6,5 @@
 #include "so3_sampling.h"
 #include "so3_core.h"
 #include "so3_conv.h"
+#include "so3_adjoint.h"
 #endif

@@ -111,7 +111,8 @@ def ref():
         for name in ("so3_core_inverse_via_ssht", "so3_core_forward_via_ssht",
                      "so3_core_inverse_via_ssht_real", "so3_core_forward_via_ssht_real",
                      "so3_core_inverse_direct", "so3_core_forward_direct",
-                     "so3_core_inverse_direct_real", "so3_core_forward_direct_real"):
+                     "so3_core_inverse_direct_real", "so3_core_forward_direct_real",
+                     "so3_adjoint_inverse_direct", "so3_adjoint_forward_direct"):
             getattr(R, name).argtypes = [_VP, _VP, _P]
             getattr(R, name).restype = None
         R.so3_conv_harmonic_convolution.argtypes = [_VP, _P, _VP, _P, _VP, _P]
@@ -179,6 +180,24 @@ def ref_forward(f, p, direct=False):
         f = np.ascontiguousarray(f, dtype=np.complex128)
         getattr(R, f"so3_core_forward_{kind}")(_ptr(flmn), _ptr(f), ctypes.byref(p))
     return flmn
+
+
+def ref_adjoint_inverse(f, p):
+    """The reference's so3_adjoint_inverse_direct (src/c/so3_adjoint.c:34)."""
+    R = ref()
+    flmn = np.zeros(R.so3_sampling_flmn_size(ctypes.byref(p)), np.complex128)
+    f = np.ascontiguousarray(f, dtype=np.complex128)
+    R.so3_adjoint_inverse_direct(_ptr(flmn), _ptr(f), ctypes.byref(p))
+    return flmn
+
+
+def ref_adjoint_forward(flmn, p):
+    """The reference's so3_adjoint_forward_direct (src/c/so3_adjoint.c:402)."""
+    R = ref()
+    f = np.zeros(f_size(p), np.complex128)
+    flmn = np.ascontiguousarray(flmn, dtype=np.complex128)
+    R.so3_adjoint_forward_direct(_ptr(f), _ptr(flmn), ctypes.byref(p))
+    return f
 
 
 def harmonic_convolution(flmn, fp: Params, glmn, gp: Params):

@@ -47,6 +47,8 @@ SIGNATURES = {
     "so3_core_inverse_direct_real": (None, [_VP, _VP, _P]),
     "so3_core_forward_direct": (None, [_VP, _VP, _P]),
     "so3_core_forward_direct_real": (None, [_VP, _VP, _P]),
+    "so3_adjoint_inverse_direct": (None, [_VP, _VP, _P]),
+    "so3_adjoint_forward_direct": (None, [_VP, _VP, _P]),
     "so3_conv_convolution": (None, [_VP, _P, _VP, _P, _VP, _P]),
     "so3_conv_harmonic_convolution": (None, [_VP, _P, _VP, _P, _VP, _P]),
     "so3_conv_get_parameters_of_convolved_lmn": (Params, [_P, _P]),

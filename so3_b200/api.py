@@ -198,6 +198,28 @@ def forward(f: np.ndarray, p) -> np.ndarray:
     return flmn
 
 
+def adjoint_inverse(f: np.ndarray, p) -> np.ndarray:
+    """Adjoint of the inverse transform (so3_adjoint_inverse_direct,
+    reference src/c/so3_adjoint.c:34): samples -> coefficients, complex MW."""
+    q = _checked(p)
+    flmn = np.zeros(flmn_size(q), np.complex128)
+    f = np.ascontiguousarray(f, dtype=np.complex128)
+    _lib.load().so3_adjoint_inverse_direct(_ptr(flmn), _ptr(f), ctypes.byref(q))
+    _lib.check("adjoint_inverse")
+    return flmn
+
+
+def adjoint_forward(flmn: np.ndarray, p) -> np.ndarray:
+    """Adjoint of the forward transform (so3_adjoint_forward_direct,
+    reference src/c/so3_adjoint.c:402): coefficients -> samples, complex MW."""
+    q = _checked(p)
+    f = np.zeros(f_size(q), np.complex128)
+    flmn = np.ascontiguousarray(flmn, dtype=np.complex128)
+    _lib.load().so3_adjoint_forward_direct(_ptr(f), _ptr(flmn), ctypes.byref(q))
+    _lib.check("adjoint_forward")
+    return f
+
+
 def get_convolved_parameters(fp, gp) -> SO3Parameters:
     h = Params()
     _lib.load().so3_conv_get_parameters_of_convolved_lmn_void(ctypes.byref(h), ctypes.byref(_s(fp)),

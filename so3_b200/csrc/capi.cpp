@@ -16,6 +16,7 @@
 #include <cstdlib>
 #include <cstring>
 
+#include "so3/so3_adjoint.h"
 #include "so3/so3_conv.h"
 #include "so3/so3_core.h"
 #include "so3/so3_sampling.h"
@@ -197,6 +198,29 @@ int dropin_forward(void* flmn, const void* f, const so3_parameters_t* p, int rea
   return drain(X, so3g::run_forward_staged(so3g::device_state(dev), &X->wk, *p, real, zero_first, io, X->stream));
 }
 
+// Adjoint transforms on host or device buffers (whole arrays staged; the
+// adjoint inverse writes every coefficient, the adjoint forward every sample).
+int dropin_adjoint(void* out, const void* in, const so3_parameters_t* p, bool inverse) {
+  if (!p) return so3g::fail(so3g::kInvalidParameter, "null parameters");
+  int dev;
+  if (int rc = current_device(&dev)) return rc;
+  DropIn* X = dropin(dev);
+  std::lock_guard<std::mutex> lk(X->mu);
+  const size_t fb = f_bytes(p, 0), lb = flmn_bytes(p, 0);
+  void *din = nullptr, *dout = nullptr;
+  bool sin = false, sout = false;
+  if (int rc = device_view(X, 0, in, inverse ? fb : lb, true, &din, &sin)) return rc;
+  if (int rc = device_view(X, 1, out, inverse ? lb : fb, false, &dout, &sout)) return rc;
+  Device* D = so3g::device_state(dev);
+  const int rc = inverse ? so3g::run_adjoint_inverse(D, &X->wk, *p, din, dout, X->stream)
+                         : so3g::run_adjoint_forward(D, &X->wk, *p, din, dout, X->stream);
+  if (rc) {
+    cudaStreamSynchronize(X->stream);
+    return rc;
+  }
+  return download(X, out, dout, inverse ? lb : fb, sout);
+}
+
 int require_mw(const so3_parameters_t* p) {
   if (p && p->sampling_scheme != SO3_SAMPLING_MW)
     return so3g::fail(so3g::kUnsupported, "the direct transforms support MW sampling only");
@@ -244,6 +268,14 @@ void so3_core_forward_direct(cd* flmn, const cd* f, const so3_parameters_t* p) {
 void so3_core_forward_direct_real(cd* flmn, const double* f, const so3_parameters_t* p) {
   int rc = require_mw(p);
   finish(rc ? rc : dropin_forward(flmn, f, p, 1, true));
+}
+
+// ------------------------------------------------------------ drop-in adjoint
+void so3_adjoint_inverse_direct(cd* flmn, const cd* f, const so3_parameters_t* p) {
+  finish(dropin_adjoint(flmn, f, p, true));
+}
+void so3_adjoint_forward_direct(cd* f, const cd* flmn, const so3_parameters_t* p) {
+  finish(dropin_adjoint(f, flmn, p, false));
 }
 
 // ------------------------------------------------------------ drop-in conv

@@ -116,6 +116,7 @@ struct InvArgs {
   int L, N, L0, plane0, n_mode, real, sym_n0;
   int nu_lo, nu_hi;  // |n| range [nu_lo, nu_hi) of this launch
   long long CS, QS;  // column-major scratch strides
+  double wconst;     // > 0: this weight for every l instead of (2l+1)/(8 pi^2) (adjoint forward)
 };
 
 // ------------------------------------------------------------------ inverse
@@ -193,7 +194,7 @@ __global__ void __launch_bounds__(kThreads, 1) inverse_contract_kernel(InvArgs a
 #pragma unroll
       for (int lc = 0; lc < kChunk; lc++) {
         const int l = lbase + lc;
-        const double cl = (2.0 * l + 1.0) * kInv8Pi2;
+        const double cl = a.wconst > 0.0 ? a.wconst : (2.0 * l + 1.0) * kInv8Pi2;
         if (a.sym_n0)
           mac_chunk<NSIGN, true>(S, lc, warp, lm, lu, cl, l & 1, mu_own, acc);
         else
@@ -230,10 +231,12 @@ __global__ void __launch_bounds__(kThreads, 1) inverse_contract_kernel(InvArgs a
 }
 
 int launch_inverse_contract(const Geometry& g, int n_mode, const double2* flmn, const long long* bases,
-                            const double* dl, double2* W, int sym_n0, cudaStream_t s, int nu_lo, int nu_hi) {
+                            const double* dl, double2* W, int sym_n0, cudaStream_t s, int nu_lo, int nu_hi,
+                            double wconst) {
   if (nu_hi < 0 || nu_hi > g.N) nu_hi = g.N;
   if (nu_lo >= nu_hi) return kOk;
-  InvArgs a{flmn, bases, dl, W + g.QOFF, g.L, g.N, g.L0, g.plane0, n_mode, g.real, sym_n0, nu_lo, nu_hi, g.CS, g.QS};
+  InvArgs a{flmn, bases, dl, W + g.QOFF, g.L, g.N, g.L0, g.plane0, n_mode, g.real, sym_n0, nu_lo, nu_hi, g.CS, g.QS,
+            wconst};
   dim3 grid((nu_hi - nu_lo + kNG - 1) / kNG, (g.L + kRows - 1) / kRows, (g.L + kCols - 1) / kCols);
   if (g.real) {
     SO3G_CUDA(cudaFuncSetAttribute(inverse_contract_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));
@@ -256,6 +259,7 @@ struct FwdArgs {
   int L, N, L0, plane0, n_mode, real, compact;
   int nu_lo, nu_hi;  // |n| range [nu_lo, nu_hi) of this launch
   long long CS, QS;  // column-major scratch strides
+  double lw;         // > 0: outputs times lw (2l+1) (adjoint inverse)
 };
 
 template <int NSIGN>
@@ -353,6 +357,7 @@ __global__ void __launch_bounds__(kThreads, 1) forward_contract_kernel(FwdArgs a
           v = acc[i][j][s];
           if (ms * ns < 0) v = sc(v, odd_l);
           v = ipow_mul(v, m - n + 4 * L);
+          if (a.lw > 0.0) v = sc(v, a.lw * (2.0 * l + 1.0));
         }
         a.flmn[a.base[a.plane0 + n] + (long long)l * l + l + m] = v;
       }
@@ -362,11 +367,11 @@ __global__ void __launch_bounds__(kThreads, 1) forward_contract_kernel(FwdArgs a
 
 int launch_forward_contract(const Geometry& g, int n_mode, const double2* W, const long long* bases,
                             const double* dl, double2* flmn, int storage_compact, cudaStream_t s, int nu_lo,
-                            int nu_hi) {
+                            int nu_hi, double lw) {
   if (nu_hi < 0 || nu_hi > g.N) nu_hi = g.N;
   if (nu_lo >= nu_hi) return kOk;
   FwdArgs a{W + g.QOFF, bases, dl, flmn, g.L, g.N, g.L0, g.plane0, n_mode, g.real, storage_compact, nu_lo, nu_hi,
-            g.CS, g.QS};
+            g.CS, g.QS, lw};
   dim3 grid((nu_hi - nu_lo + kNG - 1) / kNG, (g.L + kRows - 1) / kRows, (g.L + kCols - 1) / kCols);
   if (g.real) {
     SO3G_CUDA(cudaFuncSetAttribute(forward_contract_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));

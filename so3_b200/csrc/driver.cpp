@@ -735,4 +735,60 @@ int run_forward_ragged(Device* D, Workspace* wk, const so3_parameters_t* ps, int
   return kOk;
 }
 
+// ------------------------------------------------------------ adjoint transforms
+// Adjoints of the inverse and forward transforms (reference
+// src/c/so3_adjoint.c:34-400, :402-938; complex MW).  The reference's FFT
+// normalisations are folded into one contraction weight: the adjoint
+// inverse's analysis DFTs over gamma and alpha carry 2 pi/(2N-1) and
+// 1/(2L-1) (the forward stages'), undone in the forward contraction's
+// (2l+1)/(8 pi^2) weight; the adjoint forward's 1/((2L-1)(2N-1)) rides on the
+// inverse contraction.
+static int adjoint_check(const so3_parameters_t& p) {
+  if (int rc = validate(p, 0)) return rc;
+  if (p.reality) return fail(kUnsupported, "adjoint transforms: complex signals only on the GPU path");
+  if (p.sampling_scheme != SO3_SAMPLING_MW) return fail(kUnsupported, "adjoint transforms: MW sampling only");
+  if (p.steerable) return fail(kUnsupported, "adjoint transforms: steerable signals are not supported");
+  return kOk;
+}
+
+int run_adjoint_inverse(Device* D, Workspace* wk, const so3_parameters_t& p, const void* f_d, void* flmn_d,
+                        cudaStream_t s) {
+  if (int rc = adjoint_check(p)) return rc;
+  Resources r;
+  if (int rc = acquire(D, p, 0, s, &r, false)) return rc;
+  void* ws = nullptr;
+  if (int rc = ensure_ws(wk, workspace_bytes(p, 0), &ws)) return rc;
+  double2* W = static_cast<double2*>(ws);
+  if (int rc = ensure_tuned(D, p, 0, &r, W, s)) return rc;
+  // every coefficient starts at zero (so3_adjoint.c:234-243): skipped n-blocks and l < L0 stay zero
+  SO3G_CUDA(cudaMemsetAsync(flmn_d, 0, (size_t)so3_sampling_flmn_size(&p) * sizeof(double2), s));
+  int rc;
+  if ((rc = launch_fwd_gamma(r.g, r.pg, f_d, W, s))) return rc;
+  if ((rc = launch_fwd_alpha(r.g, r.pP, W, s))) return rc;
+  if ((rc = launch_adj_inv_beta(r.g, r.pP, W, s))) return rc;
+  const double kPi = 3.141592653589793238462643383279502884;
+  const double lw = (double)(2 * p.N - 1) * (2 * p.L - 1) / (16.0 * kPi * kPi * kPi);  // (2l+1)/(8pi^2) (2N-1)(2L-1)/(2pi)
+  return launch_forward_contract(r.g, p.n_mode, W, r.bases, r.dl, static_cast<double2*>(flmn_d),
+                                 p.storage == SO3_STORAGE_COMPACT, s, 0, -1, lw);
+}
+
+int run_adjoint_forward(Device* D, Workspace* wk, const so3_parameters_t& p, const void* flmn_d, void* f_d,
+                        cudaStream_t s) {
+  if (int rc = adjoint_check(p)) return rc;
+  Resources r;
+  if (int rc = acquire(D, p, 0, s, &r, true)) return rc;
+  void* ws = nullptr;
+  if (int rc = ensure_ws(wk, workspace_bytes(p, 0), &ws)) return rc;
+  double2* W = static_cast<double2*>(ws);
+  if (int rc = ensure_tuned(D, p, 0, &r, W, s)) return rc;
+  int rc;
+  const double wconst = 1.0 / ((double)(2 * p.L - 1) * (2 * p.N - 1));
+  if ((rc = launch_inverse_contract(r.g, p.n_mode, static_cast<const double2*>(flmn_d), r.bases, r.dl, W, 0, s, 0,
+                                    -1, wconst)))
+    return rc;
+  if ((rc = launch_adj_fwd_beta(r.g, r.pP, r.pc, r.wr, W, s))) return rc;
+  if ((rc = launch_inv_alpha(r.g, r.pP, W, s))) return rc;
+  return launch_inv_gamma(r.g, r.pg, W, f_d, s);
+}
+
 }  // namespace so3g

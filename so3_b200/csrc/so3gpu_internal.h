@@ -189,12 +189,15 @@ __host__ __device__ inline bool plane_skipped(int mode, int N, int n) {
 
 // nu_lo/nu_hi restrict a launch to the planes with |n| in [nu_lo, nu_hi)
 // (nu_hi < 0: up to N); ranges split at even |n| so CTAs never straddle.
+// wconst > 0 replaces the inverse's per-degree weight (2l+1)/(8 pi^2) by a
+// constant; lw > 0 multiplies the forward's outputs by lw (2l+1) (the
+// adjoint transforms).
 int launch_inverse_contract(const Geometry& g, int n_mode, const double2* flmn, const long long* bases,
                             const double* dl, double2* W, int sym_n0, cudaStream_t s, int nu_lo = 0,
-                            int nu_hi = -1);
+                            int nu_hi = -1, double wconst = 0.0);
 int launch_forward_contract(const Geometry& g, int n_mode, const double2* W, const long long* bases,
                             const double* dl, double2* flmn, int storage_compact, cudaStream_t s, int nu_lo = 0,
-                            int nu_hi = -1);
+                            int nu_hi = -1, double lw = 0.0);
 
 int launch_inv_beta(const Geometry& g, const FftPlan& pP, double2* W, cudaStream_t s);
 int launch_inv_alpha(const Geometry& g, const FftPlan& pP, double2* W, cudaStream_t s);
@@ -208,6 +211,17 @@ int launch_fwd_alpha(const Geometry& g, const FftPlan& pP, double2* W, cudaStrea
 int launch_fwd_beta_conv(const Geometry& g, const FftPlan& pP, const FftPlan& pc, const double2* wr,
                          double2* W, cudaStream_t s);
 
+// Beta stages of the adjoint transforms (MW, complex; stages.cu).  Inverse
+// adjoint: per column of the row-major part, zero-extend the nb beta samples
+// onto the 2L-1 circle, DFT, phase e^{-i m' pi/(2L-1)}, fold F(m') +
+// (-1)^{m+n} F(-m') onto m' >= 0 into the column-major part.  Forward
+// adjoint: per column of the column-major part, extend G(-m') = (-1)^{m+n}
+// G(m'), convolve with 4 pi^2 w (table wr), phase e^{+i m'' pi/(2L-1)},
+// inverse DFT / (2L-1), fold the periodic extension back onto the L beta
+// samples into the row-major part.
+int launch_adj_inv_beta(const Geometry& g, const FftPlan& pP, double2* W, cudaStream_t s);
+int launch_adj_fwd_beta(const Geometry& g, const FftPlan& pP, const FftPlan& pc, const double2* wr, double2* W,
+                        cudaStream_t s);
 int launch_s2toso3(const so3_parameters_t& hp, const long long* bases, const double2* flm, const double2* glm,
                    double2* hlmn, cudaStream_t s);
 int launch_harmonic_convolution(const so3_parameters_t& hp, const so3_parameters_t& fp,
@@ -306,6 +320,12 @@ int run_inverse_ragged(Device* D, Workspace* wk, const so3_parameters_t* ps, int
                        void* const* f_d, int precision, cudaStream_t s);
 int run_forward_ragged(Device* D, Workspace* wk, const so3_parameters_t* ps, int nsig, const void* const* f_d,
                        void* const* flmn_d, int precision, cudaStream_t s);
+// Adjoint transforms (complex MW): flmn <- A_inverse^H f and f <- A_forward^H
+// flmn, device pointers, on stream s.
+int run_adjoint_inverse(Device* D, Workspace* wk, const so3_parameters_t& p, const void* f_d, void* flmn_d,
+                        cudaStream_t s);
+int run_adjoint_forward(Device* D, Workspace* wk, const so3_parameters_t& p, const void* flmn_d, void* f_d,
+                        cudaStream_t s);
 // Workspace bytes of a split-precision ragged call (complex signals).
 size_t ragged_workspace_bytes(const so3_parameters_t* ps, int nsig, bool fwd);
 // Directional convolutions of one S^2 signal flm with nsig kernels glm_d[b]

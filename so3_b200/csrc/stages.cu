@@ -602,6 +602,108 @@ __global__ void __launch_bounds__(E::NT, E::MINB) fwd_beta_conv_kernel(Geometry 
   }
 }
 
+// ------------------------------------------------------------------ adjoint
+// Beta stages of the adjoint transforms (reference src/c/so3_adjoint.c,
+// complex MW).  Generic engines only (any length); one column (plane n,
+// order m, s = (-1)^{m+n}) per sequence.
+//
+// Inverse adjoint (so3_adjoint.c:190-231): the nb beta samples zero-extended
+// onto the 2L-1 circle, forward DFT, phase e^{-i m' pi/(2L-1)}, folded
+// F(m') + s F(-m') onto m' >= 0 (the contraction's sum over -l <= m' <= l).
+template <class E>
+__global__ void __launch_bounds__(E::NT, E::MINB) adj_inv_beta_kernel(Geometry g, FftPlan P, double2* __restrict__ W,
+                                                                 int T_, int ld_) {
+  static_assert(!E::fixed, "generic engines");
+  extern __shared__ double2 sm[];
+  const int T = T_, ld = ld_;
+  double2* a = sm;
+  double2* b = sm + (size_t)T * ld;
+  const int plane = blockIdx.y, n = plane - g.plane0;
+  const int c0 = blockIdx.x * T, L = g.L, ncols = 2 * L - 1, Pn = g.P;
+  const double2* base = W + (long long)plane * g.PS;
+  for (int idx = threadIdx.x; idx < Pn * T; idx += E::NT) {
+    const int t = idx % T, row = idx / T, c = c0 + t;  // columns fastest: rows read contiguously
+    a[t * ld + row] = (row < g.nb && c < ncols) ? base[(long long)row * g.RS + c] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  const double2* r = E::runP(a, b, T, ld, P);
+  double2* cbase = W + g.QOFF + (long long)plane * g.QS;
+  for (int idx = threadIdx.x; idx < L * T; idx += E::NT) {
+    const int mp = idx % L, t = idx / L, c = c0 + t;
+    if (c >= ncols) continue;
+    const int m = c - (L - 1);
+    const double sg = ((m + n) & 1) ? -1.0 : 1.0;
+    const double2 e = __ldg(P.half + mp);  // e^{-i pi m'/(2L-1)}
+    double2 v = cmul(r[t * ld + mp], e);
+    if (mp > 0) v = cadd(v, cscale(cmul(r[t * ld + Pn - mp], cconj(e)), sg));
+    cbase[(long long)c * g.CS + mp] = v;
+  }
+}
+
+// Forward adjoint (so3_adjoint.c:718-896): G(-m') = s G(m') extended from
+// the contraction's m' >= 0, convolved with the quadrature weights (F(m'') =
+// 4 pi^2 sum_{m'} G(m') w(m'' - m'), through the Pc-point product with the
+// table's full-weight spectrum), phase e^{+i m'' pi/(2L-1)}, inverse DFT over
+// the 2L-1 circle divided by 2L-1, and the adjoint of the periodic
+// extension: out(b) = y(b) + s y(2L-2-b) for b < L-1, out(L-1) = y(L-1).
+template <class E>
+__global__ void __launch_bounds__(E::NT, E::MINB) adj_fwd_beta_kernel(Geometry g, FftPlan P, FftPlan Pc,
+                                                                 const double2* __restrict__ wr,
+                                                                 double2* __restrict__ W, int T_, int ld_) {
+  static_assert(!E::fixed, "generic engines");
+  extern __shared__ double2 sm[];
+  const int T = T_, ld = ld_;
+  double2* a = sm;
+  double2* b = sm + (size_t)T * ld;
+  const int plane = blockIdx.y, n = plane - g.plane0;
+  const int c0 = blockIdx.x * T, L = g.L, ncols = 2 * L - 1, Pn = g.P, pc = g.Pc;
+  const double2* cbase = W + g.QOFF + (long long)plane * g.QS;
+  for (int idx = threadIdx.x; idx < pc * T; idx += E::NT) {
+    const int k = idx % pc, t = idx / pc, c = c0 + t;  // m' fastest: columns read contiguously
+    double2 v = make_double2(0.0, 0.0);
+    if (c < ncols) {
+      const int m = c - (L - 1);
+      const double sg = ((m + n) & 1) ? -1.0 : 1.0;
+      if (k < L) v = cbase[(long long)c * g.CS + k];
+      else if (k > pc - L) v = cscale(cbase[(long long)c * g.CS + (pc - k)], sg);
+    }
+    a[t * ld + k] = v;
+  }
+  __syncthreads();
+  double2* y = E::runC(a, b, T, ld, Pc);  // forward DFT
+  const double2* wf = wr + 2 * (size_t)L + pc;
+  for (int idx = threadIdx.x; idx < pc * T; idx += E::NT) {
+    const int k = idx % pc, t = idx / pc;
+    y[t * ld + k] = cconj(cmul(y[t * ld + k], __ldg(wf + k)));
+  }
+  __syncthreads();
+  double2* o = (y == a) ? b : a;
+  double2* cv = E::runC(y, o, T, ld, Pc);  // conj: 4 pi^2 (G * w)
+  double2* d = (cv == a) ? b : a;
+  for (int idx = threadIdx.x; idx < Pn * T; idx += E::NT) {
+    const int k = idx % Pn, t = idx / Pn;
+    const int mpp = k <= L - 1 ? k : k - Pn;  // m'' in [-(L-1), L-1]
+    const double2 F = cconj(cv[t * ld + (mpp < 0 ? mpp + pc : mpp)]);
+    const double2 e = __ldg(P.half + (mpp < 0 ? -mpp : mpp));  // e^{-i pi |m''|/(2L-1)}
+    const double2 ph = mpp < 0 ? e : cconj(e);                   // e^{+i pi m''/(2L-1)}
+    d[t * ld + k] = cconj(cmul(F, ph));
+  }
+  __syncthreads();
+  double2* other = (d == a) ? b : a;
+  const double2* yb = E::runP(d, other, T, ld, P);  // conj: (2L-1) y(b)
+  const double invP = 1.0 / Pn;
+  double2* base = W + (long long)plane * g.PS;
+  for (int idx = threadIdx.x; idx < g.nb * T; idx += E::NT) {
+    const int t = idx % T, row = idx / T, c = c0 + t;  // columns fastest: rows written contiguously
+    if (c >= ncols) continue;
+    const int m = c - (L - 1);
+    const double sg = ((m + n) & 1) ? -1.0 : 1.0;
+    double2 v = cscale(cconj(yb[t * ld + row]), invP);
+    if (row < L - 1) v = cadd(v, cscale(cconj(yb[t * ld + (Pn - 1 - row)]), sg * invP));
+    base[(long long)row * g.RS + c] = v;
+  }
+}
+
 // ------------------------------------------------------------------ launchers
 namespace {
 
@@ -845,6 +947,41 @@ int launch_fwd_beta_conv(const Geometry& g, const FftPlan& p, const FftPlan& pc,
     rc = fwd_beta_conv<Gen<true>>(g, p, pc, wr, W, s);
   else
     rc = fwd_beta_conv<Gen<false>>(g, p, pc, wr, W, s);
+  return rc ? rc : launched();
+}
+
+namespace {
+template <class E>
+int adj_inv_beta(const Geometry& g, const FftPlan& p, double2* W, cudaStream_t s) {
+  const Sizing z = sizing<E>(p.ld(), 16);
+  dim3 grid((2 * g.L - 1 + z.T - 1) / z.T, g.nplanes);
+  if (int rc = set_smem(adj_inv_beta_kernel<E>, z.smem)) return rc;
+  adj_inv_beta_kernel<E><<<grid, E::NT, z.smem, s>>>(g, p, W, z.T, p.ld());
+  return kOk;
+}
+template <class E>
+int adj_fwd_beta(const Geometry& g, const FftPlan& p, const FftPlan& pc, const double2* wr, double2* W,
+                 cudaStream_t s) {
+  const int ld = p.ld() > pc.ld() ? p.ld() : pc.ld();
+  const Sizing z = sizing<E>(ld, 8);
+  dim3 grid((2 * g.L - 1 + z.T - 1) / z.T, g.nplanes);
+  if (int rc = set_smem(adj_fwd_beta_kernel<E>, z.smem)) return rc;
+  adj_fwd_beta_kernel<E><<<grid, E::NT, z.smem, s>>>(g, p, pc, wr, W, z.T, ld);
+  return kOk;
+}
+}  // namespace
+
+int launch_adj_inv_beta(const Geometry& g, const FftPlan& p, double2* W, cudaStream_t s) {
+  if (!g.mw || g.real) return fail(kUnsupported, "adjoint transforms: complex MW sampling only");
+  const int rc = p.big() ? adj_inv_beta<Gen<true>>(g, p, W, s) : adj_inv_beta<Gen<false>>(g, p, W, s);
+  return rc ? rc : launched();
+}
+
+int launch_adj_fwd_beta(const Geometry& g, const FftPlan& p, const FftPlan& pc, const double2* wr, double2* W,
+                        cudaStream_t s) {
+  if (!g.mw || g.real) return fail(kUnsupported, "adjoint transforms: complex MW sampling only");
+  const int rc = (p.big() || pc.big()) ? adj_fwd_beta<Gen<true>>(g, p, pc, wr, W, s)
+                                       : adj_fwd_beta<Gen<false>>(g, p, pc, wr, W, s);
   return rc ? rc : launched();
 }
 

@@ -122,7 +122,7 @@ size_t resident_bytes(Device* D) {
     if (t.d) b += (size_t)dl_plane_offset(t.Lcap) * sizeof(double);
   for (const auto& t : D->digit_tables) b += t->bytes + (size_t)t->L * t->N * sizeof(long long);
   for (const auto& t : D->beta_tables) b += t->bytes;
-  for (const auto& kv : D->conv_kernels) b += (size_t)(8 * (kv.first / 2) + 2 * (kv.first / 2)) * sizeof(double2);  // Pc <= 8L, plus 2L
+  for (const auto& kv : D->conv_kernels) b += (size_t)(16 * (kv.first / 2) + 2 * (kv.first / 2)) * sizeof(double2);  // 2 Pc <= 16L, plus 2L
   for (const auto& kv : D->ffts) b += (size_t)4 * (kv.first + 256) * sizeof(double2);
   for (const auto& kv : D->bases) b += 4096 * sizeof(long long);
   return b;
@@ -405,7 +405,9 @@ int ensure_fft(Device* D, int n, FftPlan* out) {
 //                 a unit sample at its first self-mirror beta row (MW: row
 //                 L-1 at beta = pi; MWSS: row 0 at beta = 0), with the full
 //                 weights w (so3_sampling.c:32-51);
-//  [Pc + L, Pc + 2L) h_1(m'): the same for MWSS row L (beta = pi); zero for MW.
+//  [Pc + L, Pc + 2L) h_1(m'): the same for MWSS row L (beta = pi); zero for MW;
+//  [Pc + 2L, 2 Pc + 2L) 4 pi^2 / Pc * DFT(w) of the full weights (the
+//                 convolution of the adjoint forward transform).
 // h(m') = G(m') - G(-m') (m' >= 1), G(0), with G = 2 pi v * w and v(m'') =
 // e^{-i m'' beta} / P, m'' in [-(L-1), L-1].
 int ensure_conv_kernel(Device* D, const Geometry& g, const double2** out) {
@@ -426,7 +428,16 @@ int ensure_conv_kernel(Device* D, const Geometry& g, const double2** out) {
   std::vector<cld> w(Pc, cld(0, 0));
   for (int p = -2 * (L - 1); p <= 2 * (L - 1); p += 2) w[((p % Pc) + Pc) % Pc] += weight(p);
   fft_ld(w, +1);
-  std::vector<double2> host((size_t)Pc + 2 * (size_t)L, make_double2(0.0, 0.0));
+  std::vector<double2> host(2 * (size_t)Pc + 2 * (size_t)L, make_double2(0.0, 0.0));
+  {
+    std::vector<cld> wf(Pc, cld(0, 0));
+    for (int p = -2 * (L - 1); p <= 2 * (L - 1); p++) wf[((p % Pc) + Pc) % Pc] += weight(p);
+    fft_ld(wf, -1);  // forward DFT
+    for (int r = 0; r < Pc; r++) {
+      const cld v = wf[r] * (4.0L * kPiL * kPiL / (long double)Pc);
+      host[(size_t)Pc + 2 * (size_t)L + r] = make_double2((double)v.real(), (double)v.imag());
+    }
+  }
   for (int r = 0; r < Pc; r++) {
     // w_e is real and even: its spectrum is real
     const long double v = w[r].real() * (2.0L * kPiL / (long double)Pc);

@@ -163,3 +163,24 @@ def test_harmonic_convolution_oracle_matches_reference(O):
                                             f.ctypes.data_as(ctypes.c_void_p), ctypes.byref(op),
                                             g.ctypes.data_as(ctypes.c_void_p), ctypes.byref(op))
             assert np.abs(h - hr).max() < 1e-12
+
+
+def test_reference_adjoints_are_adjoint_to_its_direct_transforms(O):
+    """Pins the reference's adjoint build (src/c/so3_adjoint.c) against its own
+    direct transforms: <y, A x> = <A^H y, x> for the inverse and forward."""
+    import numpy as np
+    from so3_b200 import synth
+    from tests.helpers import oparams, params
+    if O.ref() is None:
+        import pytest
+        pytest.skip("reference C (oracle/_ref) not built")
+    for p in (params(8, 4), params(6, 6, mode=2, L0=2), params(7, 3, storage=1, order=0, method=1)):
+        op = oparams(O, p)
+        rng = np.random.default_rng(1)
+        x = synth.gen_flmn(p, 3)
+        y = rng.normal(size=O.f_size(op)) + 1j * rng.normal(size=O.f_size(op))
+        a = np.vdot(y, O.ref_inverse(x, op, direct=True))
+        assert abs(a - np.vdot(O.ref_adjoint_inverse(y, op), x)) / abs(a) < 1e-13
+        z = synth.gen_flmn(p, 5)
+        b = np.vdot(z, O.ref_forward(y, op, direct=True))
+        assert abs(b - np.vdot(O.ref_adjoint_forward(z, op), y)) / abs(b) < 1e-13

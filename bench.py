@@ -427,6 +427,8 @@ def run_ours(a):
     from so3_b200 import peaks
     fp64_peak = peaks.fp64_tflops(local)
     int8_peak = peaks.int8_mma_tops(local)
+    probes = {"fp64_fma_tflops": fp64_peak, "fp64_dmma_tflops": peaks.dmma_tflops(local),
+              "int8_tcgen05_tops": int8_peak, "hbm_copy_gbs": peaks.hbm_copy_gbs(local)}
 
     # ---- plain FP64 path, one signal per step
     fl_host = synth.gen_flmn(p, sdist.signal_seed(1000, rank, 0), "uniform")
@@ -632,6 +634,7 @@ def run_ours(a):
                 "latency_ms": {"p50": statistics.median(lat), "p99": pct(lat, 0.99)},
                 "stage_ms_per_transform": {k: round(v, 4) for k, v in per_signal.items()},
                 "gpu_launches": int(run["launches"]), "roofline": roof, "stage_hbm": hbm_stages,
+                "probes": probes,
                 "c3": c3, "c4": c4, "e2e": e2e, "cpu_baseline": cpu,
                 "serving": serving,
                 "clocks": run["clocks"]}

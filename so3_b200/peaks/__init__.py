@@ -17,7 +17,8 @@ def _load():
         if not os.path.exists(LIB_PATH):
             raise OSError(f"{LIB_PATH} missing: run python -m so3_b200.build")
         L = ctypes.CDLL(LIB_PATH)
-        for name in ("so3peaks_fp64_tflops", "so3peaks_int8_mma_tops", "so3peaks_hbm_copy_gbs"):
+        for name in ("so3peaks_fp64_tflops", "so3peaks_int8_mma_tops", "so3peaks_hbm_copy_gbs",
+                     "so3peaks_dmma_tflops"):
             getattr(L, name).restype = ctypes.c_double
             getattr(L, name).argtypes = [ctypes.c_int]
         _lib = L
@@ -43,3 +44,8 @@ def int8_mma_tops(device: int = 0) -> float:
 def hbm_copy_gbs(device: int = 0) -> float:
     """Measured device-to-device copy bandwidth (GB/s, read + write)."""
     return _checked(_load().so3peaks_hbm_copy_gbs(device), "HBM copy probe")
+
+
+def dmma_tflops(device: int = 0) -> float:
+    """Measured FP64 tensor-core (mma.sync m8n8k4 f64) throughput (TFLOP/s)."""
+    return _checked(_load().so3peaks_dmma_tflops(device), "FP64 tensor-core probe")

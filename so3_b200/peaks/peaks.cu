@@ -139,6 +139,55 @@ double fp64_tflops() {
   return flops / (best * 1e-3) / 1e12;
 }
 
+// FP64 tensor-core throughput: each warp runs 8 independent chains of
+// mma.sync.aligned.m8n8k4 f64 (8 x 8 x 4 = 256 multiply-adds per instruction).
+__global__ void dmma_chain(double* out, int iters) {
+  double a = 1.0 + 1e-9 * threadIdx.x, b = 0.999999;
+  double c[8][2];
+#pragma unroll
+  for (int i = 0; i < 8; i++) c[i][0] = c[i][1] = 1e-3 * i;
+  for (int it = 0; it < iters; it++) {
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+      asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                   : "+d"(c[i][0]), "+d"(c[i][1])
+                   : "d"(a), "d"(b));
+  }
+  double s = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) s += c[i][0] + c[i][1];
+  if (s == 12345.678) out[0] = s;  // keeps the chains live
+}
+
+double dmma_tflops() {
+  int dev = 0, sms = 0;
+  PK_CUDA(cudaGetDevice(&dev));
+  PK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  double* out = nullptr;
+  PK_CUDA(cudaMalloc(&out, sizeof(double)));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int blocks = sms * 4, threads = 256, iters = 2048;
+  dmma_chain<<<blocks, threads>>>(out, iters);  // warm-up
+  float best = 1e30f;
+  for (int r = 0; r < 5; r++) {
+    cudaEventRecord(e0);
+    dmma_chain<<<blocks, threads>>>(out, iters);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best) best = ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  PK_CUDA(cudaGetLastError());
+  const double flops = 2.0 * 256.0 * 8.0 * iters * (double)blocks * (threads / 32);
+  return flops / (best * 1e-3) / 1e12;
+}
+
 // Device-to-device copy of 4 GiB (read + write counted), best of 5.
 double hbm_copy_gbs() {
   const size_t bytes = size_t(4) << 30;
@@ -183,6 +232,10 @@ extern "C" double so3peaks_fp64_tflops(int device) {
 extern "C" double so3peaks_int8_mma_tops(int device) {
   if (cudaSetDevice(device) != cudaSuccess) return -1.0;
   return int8_mma_tops();
+}
+extern "C" double so3peaks_dmma_tflops(int device) {
+  if (cudaSetDevice(device) != cudaSuccess) return -1.0;
+  return dmma_tflops();
 }
 extern "C" double so3peaks_hbm_copy_gbs(int device) {
   if (cudaSetDevice(device) != cudaSuccess) return -1.0;

@@ -25,6 +25,8 @@
 //    (1 wavefront each), for 72 FP64 instructions per lane.
 //  * Grid order |n|-pair fastest, then rows, then |m|: CTAs resident at the
 //    same time share one Delta tile column and one coefficient slice in L2.
+#include <cstdlib>
+
 #include "so3gpu_internal.h"
 
 namespace so3g {
@@ -107,6 +109,13 @@ __device__ __forceinline__ void mac_chunk(const Slab& S, int lc, int warp, int l
   }
 }
 }  // namespace
+
+// FP64 contraction engine: the FP64 tensor cores (mma.sync f64) when the
+// environment sets SO3GPU_FP64_MMA=1, else the FP64 FMA kernels.
+static bool fp64_tensor_cores() {
+  const char* e = getenv("SO3GPU_FP64_MMA");
+  return e && e[0] == '1';
+}
 
 struct InvArgs {
   const double2* flmn;
@@ -230,6 +239,168 @@ __global__ void __launch_bounds__(kThreads, 1) inverse_contract_kernel(InvArgs a
   }
 }
 
+// ------------------------------------------------------------------ inverse, FP64 tensor cores
+// The same contraction as inverse_contract_kernel on the FP64 tensor cores
+// (mma.sync.aligned.m8n8k4 f64): for a pair (mu, nu) = (|m|, |n|) it is the
+// product Y[m', c] = sum_l W[m', l] X[l, c] with W[m', l] = Delta^l_{m' mu}
+// Delta^l_{m' nu} and one column c = 2 s + part per sign combination s
+// (bit 0: m = -mu, bit 1: n = -nu) and real / imaginary part; X carries
+// (2l+1)/(8 pi^2), and (-1)^l on combinations with one negative index (the
+// output carries the (-1)^{m'} of those).  One MMA: 8 rows m' x 8 columns x
+// 4 reduction steps l (256 multiply-adds).  CTA tile: 32 m' x 16 mu x 2 nu;
+// warp w: rows 8 (w & 3) .. +7, mu block 8 (w >> 2) .. +7, both nu: 16 MMAs
+// (32 accumulators per lane) per 4-step chunk.  Delta tiles staged with
+// cp.async (double buffered); X built from the coefficients with the weights
+// applied while staging (its loads are issued one chunk ahead).
+namespace {
+constexpr int kDT = 256;       // threads
+constexpr int kDR = 32;        // m' per CTA
+constexpr int kDM = 16;        // mu per CTA
+constexpr int kDN = 2;         // nu per CTA
+constexpr int kDK = 4;         // l per chunk (MMA K)
+constexpr int kBP = 17;        // Bm pitch (doubles): lanes (g, q) hit distinct bank pairs
+constexpr int kAP = 3;         // An pitch
+struct DSlab {
+  double Bm[kDR][kDK][kBP];           // Delta^l_{m', mu0 + j}
+  double An[kDR][kDK][kAP];           // Delta^l_{m', nu0 + j}
+  double X[kDM][kDN][8][kDK];         // [mu][nu][c][l], weighted and sign-folded
+};
+
+__device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(c[0]), "+d"(c[1])
+               : "d"(a), "d"(b));
+}
+}  // namespace
+
+template <int NSIGN>
+__global__ void __launch_bounds__(kDT, 2) inverse_contract_dmma_kernel(InvArgs a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  DSlab* st = reinterpret_cast<DSlab*>(smraw);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, q = lane & 3;
+  const int nu0 = a.nu_lo + blockIdx.x * kDN, mp0 = blockIdx.y * kDR, mu0 = blockIdx.z * kDM;
+  const int L = a.L;
+  bool act[kDN];
+#pragma unroll
+  for (int j = 0; j < kDN; j++) act[j] = (nu0 + j < a.nu_hi) && !plane_skipped(a.n_mode, a.N, nu0 + j);
+  const int mb = warp & 3, jm0 = 8 * (warp >> 2);  // rows 8 mb .., mu block jm0 ..
+  double acc[8][kDN][2];
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+#pragma unroll
+    for (int j = 0; j < kDN; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+  // reduction range, aligned to the chunk: l in [l_lo, L), l_lo = 4 floor(max(...)/4)
+  const int lstart = max(max(a.L0, nu0), max(mp0, mu0));
+  const int l_lo = lstart & ~(kDK - 1);
+  const int nchunk = l_lo < L ? (L - l_lo + kDK - 1) / kDK : 0;
+  long long bsel[kDN][2];
+#pragma unroll
+  for (int j = 0; j < kDN; j++) {
+    const int nu = min(nu0 + j, a.N - 1);
+    bsel[j][0] = a.base[a.plane0 + nu];
+    bsel[j][1] = NSIGN == 4 ? a.base[a.plane0 - nu] : 0;
+  }
+
+  auto stage_delta = [&](int c, DSlab& S) {
+    const int lb = l_lo + c * kDK;
+    for (int idx = tid; idx < kDR * kDK * kDM; idx += kDT) {  // mu fastest: a row segment of a plane
+      const int j = idx % kDM, rest = idx / kDM, lc = rest % kDK, r = rest / kDK;
+      const int l = lb + lc, mp = mp0 + r, mu = mu0 + j;
+      const bool ok = l < L && l >= lstart && mp <= l && mu <= l;
+      const double* src = ok ? a.dl + dl_plane_offset(l) + (long long)mp * (l + 1) + mu : a.dl;
+      cp_async8(&S.Bm[r][lc][j], src, ok);
+    }
+    for (int idx = tid; idx < kDR * kDK * kDN; idx += kDT) {
+      const int j = idx % kDN, rest = idx / kDN, lc = rest % kDK, r = rest / kDK;
+      const int l = lb + lc, mp = mp0 + r, nu = nu0 + j;
+      const bool ok = l < L && l >= lstart && act[j] && mp <= l && nu <= l;
+      const double* src = ok ? a.dl + dl_plane_offset(l) + (long long)mp * (l + 1) + nu : a.dl;
+      cp_async8(&S.An[r][lc][j], src, ok);
+    }
+  };
+  // coefficient loads of a chunk: 4 l x 16 mu x 2 nu x NSIGN complex values, 2 per thread
+  constexpr int kXN = kDK * kDM * kDN * 4;  // 512 (NSIGN 4) slots, 2 per thread
+  double2 xv[2];
+  auto load_x = [&](int c) {
+    const int lb = l_lo + c * kDK;
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const int idx = tid + u * kDT;  // sg fastest, then nu, mu, l
+      const int sg = idx & 3, j = (idx >> 2) & 1, jm = (idx >> 3) & 15, lc = idx >> 7;
+      const int l = lb + lc, mu = mu0 + jm, nu = nu0 + j;
+      const bool ok = sg < NSIGN && l < L && l >= lstart && act[j] && mu <= l && nu <= l &&
+                      !((sg & 1) && mu == 0) && !((sg & 2) && nu == 0);
+      const int m = (sg & 1) ? -mu : mu;
+      xv[u] = ok ? __ldg(a.flmn + bsel[j][sg >> 1] + (long long)l * l + l + m) : make_double2(0.0, 0.0);
+    }
+  };
+  auto store_x = [&](int c, DSlab& S) {
+    const int lb = l_lo + c * kDK;
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const int idx = tid + u * kDT;
+      const int sg = idx & 3, j = (idx >> 2) & 1, jm = (idx >> 3) & 15, lc = idx >> 7;
+      const int l = lb + lc;
+      double w = (2.0 * l + 1.0) * kInv8Pi2;
+      if ((sg == 1 || sg == 2) && (l & 1)) w = -w;  // one negative index: (-1)^l here
+      S.X[jm][j][2 * sg][lc] = xv[u].x * w;
+      S.X[jm][j][2 * sg + 1][lc] = xv[u].y * w;
+    }
+  };
+  static_assert(kXN == 2 * kDT, "two coefficient slots per thread");
+
+  if (nchunk > 0) {
+    stage_delta(0, st[0]);
+    cp_commit();
+    load_x(0);
+    for (int c = 0; c < nchunk; c++) {
+      DSlab& S = st[c & 1];
+      store_x(c, S);
+      if (c + 1 < nchunk) {
+        stage_delta(c + 1, st[(c + 1) & 1]);
+        cp_commit();
+        load_x(c + 1);
+        cp_wait<1>();
+      } else {
+        cp_wait<0>();
+      }
+      __syncthreads();
+      // fragments: A (W) row g = m' 8 mb + g, column q = l; B (X) row q = l, column g = c
+      const double an0 = S.An[8 * mb + g][q][0], an1 = S.An[8 * mb + g][q][1];
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        const double bm = S.Bm[8 * mb + g][q][jm0 + i];
+        dmma(acc[i][0], bm * an0, S.X[jm0 + i][0][g][q]);
+        dmma(acc[i][1], bm * an1, S.X[jm0 + i][1][g][q]);
+      }
+      __syncthreads();
+    }
+  }
+
+  // accumulator (row g, columns 2q, 2q+1) = sign combination q, real / imaginary part
+  const int mp = mp0 + 8 * mb + g;
+  const int s = q;
+  if (mp >= L || s >= NSIGN) return;
+  const int ms = (s & 1) ? -1 : 1, ns = (s & 2) ? -1 : 1;
+  const double odd_mp = (mp & 1) ? -1.0 : 1.0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const int mu = mu0 + jm0 + i;
+    if (mu >= L || (ms < 0 && mu == 0)) continue;
+#pragma unroll
+    for (int j = 0; j < kDN; j++) {
+      const int nu = nu0 + j;
+      if (nu >= a.nu_hi || (ns < 0 && nu == 0)) continue;
+      const int m = ms * mu, n = ns * nu;
+      double2 v = make_double2(acc[i][j][0], acc[i][j][1]);
+      if (ms * ns < 0) v = sc(v, odd_mp);
+      v = ipow_mul(v, n - m + 4 * L);
+      a.W[(long long)(a.plane0 + n) * a.QS + (long long)(m + L - 1) * a.CS + mp] = v;
+    }
+  }
+}
+
 int launch_inverse_contract(const Geometry& g, int n_mode, const double2* flmn, const long long* bases,
                             const double* dl, double2* W, int sym_n0, cudaStream_t s, int nu_lo, int nu_hi,
                             double wconst) {
@@ -237,6 +408,15 @@ int launch_inverse_contract(const Geometry& g, int n_mode, const double2* flmn, 
   if (nu_lo >= nu_hi) return kOk;
   InvArgs a{flmn, bases, dl, W + g.QOFF, g.L, g.N, g.L0, g.plane0, n_mode, g.real, sym_n0, nu_lo, nu_hi, g.CS, g.QS,
             wconst};
+  if (!g.real && !sym_n0 && fp64_tensor_cores()) {
+    dim3 gd((nu_hi - nu_lo + kDN - 1) / kDN, (g.L + kDR - 1) / kDR, (g.L + kDM - 1) / kDM);
+    const int smem = (int)(2 * sizeof(DSlab));
+    SO3G_CUDA(cudaFuncSetAttribute(inverse_contract_dmma_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    inverse_contract_dmma_kernel<4><<<gd, kDT, smem, s>>>(a);
+    SO3G_LAUNCHED();
+    SO3G_CUDA(cudaGetLastError());
+    return kOk;
+  }
   dim3 grid((nu_hi - nu_lo + kNG - 1) / kNG, (g.L + kRows - 1) / kRows, (g.L + kCols - 1) / kCols);
   if (g.real) {
     SO3G_CUDA(cudaFuncSetAttribute(inverse_contract_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));

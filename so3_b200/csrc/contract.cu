@@ -545,6 +545,132 @@ __global__ void __launch_bounds__(kThreads, 1) forward_contract_kernel(FwdArgs a
   }
 }
 
+// ------------------------------------------------------------------ forward, FP64 tensor cores
+// The forward contraction on the FP64 tensor cores: for a pair (mu, nu),
+// Y[l, c] = sum_{m'} W[l, m'] X[m', c] with W[l, m'] = Delta^l_{m' mu}
+// Delta^l_{m' nu} (m' <= l) and X the spectra G(n, m, m') of the column-major
+// scratch, (-1)^{m'} folded in for combinations with one negative index (the
+// output carries their (-1)^l).  CTA tile 32 l x 16 mu x 2 nu, warps and
+// staging as in inverse_contract_dmma_kernel.
+template <int NSIGN>
+__global__ void __launch_bounds__(kDT, 2) forward_contract_dmma_kernel(FwdArgs a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  DSlab* st = reinterpret_cast<DSlab*>(smraw);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, q = lane & 3;
+  const int nu0 = a.nu_lo + blockIdx.x * kDN, l0 = blockIdx.y * kDR, mu0 = blockIdx.z * kDM;
+  const int L = a.L;
+  bool act[kDN];
+#pragma unroll
+  for (int j = 0; j < kDN; j++) act[j] = (nu0 + j < a.nu_hi) && !plane_skipped(a.n_mode, a.N, nu0 + j);
+  if (!act[0] && !act[1]) return;  // caller-zeroed blocks stay untouched
+  const int mb = warp & 3, jm0 = 8 * (warp >> 2);
+  double acc[8][kDN][2];
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+#pragma unroll
+    for (int j = 0; j < kDN; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+  const int ltop = min(L - 1, l0 + kDR - 1);
+  const bool any = ltop >= max(max(a.L0, nu0), mu0);
+  const int nchunk = any ? (ltop + 1 + kDK - 1) / kDK : 0;  // m' = 0 .. ltop
+
+  auto stage_delta = [&](int c, DSlab& S) {
+    const int mb0 = c * kDK;
+    for (int idx = tid; idx < kDR * kDK * kDM; idx += kDT) {
+      const int j = idx % kDM, rest = idx / kDM, mc = rest % kDK, r = rest / kDK;
+      const int mp = mb0 + mc, l = l0 + r, mu = mu0 + j;
+      const bool ok = l < L && mp <= l && mu <= l;
+      const double* src = ok ? a.dl + dl_plane_offset(l) + (long long)mp * (l + 1) + mu : a.dl;
+      cp_async8(&S.Bm[r][mc][j], src, ok);
+    }
+    for (int idx = tid; idx < kDR * kDK * kDN; idx += kDT) {
+      const int j = idx % kDN, rest = idx / kDN, mc = rest % kDK, r = rest / kDK;
+      const int mp = mb0 + mc, l = l0 + r, nu = nu0 + j;
+      const bool ok = l < L && act[j] && mp <= l && nu <= l;
+      const double* src = ok ? a.dl + dl_plane_offset(l) + (long long)mp * (l + 1) + nu : a.dl;
+      cp_async8(&S.An[r][mc][j], src, ok);
+    }
+  };
+  double2 xv[2];
+  auto load_x = [&](int c) {
+    const int mb0 = c * kDK;
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const int idx = tid + u * kDT;  // m' fastest (contiguous in a column), then sign, nu, mu
+      const int mc = idx & 3, sg = (idx >> 2) & 3, j = (idx >> 4) & 1, jm = idx >> 5;
+      const int mp = mb0 + mc, mu = mu0 + jm, nu = nu0 + j;
+      const bool ok = sg < NSIGN && mp < L && act[j] && mu < L && !((sg & 1) && mu == 0) && !((sg & 2) && nu == 0);
+      const int n = (sg & 2) ? -nu : nu, m = (sg & 1) ? -mu : mu;
+      xv[u] = ok ? __ldg(a.W + (long long)(a.plane0 + n) * a.QS + (long long)(L - 1 + m) * a.CS + mp)
+                 : make_double2(0.0, 0.0);
+    }
+  };
+  auto store_x = [&](int c, DSlab& S) {
+    const int mb0 = c * kDK;
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const int idx = tid + u * kDT;
+      const int mc = idx & 3, sg = (idx >> 2) & 3, j = (idx >> 4) & 1, jm = idx >> 5;
+      const double w = ((sg == 1 || sg == 2) && ((mb0 + mc) & 1)) ? -1.0 : 1.0;  // (-1)^{m'}
+      S.X[jm][j][2 * sg][mc] = xv[u].x * w;
+      S.X[jm][j][2 * sg + 1][mc] = xv[u].y * w;
+    }
+  };
+
+  if (nchunk > 0) {
+    stage_delta(0, st[0]);
+    cp_commit();
+    load_x(0);
+    for (int c = 0; c < nchunk; c++) {
+      DSlab& S = st[c & 1];
+      store_x(c, S);
+      if (c + 1 < nchunk) {
+        stage_delta(c + 1, st[(c + 1) & 1]);
+        cp_commit();
+        load_x(c + 1);
+        cp_wait<1>();
+      } else {
+        cp_wait<0>();
+      }
+      __syncthreads();
+      const double an0 = S.An[8 * mb + g][q][0], an1 = S.An[8 * mb + g][q][1];
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        const double bm = S.Bm[8 * mb + g][q][jm0 + i];
+        dmma(acc[i][0], bm * an0, S.X[jm0 + i][0][g][q]);
+        dmma(acc[i][1], bm * an1, S.X[jm0 + i][1][g][q]);
+      }
+      __syncthreads();
+    }
+  }
+
+  const int l = l0 + 8 * mb + g;
+  const int s = q;
+  if (l >= L || s >= NSIGN) return;
+  const int ms = (s & 1) ? -1 : 1, ns = (s & 2) ? -1 : 1;
+  const double odd_l = (l & 1) ? -1.0 : 1.0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const int mu = mu0 + jm0 + i;
+    if (mu >= L || mu > l || (ms < 0 && mu == 0)) continue;
+#pragma unroll
+    for (int j = 0; j < kDN; j++) {
+      const int nu = nu0 + j;
+      if (!act[j] || (ns < 0 && nu == 0)) continue;
+      if (a.compact && l < nu) continue;  // not stored
+      const int m = ms * mu, n = ns * nu;
+      double2 v = make_double2(0.0, 0.0);
+      if (l >= max(a.L0, nu)) {
+        v = make_double2(acc[i][j][0], acc[i][j][1]);
+        if (ms * ns < 0) v = sc(v, odd_l);
+        v = ipow_mul(v, m - n + 4 * L);
+        if (a.lw > 0.0) v = sc(v, a.lw * (2.0 * l + 1.0));
+      }
+      a.flmn[a.base[a.plane0 + n] + (long long)l * l + l + m] = v;
+    }
+  }
+}
+
 int launch_forward_contract(const Geometry& g, int n_mode, const double2* W, const long long* bases,
                             const double* dl, double2* flmn, int storage_compact, cudaStream_t s, int nu_lo,
                             int nu_hi, double lw) {
@@ -552,6 +678,15 @@ int launch_forward_contract(const Geometry& g, int n_mode, const double2* W, con
   if (nu_lo >= nu_hi) return kOk;
   FwdArgs a{W + g.QOFF, bases, dl, flmn, g.L, g.N, g.L0, g.plane0, n_mode, g.real, storage_compact, nu_lo, nu_hi,
             g.CS, g.QS, lw};
+  if (!g.real && fp64_tensor_cores()) {
+    dim3 gd((nu_hi - nu_lo + kDN - 1) / kDN, (g.L + kDR - 1) / kDR, (g.L + kDM - 1) / kDM);
+    const int smem = (int)(2 * sizeof(DSlab));
+    SO3G_CUDA(cudaFuncSetAttribute(forward_contract_dmma_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    forward_contract_dmma_kernel<4><<<gd, kDT, smem, s>>>(a);
+    SO3G_LAUNCHED();
+    SO3G_CUDA(cudaGetLastError());
+    return kOk;
+  }
   dim3 grid((nu_hi - nu_lo + kNG - 1) / kNG, (g.L + kRows - 1) / kRows, (g.L + kCols - 1) / kCols);
   if (g.real) {
     SO3G_CUDA(cudaFuncSetAttribute(forward_contract_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));

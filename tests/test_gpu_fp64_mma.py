@@ -26,12 +26,20 @@ def test_fp64_mma_inverse_against_oracle_and_fma(O, monkeypatch, kw):
     f_mma = so3.inverse(fl, p)
     assert rel_err(f_mma, f_fma) < 1e-13
     assert rel_err(f_mma, O.inverse(fl, oparams(O, p))) < 1e-12
-    back = so3.forward(f_mma, p)
-    assert rel_err(back, fl) < 1e-11
+    f_ref = O.inverse(fl, oparams(O, p))
+    monkeypatch.setenv("SO3GPU_FP64_MMA", "0")
+    b_fma = so3.forward(f_ref, p)
+    monkeypatch.setenv("SO3GPU_FP64_MMA", "1")
+    b_mma = so3.forward(f_ref, p)
+    assert rel_err(b_mma, b_fma) < 1e-13
+    assert rel_err(b_mma, O.forward(f_ref, oparams(O, p))) < 1e-12
+    assert rel_err(so3.forward(f_mma, p), fl) < 1e-11
 
 
 def test_fp64_mma_metric_geometry_max_planes(O, monkeypatch):
     monkeypatch.setenv("SO3GPU_FP64_MMA", "1")
     p = params(512, 64, mode=3)
     fl = synth.gen_flmn(p, 4243)
-    assert rel_err(so3.inverse(fl, p), O.inverse(fl, oparams(O, p))) < 1e-12
+    f_ref = O.inverse(fl, oparams(O, p))
+    assert rel_err(so3.inverse(fl, p), f_ref) < 1e-12
+    assert rel_err(so3.forward(f_ref, p), O.forward(f_ref, oparams(O, p))) < 1e-12

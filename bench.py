@@ -443,6 +443,29 @@ def run_ours(a):
     r64 = timed_steps(step64, a.steps, a.warmup, stream, ctx, so3, sdist, local, world, a.profile_region and B == 0)
     fp64_value = sdist.job_throughput(world * a.steps, r64["total_ms"] / 1e3)
     rt_err = float(((d_back - d_flmn).abs().max() / d_flmn.abs().max()).item())
+    # the other FP64 contraction engine (FP64 tensor cores <-> FMA kernels), same step, same inputs
+    other = "0" if os.environ.get("SO3GPU_FP64_MMA", "0") == "1" else "1"
+    prev = os.environ.get("SO3GPU_FP64_MMA")
+    os.environ["SO3GPU_FP64_MMA"] = other
+    d_back2 = torch.empty_like(d_back)
+    ref_back = d_back.clone()
+
+    def step64b():
+        ctx.inverse(d_flmn, p, out=d_f)
+        ctx.forward(d_f, p, out=d_back2)
+
+    r64b = timed_steps(step64b, a.steps, a.warmup, stream, ctx, so3, sdist, local, world)
+    torch.cuda.synchronize()
+    fp64_alt = {"engine": "fp64 tensor cores (mma.sync m8n8k4)" if other == "1" else "fp64 FMA kernels",
+                "value": sdist.job_throughput(world * a.steps, r64b["total_ms"] / 1e3),
+                "ms_per_step": r64b["total_ms"] / a.steps,
+                "stage_ms": {k: round(v[0] / v[1], 4) for k, v in r64b["stages"].items()},
+                "rel_diff_vs_default_engine": float(((d_back2 - ref_back).abs().max() / ref_back.abs().max()).item())}
+    if prev is None:
+        del os.environ["SO3GPU_FP64_MMA"]
+    else:
+        os.environ["SO3GPU_FP64_MMA"] = prev
+    del d_back2, ref_back
     del d_back
 
     # ---- split-precision batch path: B signals per step
@@ -627,6 +650,7 @@ def run_ours(a):
                                if mixed else "one inverse + one forward, FP64"),
                 "precision": headline["precision"],
                 "mixed": mixed,
+                "fp64_other_engine": fp64_alt,
                 "fp64": {"value": fp64_value, "unit": UNIT, "ms_per_step": r64["total_ms"] / a.steps,
                          "roundtrip_rel_err": rt_err,
                          "stage_ms": {k: round(v[0] / v[1], 4) for k, v in r64["stages"].items()},

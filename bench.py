@@ -39,6 +39,14 @@ METRIC = "inv+fwd transforms/s at L=512,N=64: mixed vs FP64 GPU at ≤1e-10 rel 
 UNIT = "transforms/s"
 
 
+_T0 = time.perf_counter()
+
+
+def log(msg):
+    """Progress of the legs on stderr (the JSON line goes to stdout)."""
+    print(f"[bench {time.perf_counter() - _T0:7.1f} s] {msg}", file=sys.stderr, flush=True)
+
+
 def args_():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -425,11 +433,13 @@ def run_ours(a):
     ctx = so3.Context(local, stream=stream)
     ctx.prepare(p)
     from so3_b200 import peaks
+    log("probes")
     fp64_peak = peaks.fp64_tflops(local)
     int8_peak = peaks.int8_mma_tops(local)
     probes = {"fp64_fma_tflops": fp64_peak, "fp64_dmma_tflops": peaks.dmma_tflops(local),
               "int8_tcgen05_tops": int8_peak, "hbm_copy_gbs": peaks.hbm_copy_gbs(local)}
 
+    log("fp64 leg")
     # ---- plain FP64 path, one signal per step
     fl_host = synth.gen_flmn(p, sdist.signal_seed(1000, rank, 0), "uniform")
     d_flmn = torch.from_numpy(fl_host).to(dev)
@@ -443,6 +453,7 @@ def run_ours(a):
     r64 = timed_steps(step64, a.steps, a.warmup, stream, ctx, so3, sdist, local, world, a.profile_region and B == 0)
     fp64_value = sdist.job_throughput(world * a.steps, r64["total_ms"] / 1e3)
     rt_err = float(((d_back - d_flmn).abs().max() / d_flmn.abs().max()).item())
+    log("fp64 leg, other contraction engine")
     # the other FP64 contraction engine (FP64 tensor cores <-> FMA kernels), same step, same inputs
     other = "0" if os.environ.get("SO3GPU_FP64_MMA", "0") == "1" else "1"
     prev = os.environ.get("SO3GPU_FP64_MMA")
@@ -468,6 +479,7 @@ def run_ours(a):
     del d_back2, ref_back
     del d_back
 
+    log("split-precision leg")
     # ---- split-precision batch path: B signals per step
     mixed = None
     headline = {"value": fp64_value, "run": r64, "units_per_step": 1, "precision": "fp64"}
@@ -574,16 +586,19 @@ def run_ours(a):
     if mixed:
         hbm_stages["split_step"] = stage_roof(run["stages"], lambda k: B if k.startswith("mixed") else 1)
 
+    log("C3 leg")
     # ---- config C3: 512 signals, L=128, N=16, Gaussian (l+1)^-2, split vs FP64
     c3 = None
     if a.c3 > 0 and B > 0:
         c3 = run_c3(so3, synth, a.c3, rank, dev, a.steps, a.warmup, stream, sdist, local, world)
 
+    log("C4 leg")
     # ---- config C4: one S^2 signal at L=1024 convolved with kernels (N=8), inverse to samples
     c4 = None
     if a.c4 > 0 and B > 0:
         c4 = run_c4(so3, synth, a.c4, rank, dev, stream, sdist, local, world)
 
+    log("e2e leg")
     # ---- end to end through the drop-in C ABI with host buffers
     e2e = None
     if not a.no_e2e:
@@ -605,6 +620,7 @@ def run_ours(a):
         for rate in rates:
             row = {"offered_rate_rps": rate}
             for prec in ("fp64", "mixed"):
+                log(f"serving {prec} at {rate:g}/s")
                 row[prec] = sserve.serving_run(a.serve, rate, seed=rank + 11, precision=prec, device=local,
                                                max_batch=16)
             serving["by_rate"].append(row)
@@ -619,6 +635,7 @@ def run_ours(a):
                                                             device=local, shapes=shapes)
 
     cpu = None
+    log("cpu baseline")
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
             procs = cpu_procs(L, N)
@@ -630,6 +647,7 @@ def run_ours(a):
                              f"planes; {procs} concurrent single-threaded processes",
                    "seconds_per_unit_per_process": unit_s}
             if a.cpu_full_unit:
+                log("cpu full unit")
                 full_s = cpu_full_unit_seconds(L, N, procs)
                 cpu["full_unit_check"] = {"seconds_per_unit_per_process": full_s, "value": procs / full_s,
                                           "estimate_over_full": unit_s / full_s,

@@ -135,6 +135,17 @@ class Server {
       for (int m = 0; m < 2; m++)
         if (int rc = ensure_dl(D_, max_L_, m, slots_[0]->s, &t)) return rc;
     }
+    // tables resident before the server existed belong to other users of the
+    // device; the budget is charged for the Delta tables the server reads
+    // (to max_L) and for every table built after this point
+    base_resident_ = resident_bytes(D_);
+    dl_charge_ = 0;
+    if (max_L_ > 0) {
+      int cap = 1;
+      while (cap < max_L_) cap <<= 1;
+      if (cap < 64) cap = 64;
+      dl_charge_ = 2 * (size_t)dl_plane_offset(cap) * sizeof(double);
+    }
     worker_ = std::thread([this] {
       set_thread_autotune(false);  // never stall admission on tuning a new geometry
       loop();
@@ -379,7 +390,8 @@ class Server {
           }
         if (!free_slot) break;
         std::vector<Req*> unit = pick_unit();
-        const size_t resident = resident_bytes(D_);
+        const size_t now_res = resident_bytes(D_);
+        const size_t resident = dl_charge_ + (now_res > base_resident_ ? now_res - base_resident_ : 0);
         const size_t room = budget_ > resident ? budget_ - resident : 0;
         size_t need = unit_bytes(unit);
         while (need > room && unit.size() > 1) {  // shrink the batch to fit
@@ -444,6 +456,7 @@ class Server {
   std::unordered_map<long long, Req*> reqs_;
   long long next_id_ = 0, completed_ = 0, units_ = 0;
   size_t inflight_bytes_ = 0, peak_bytes_ = 0;
+  size_t base_resident_ = 0, dl_charge_ = 0;  // see start()
   int busy_ = 0;
   bool stop_ = false;
 };

@@ -7,6 +7,7 @@
 // device-to-device copy of a buffer far larger than L2.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "tc_sm100.cuh"
@@ -168,7 +169,19 @@ double dmma_tflops() {
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  const int blocks = sms * 4, threads = 256, iters = 2048;
+  const int blocks = sms * 4, threads = 256;
+  // a short launch first: the iteration count is sized for about 20 ms per launch
+  int iters = 16;
+  {
+    cudaEventRecord(e0);
+    dmma_chain<<<blocks, threads>>>(out, iters);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    const double per_iter = ms > 0 ? ms / iters : 1e-3;
+    iters = (int)std::min(4096.0, std::max(16.0, 20.0 / per_iter));
+  }
   dmma_chain<<<blocks, threads>>>(out, iters);  // warm-up
   float best = 1e30f;
   for (int r = 0; r < 5; r++) {

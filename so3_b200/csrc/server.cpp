@@ -242,9 +242,10 @@ class Server {
   static int unit_precision(const std::vector<Req*>& b) {
     return (b[0]->precision == kPrecMixedInt8 && (int)b.size() >= kMinSplitBatch) ? kPrecMixedInt8 : kPrecFp64;
   }
-  // A split-precision unit whose requests differ in parameters (ragged path).
+  // A unit whose requests differ in parameters: the ragged drivers, which run
+  // each signal with its own parameters (in split precision, one shared
+  // tensor-core contraction; in FP64, one transform after the other).
   static bool unit_ragged(const std::vector<Req*>& b) {
-    if (unit_precision(b) != kPrecMixedInt8) return false;
     for (const Req* r : b)
       if (!same_params(*r, *b[0])) return true;
     return false;
@@ -254,10 +255,13 @@ class Server {
     const Req& r = *b[0];
     const int real = r.p.reality != 0;
     size_t need;
-    if (unit_ragged(b)) {
+    if (unit_ragged(b) && unit_precision(b) == kPrecMixedInt8) {
       std::vector<so3_parameters_t> ps;
       for (const Req* q : b) ps.push_back(q->p);
       need = ragged_workspace_bytes(ps.data(), (int)ps.size(), r.kind == 1);
+    } else if (unit_ragged(b)) {  // FP64, one signal at a time in one workspace
+      need = 0;
+      for (const Req* q : b) need = std::max(need, workspace_bytes(q->p, q->p.reality != 0));
     } else {
       need = batch_workspace_bytes(r.p, real, (int)b.size(), unit_precision(b));
     }
@@ -311,6 +315,7 @@ class Server {
     if (rc == kOk) {
       sl->wk.ws = ws;
       sl->wk.ws_bytes = sl->bytes;
+      sl->wk.borrowed = true;  // a size mismatch fails the unit instead of reallocating
       if (r.kind == 2) {
         const size_t wb = (workspace_bytes(r.p, 0) + 255) & ~size_t(255);
         double2* hlmn = reinterpret_cast<double2*>(static_cast<char*>(ws) + wb);

@@ -158,6 +158,7 @@ int timer_collect(StageTimer* t);  // synchronises on the recorded events
 struct Workspace {
   void* ws = nullptr;
   size_t ws_bytes = 0;
+  bool borrowed = false;  // ws is owned by the caller (never reallocated or freed here)
   StageTimer timer;
 };
 Device* device_state(int device);  // lazily created per CUDA device

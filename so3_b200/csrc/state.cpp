@@ -182,6 +182,8 @@ int timer_collect(StageTimer* t) {
 }
 
 int ensure_ws(Workspace* W, size_t bytes, void** out) {
+  if (bytes > W->ws_bytes && W->borrowed)
+    return fail(kOutOfMemory, "borrowed workspace too small for this call");
   if (bytes > W->ws_bytes) {
     if (W->ws) cudaFree(W->ws);
     W->ws = nullptr;

@@ -178,14 +178,15 @@ def latency_summary(res, wall):
             "mean_batch": float(np.mean([r.batch for r in res])) if res else None}
 
 
-def replay_stream(server: Server, trace, time_scale: float = 1.0, seed: int = 5):
+def replay_stream(server: Server, trace, time_scale: float = 1.0, seed: int = 5, timeout_s: float = 600.0):
     """Replays a trace of arbitrary length with bounded device memory.  The
     inverse and forward inputs of every request are prefixes of one seeded
     pool of U(-1,1) complex values as large as the largest input of the trace
     (transforms read no entry outside their band limits, so any prefix is a
     valid input); directional-convolution requests get their own buffers.
     Every request gets its own output buffer at submission, released once it
-    has completed.  Returns (results, wall seconds)."""
+    has completed.  Returns (results, wall seconds); raises TimeoutError when
+    requests are still pending timeout_s after the first submission."""
     import torch
     need = 0
     for r in trace:
@@ -225,8 +226,16 @@ def replay_stream(server: Server, trace, time_scale: float = 1.0, seed: int = 5)
             if d is not None:
                 done[k] = d
                 del live[k]
-    for k in list(live):
-        done[k] = server.wait(k)
+    while live:  # bounded: a request that never completes raises instead of blocking forever
+        for k in list(live):
+            d = server.poll(k)
+            if d is not None:
+                done[k] = d
+                del live[k]
+        if live:
+            if time.perf_counter() - t0 > timeout_s:
+                raise TimeoutError(f"{len(live)} requests still pending after {timeout_s:g} s")
+            time.sleep(0.001)
     wall = time.perf_counter() - t0
     live.clear()
     return [done[i] for i in ids], wall

@@ -387,6 +387,25 @@ def pct(lat, q):
     return s[min(len(s) - 1, max(0, math.ceil(q * len(s)) - 1))]
 
 
+def serving_child(n, rate, seed, prec, device, max_batch, shapes, warm=False, timeout=420):
+    """One serving measurement in a child process (its own CUDA context and
+    tables), killed after `timeout` seconds: a stalled trace cannot hold up
+    the rest of the bench.  warm: one untimed pass of the same trace first."""
+    code = ("import json,sys; sys.path.insert(0, %r); from so3_b200 import serve as s; "
+            "kw=dict(seed=%d, precision=%r, device=%d, max_batch=%d, shapes=%r); "
+            "%s print(json.dumps(s.serving_run(%d, %r, **kw)))"
+            % (ROOT, seed, prec, device, max_batch, shapes,
+               ("s.serving_run(%d, %r, **kw); " % (n, rate)) if warm else "", n, rate))
+    try:
+        r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=timeout)
+    except subprocess.TimeoutExpired:
+        return {"timed_out_s": timeout, "requests": n, "offered_rate_rps": rate, "precision": prec}
+    if r.returncode != 0:
+        return {"failed": r.stderr.strip().splitlines()[-1:] if r.stderr else ["no output"], "requests": n,
+                "offered_rate_rps": rate, "precision": prec}
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
 def run_serve_sweep(a):
     """Config C5 at its stated size: 20,000 seeded requests (60 % inverse /
     40 % forward complex MW, L log-uniform in [16, 1024], N uniform in
@@ -621,8 +640,7 @@ def run_ours(a):
             row = {"offered_rate_rps": rate}
             for prec in ("fp64", "mixed"):
                 log(f"serving {prec} at {rate:g}/s")
-                row[prec] = sserve.serving_run(a.serve, rate, seed=rank + 11, precision=prec, device=local,
-                                               max_batch=16)
+                row[prec] = serving_child(a.serve, rate, rank + 11, prec, local, 16, None)
             serving["by_rate"].append(row)
         # recurring geometries offered as a burst: split-precision requests batch (up to 8 per launch)
         shapes = [(512, 16), (256, 32), (128, 64)]
@@ -630,9 +648,8 @@ def run_ours(a):
                                          f"Poisson 1000/s offered, batches of up to 8; measured after one untimed "
                                          f"pass of the same trace (resident tables built)"}
         for prec in ("fp64", "mixed"):
-            sserve.serving_run(256, 1000.0, seed=rank + 21, precision=prec, device=local, shapes=shapes)  # warm-up
-            serving["recurring"][prec] = sserve.serving_run(256, 1000.0, seed=rank + 21, precision=prec,
-                                                            device=local, shapes=shapes)
+            log(f"serving recurring {prec}")
+            serving["recurring"][prec] = serving_child(256, 1000.0, rank + 21, prec, local, 8, shapes, warm=True)
 
     cpu = None
     log("cpu baseline")

@@ -178,14 +178,18 @@ def latency_summary(res, wall):
             "mean_batch": float(np.mean([r.batch for r in res])) if res else None}
 
 
-def replay_stream(server: Server, trace, time_scale: float = 1.0, seed: int = 5, timeout_s: float = 600.0):
+def replay_stream(server: Server, trace, time_scale: float = 1.0, seed: int = 5, timeout_s: float = 600.0,
+                  max_out_bytes: int = 16 << 30):
     """Replays a trace of arbitrary length with bounded device memory.  The
     inverse and forward inputs of every request are prefixes of one seeded
     pool of U(-1,1) complex values as large as the largest input of the trace
     (transforms read no entry outside their band limits, so any prefix is a
     valid input); directional-convolution requests get their own buffers.
     Every request gets its own output buffer at submission, released once it
-    has completed.  Returns (results, wall seconds); raises TimeoutError when
+    has completed; while the outstanding outputs exceed max_out_bytes the
+    client waits for its oldest request before submitting the next (a client
+    with bounded memory: at offered rates above capacity the submissions
+    then follow the completions).  Returns (results, wall seconds); raises TimeoutError when
     requests are still pending timeout_s after the first submission."""
     import torch
     need = 0
@@ -200,6 +204,7 @@ def replay_stream(server: Server, trace, time_scale: float = 1.0, seed: int = 5,
     conv = {}
     torch.cuda.synchronize()
     live, done = {}, {}
+    live_bytes = 0
     ids = []
     t0 = time.perf_counter()
     for r in trace:
@@ -217,15 +222,20 @@ def replay_stream(server: Server, trace, time_scale: float = 1.0, seed: int = 5,
             if key not in conv:
                 conv[key] = request_buffers(r)[1:3]
             (a, b), n_out = conv[key], f_size(p)
+        while live and live_bytes + 16 * n_out > max_out_bytes:  # bounded client memory
+            k = next(iter(live))
+            done[k] = server.wait(k)
+            live_bytes -= live.pop(k).numel() * 16
         out = torch.empty(n_out, dtype=torch.complex128, device="cuda")
         rid = server.submit(r["kind"], p, a, out, r["precision"], inp2=b)
         ids.append(rid)
         live[rid] = out
+        live_bytes += 16 * n_out
         for k in list(live):  # a completed poll hands over (and forgets) the record
             d = server.poll(k)
             if d is not None:
                 done[k] = d
-                del live[k]
+                live_bytes -= live.pop(k).numel() * 16
     while live:  # bounded: a request that never completes raises instead of blocking forever
         for k in list(live):
             d = server.poll(k)

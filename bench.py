@@ -412,16 +412,12 @@ def run_serve_sweep(a):
     [1, min(L, 64)], U(-1,1) inputs, Poisson arrivals) at each offered rate,
     FP64 and split precision, 120 GB admission budget: throughput, p50 / p99
     latency, mean unit size."""
-    import torch
-
-    from so3_b200 import serve as sserve
-    torch.cuda.set_device(0)
     rates = [float(x) for x in a.serve_sweep.split(",") if x]
     rows = []
     for rate in rates:
         row = {"offered_rate_rps": rate}
         for prec in ("fp64", "mixed"):
-            row[prec] = sserve.serving_run(20000, rate, seed=11, precision=prec, device=0, max_batch=16)
+            row[prec] = serving_child(20000, rate, 11, prec, 0, 16, None, timeout=1500)
         rows.append(row)
         print(json.dumps({"partial": row}), file=sys.stderr, flush=True)
     print(json.dumps({"serving_sweep": rows, "requests_per_rate": 20000,

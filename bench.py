@@ -146,21 +146,22 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------------- CPU side
+CPU_SAMPLE_N = 8  # the sampled unit's N: 2 * 8 - 1 = 15 of the n-planes
+
+
 def _cpu_sample_worker(args):
-    """One bounded sample of the reference's own CPU path (run in a spawned
-    process): so3_core_inverse_via_ssht + so3_core_forward_via_ssht at the
-    bench's L and N restricted to n_mode=MAXIMUM (2 of the 2N-1 n-planes per
-    direction), plus the gamma-axis FFT passes alone, so the full unit can be
-    rebuilt as t_gamma + (2N-1)/2 * (t_sample - t_gamma)."""
+    """One timed run of the reference's own CPU path (in a spawned process):
+    so3_core_inverse_via_ssht + so3_core_forward_via_ssht, all n-planes, at
+    band limit L and N (the bench's N for the full-unit check, CPU_SAMPLE_N
+    for the bounded sample).  Returns wall seconds."""
     L, N, use_ref = args[:3]
-    full = len(args) > 3 and args[3]
     import ctypes
 
     import numpy as np
     sys.path.insert(0, ROOT)
     from oracle import oracle as O
     from so3_b200 import synth
-    p = O.params(L, N, mode=O.ALL if full else O.MAXIMUM)
+    p = O.params(L, N)
     fl = synth.gen_flmn(p, 77, "uniform")
     R = O.ref() if use_ref else None
     f = np.zeros(O.f_size(p), np.complex128)
@@ -174,32 +175,25 @@ def _cpu_sample_worker(args):
     else:
         f = O.inverse(fl, p)
         O.forward(f, p, out=out)
-    t1 = time.perf_counter()
-    if full:
-        return t1 - t0, 0.0
-    # the gamma passes (one backward, one forward over all samples)
-    stride = L * (2 * L - 1)
-    g = np.zeros((2 * N - 1) * stride, np.complex128)
-    t2 = time.perf_counter()
-    O.dft_strided(g, 2 * N - 1, stride, stride, 1, +1)
-    O.dft_strided(g, 2 * N - 1, stride, stride, 1, -1)
-    t3 = time.perf_counter()
-    return t1 - t0, t3 - t2
+    return time.perf_counter() - t0
 
 
 def cpu_unit_seconds(L, N, procs):
-    """Per-process wall seconds of one full unit, estimated from the sample."""
+    """Per-process wall seconds of one full unit at (L, N), estimated from a
+    complete transform at (L, CPU_SAMPLE_N) scaled by the number of n-planes
+    (the per-plane work of the reference, one spin SHT and its share of the
+    gamma FFT, hardly depends on n; checked against a full unit at L=512,
+    N=64 with --cpu-full-unit)."""
     import multiprocessing as mp
     from oracle import oracle as O
     O.build()
     use_ref = O.ref() is not None
+    ns = min(N, CPU_SAMPLE_N)
     ctx = mp.get_context("spawn")
     with ctx.Pool(procs) as pool:
-        res = pool.map(_cpu_sample_worker, [(L, N, use_ref)] * procs)
-    units = []
-    for ts, tg in res:
-        units.append(tg + (2 * N - 1) / 2.0 * max(ts - tg, 0.0))
-    return statistics.median(units), statistics.median([r[0] for r in res]), use_ref
+        res = pool.map(_cpu_sample_worker, [(L, ns, use_ref)] * procs)
+    t = statistics.median(res)
+    return t * (2 * N - 1) / (2 * ns - 1), t, use_ref
 
 
 def cpu_full_unit_seconds(L, N, procs):
@@ -212,8 +206,8 @@ def cpu_full_unit_seconds(L, N, procs):
     use_ref = O.ref() is not None
     ctx = mp.get_context("spawn")
     with ctx.Pool(procs) as pool:
-        res = pool.map(_cpu_sample_worker, [(L, N, use_ref, True)] * procs)
-    return statistics.median([r[0] for r in res])
+        res = pool.map(_cpu_sample_worker, [(L, N, use_ref)] * procs)
+    return statistics.median(res)
 
 
 def cpu_procs(L, N):
@@ -244,9 +238,10 @@ def run_reference(a):
         vals.append(procs / unit_s)
     wall = time.perf_counter() - t0
     v = statistics.median(vals)
-    sample = (f"so3_core_inverse_via_ssht + so3_core_forward_via_ssht at L={a.L}, N={a.N}, n_mode=MAXIMUM "
-              f"(2 of {2 * a.N - 1} n-planes per direction) per process plus the gamma FFT passes alone, "
-              f"scaled to all {2 * a.N - 1} planes; {procs} concurrent processes")
+    ns = min(a.N, CPU_SAMPLE_N)
+    sample = (f"so3_core_inverse_via_ssht + so3_core_forward_via_ssht at L={a.L}, N={ns} (all {2 * ns - 1} "
+              f"n-planes) per process, scaled by n-planes to N={a.N} ({2 * a.N - 1} planes); {procs} concurrent "
+              f"single-threaded processes")
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * wall / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -470,7 +465,7 @@ def run_ours(a):
     rt_err = float(((d_back - d_flmn).abs().max() / d_flmn.abs().max()).item())
     log("fp64 leg, other contraction engine")
     # the other FP64 contraction engine (FP64 tensor cores <-> FMA kernels), same step, same inputs
-    other = "0" if os.environ.get("SO3GPU_FP64_MMA", "0") == "1" else "1"
+    other = "0" if os.environ.get("SO3GPU_FP64_MMA", "1") != "0" else "1"
     prev = os.environ.get("SO3GPU_FP64_MMA")
     os.environ["SO3GPU_FP64_MMA"] = other
     d_back2 = torch.empty_like(d_back)
@@ -655,9 +650,9 @@ def run_ours(a):
             unit_s, samp_s, use_ref = cpu_unit_seconds(L, N, procs)
             cpu = {"value": procs / unit_s, "unit": UNIT, "cores": procs,
                    "kind": "reference" if use_ref else "port",
-                   "sample": f"inverse+forward at L={L}, N={N} restricted to n_mode=MAXIMUM (2 of {2 * N - 1} "
-                             f"n-planes per direction, {samp_s:.1f} s) plus the gamma FFT passes, scaled to all "
-                             f"planes; {procs} concurrent single-threaded processes",
+                   "sample": f"inverse+forward at L={L}, N={min(N, CPU_SAMPLE_N)} (all {2 * min(N, CPU_SAMPLE_N) - 1} "
+                             f"n-planes, {samp_s:.1f} s per process), scaled by n-planes to N={N}; {procs} "
+                             f"concurrent single-threaded processes",
                    "seconds_per_unit_per_process": unit_s}
             if a.cpu_full_unit:
                 log("cpu full unit")

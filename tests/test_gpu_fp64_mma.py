@@ -1,5 +1,6 @@
-"""FP64 contraction on the FP64 tensor cores (mma.sync m8n8k4 f64,
-SO3GPU_FP64_MMA=1) against the oracle and against the FP64 FMA kernels, on
+"""FP64 contraction on the FP64 tensor cores (mma.sync m8n8k4 f64, the
+default for complex signals; SO3GPU_FP64_MMA=0 selects the FMA kernels)
+against the oracle and against the FP64 FMA kernels, on
 the same seeded inputs: 1e-12 normwise relative error, as every FP64 parity
 test."""
 import pytest

@@ -651,8 +651,11 @@ int run_inverse_ragged(Device* D, Workspace* wk, const so3_parameters_t* ps, int
       std::lock_guard<std::mutex> lk(D->mu);
       if ((rc = ensure_dl(D, 1, m, s, &dl))) return rc;  // current table (already large enough)
     }
+    int Lm = 0, Nm = 0;
+    for (const RaggedSig& r : rs[m]) Lm = std::max(Lm, r.g.L), Nm = std::max(Nm, r.g.N);
+    const DigitTable* tab = covering_digit_table(D, Lm, Nm, m, dl, true, s);
     timer_begin(T, s, &ev);
-    if ((rc = launch_mixed_ragged(false, rs[m], dl, wsb + sig_end, s))) return rc;
+    if ((rc = launch_mixed_ragged(false, rs[m], dl, tab, wsb + sig_end, s))) return rc;
     timer_end(T, s, kStMixInv, ev);
   }
   for (const RagItem& it : items) {
@@ -728,8 +731,11 @@ int run_forward_ragged(Device* D, Workspace* wk, const so3_parameters_t* ps, int
       std::lock_guard<std::mutex> lk(D->mu);
       if ((rc = ensure_dl(D, 1, m, s, &dl))) return rc;
     }
+    int Lm = 0, Nm = 0;
+    for (const RaggedSig& r : rs[m]) Lm = std::max(Lm, r.g.L), Nm = std::max(Nm, r.g.N);
+    const DigitTable* tab = covering_digit_table(D, Lm, Nm, m, dl, true, s);
     timer_begin(T, s, &ev);
-    if ((rc = launch_mixed_ragged(true, rs[m], dl, wsb + sig_end, s))) return rc;
+    if ((rc = launch_mixed_ragged(true, rs[m], dl, tab, wsb + sig_end, s))) return rc;
     timer_end(T, s, kStMixFwd, ev);
   }
   return kOk;

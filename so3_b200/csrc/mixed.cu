@@ -1198,6 +1198,12 @@ struct RagArgs {
   const GroupDesc* groups;
   const double* dl;
   int ngroups;
+  // resident digit table (null: generate A from dl): blocks of pair (mu, nu)
+  // from pair_off[mu * tab_N + nu], tab_nc chunks (every group has L <= tab_L
+  // and N <= tab_N, so its blocks are the table's)
+  const uint8_t* tab;
+  const long long* pair_off;
+  int tab_N, tab_nc;
 };
 
 // Group of a 1-D block index (prefix offsets item0 or slice0, ascending).
@@ -1392,7 +1398,7 @@ __global__ void __launch_bounds__(256) ragged_slice_fwd_kernel(RagArgs a) {
 // Tensor-core products of a ragged batch: one CTA per item (group, mu, tile,
 // nu), the producer warps generating A from Delta as mixed_tc_kernel does;
 // outputs in each signal's own layout.
-template <bool FWD>
+template <bool FWD, bool TAB>
 __global__ void __launch_bounds__(kThreads, 1) ragged_tc_kernel(RagArgs ra) {
   extern __shared__ __align__(1024) unsigned char smraw[];
   TcSmem& S = *reinterpret_cast<TcSmem*>(smraw);
@@ -1427,7 +1433,7 @@ __global__ void __launch_bounds__(kThreads, 1) ragged_tc_kernel(RagArgs ra) {
   const uint32_t accum = tc::smem_u32(&S.accum);
   if (tid == 0) {
     for (int s = 0; s < kStages; s++) {
-      tc::mbar_init(full0 + 8 * s, kGen + 1);
+      tc::mbar_init(full0 + 8 * s, TAB ? 1 : kGen + 1);
       tc::mbar_init(empty0 + 8 * s, 1);
     }
     tc::mbar_init(accum, 1);
@@ -1441,7 +1447,9 @@ __global__ void __launch_bounds__(kThreads, 1) ragged_tc_kernel(RagArgs ra) {
 
   if (warp == 0) {
     if (lane == 0 && nk > 0) {
-      constexpr uint32_t idesc = tc::idesc_s8(kM, kN);
+      // table blocks are stored rows m', reduction l; the forward reads them
+      // transposed as an MN-major operand
+      constexpr uint32_t idesc = tc::idesc_s8(kM, kN) | ((FWD && TAB) ? (1u << 16) : 0u);
       for (int k = 0; k < nk; k++) {
         const int s = k & 1;
         tc::mbar_wait(full0 + 8 * s, (k >> 1) & 1, &g_tc_error, 2);
@@ -1454,7 +1462,8 @@ __global__ void __launch_bounds__(kThreads, 1) ragged_tc_kernel(RagArgs ra) {
             const uint64_t ad = tc::smem_desc(xb + i * (kM * kKC) + ks * 2 * (kM * 16), kM * 16, 128);
 #pragma unroll
             for (int j = 0; j + i < kND; j++) {
-              const uint64_t bd = tc::smem_desc(ab + j * (kN * kKC) + ks * 2 * (kN * 16), kN * 16, 128);
+              const uint64_t bd = (FWD && TAB) ? tc::smem_desc(ab + j * (kN * kKC) + ks * 512, 128, 1024)
+                                               : tc::smem_desc(ab + j * (kN * kKC) + ks * 2 * (kN * 16), kN * 16, 128);
               tc::mma_i8(tbase + (uint32_t)(kN * (i + j)), ad, bd, idesc, (k | ks | i) != 0);
             }
           }
@@ -1465,18 +1474,24 @@ __global__ void __launch_bounds__(kThreads, 1) ragged_tc_kernel(RagArgs ra) {
     }
   } else if (warp == 1) {
     if (lane == 0) {
+      const int q = max(mu, nu) / kKC;
+      const uint8_t* tb = TAB ? ra.tab + (long long)ra.pair_off[(long long)mu * ra.tab_N + nu] * kAStage : nullptr;
       for (int k = 0; k < nk; k++) {
         const int s = k & 1;
         if (k >= kStages) tc::mbar_wait(empty0 + 8 * s, ((k >> 1) - 1) & 1, &g_tc_error, 2);
-        tc::mbar_arrive_expect_tx(full0 + 8 * s, kXStage);
+        tc::mbar_arrive_expect_tx(full0 + 8 * s, TAB ? kXStage + kAStage : kXStage);
         tc::bulk_g2s(tc::smem_u32(&S.X[s][0]), xs + (long long)(kc0 + k) * kXStage, kXStage, full0 + 8 * s);
+        if (TAB) {
+          const long long blk = FWD ? digit_block(k, t, q, ra.tab_nc) : digit_block(t, kc0 + k, q, ra.tab_nc);
+          tc::bulk_g2s(tc::smem_u32(&S.A[s][0]), tb + blk * kAStage, kAStage, full0 + 8 * s);
+        }
       }
     }
   } else {
     const int gw = warp - 2;
     double xa[4][4], xb[4][4];
-    if (nk > 0) gen_load<FWD>(a, mu, nu, lmin, r0, kc0 * kKC, gw, lane, xa);
-    for (int k = 0; k < nk; k += 2) {
+    if (!TAB && nk > 0) gen_load<FWD>(a, mu, nu, lmin, r0, kc0 * kKC, gw, lane, xa);
+    for (int k = 0; k < (TAB ? 0 : nk); k += 2) {
       if (k + 1 < nk) gen_load<FWD>(a, mu, nu, lmin, r0, (kc0 + k + 1) * kKC, gw, lane, xb);
       if (k >= kStages) tc::mbar_wait(empty0, ((k >> 1) - 1) & 1, &g_tc_error, 2);
       gen_store(&S.A[0][0], gw, lane, xa);
@@ -1635,7 +1650,7 @@ size_t digit_table_bytes(int L, int N) {
 // never see it change.  Without a table the kernels generate the digits from
 // Delta.
 int ensure_digit_table(Device* D, const Geometry& g, int method, const double* dl, cudaStream_t s,
-                       const DigitTable** out) {
+                       const DigitTable** out, bool force) {
   *out = nullptr;
   const char* env = getenv("SO3GPU_DIGIT_TABLE");
   if (env && env[0] == '0') return kOk;
@@ -1646,7 +1661,7 @@ int ensure_digit_table(Device* D, const Geometry& g, int method, const double* d
       return kOk;
     }
   const long long key = ((long long)g.L << 20) ^ ((long long)g.N << 2) ^ method;
-  if (++D->digit_uses[key] < 2 && !(env && env[0] == '1')) return kOk;
+  if (++D->digit_uses[key] < 2 && !(env && env[0] == '1') && !force) return kOk;
   const size_t bytes = digit_table_bytes(g.L, g.N);
   size_t used = 0;
   for (const auto& t : D->digit_tables) used += t->bytes;
@@ -1678,6 +1693,28 @@ int ensure_digit_table(Device* D, const Geometry& g, int method, const double* d
   *out = t.get();
   D->digit_tables.push_back(std::move(t));
   return kOk;
+}
+
+// A resident digit table whose (L, N) cover (L, N) for this recursion, for
+// the ragged contractions (digits do not depend on the band limits); with
+// build, the L = 512, N = 64 table is built when none covers and (L, N) fit
+// it (same memory rule as ensure_digit_table).  Null: generate from Delta.
+const DigitTable* covering_digit_table(Device* D, int L, int N, int method, const double* dl, bool build,
+                                       cudaStream_t s) {
+  {
+    std::lock_guard<std::mutex> lk(D->mu);
+    for (const auto& t : D->digit_tables)
+      if (t->method == method && t->L >= L && t->N >= N) return t.get();
+  }
+  const char* env = getenv("SO3GPU_DIGIT_TABLE");
+  if (!build || L > 512 || N > 64 || (env && env[0] == '0')) return nullptr;
+  Geometry g{};
+  g.L = 512, g.N = 64;
+  const DigitTable* t = nullptr;
+  // built now, not on a geometry's second request as ensure_digit_table
+  // would: the ragged path has no per-geometry history
+  const int rc = ensure_digit_table(D, g, method, dl, s, &t, true);
+  return rc == kOk ? t : nullptr;
 }
 
 // Streaming multiprocessors of the current device (persistent grids).
@@ -1917,8 +1954,8 @@ size_t ragged_scratch_bytes(const std::vector<RaggedSig>& sigs, bool fwd) {
   return sigs.empty() ? 0 : ragged_plan(sigs, fwd).total;
 }
 
-int launch_mixed_ragged(bool fwd, const std::vector<RaggedSig>& sigs, const double* dl, void* scratch,
-                        cudaStream_t s) {
+int launch_mixed_ragged(bool fwd, const std::vector<RaggedSig>& sigs, const double* dl, const DigitTable* tab,
+                        void* scratch, cudaStream_t s) {
   if (sigs.empty()) return kOk;
   for (const auto& r : sigs)
     if (r.g.real) return fail(kUnsupported, "split-precision contractions take complex signals");
@@ -1938,6 +1975,14 @@ int launch_mixed_ragged(bool fwd, const std::vector<RaggedSig>& sigs, const doub
   a.groups = reinterpret_cast<const GroupDesc*>(base + P.grp_off);
   a.dl = dl;
   a.ngroups = (int)P.groups.size();
+  bool use_tab = tab != nullptr;
+  for (const GroupDesc& G : P.groups) use_tab = use_tab && G.Lg <= tab->L && G.Ng <= tab->N;
+  if (use_tab) {
+    a.tab = tab->d;
+    a.pair_off = tab->pair_off;
+    a.tab_N = tab->N;
+    a.tab_nc = (tab->L + kKC - 1) / kKC;
+  }
   if (fwd)
     ragged_slice_fwd_kernel<<<(unsigned)P.slices, 256, 0, s>>>(a);
   else
@@ -1946,13 +1991,17 @@ int launch_mixed_ragged(bool fwd, const std::vector<RaggedSig>& sigs, const doub
   SO3G_CUDA(cudaGetLastError());
   if (P.items == 0) return kOk;
   const int smem = (int)sizeof(TcSmem);
-  if (fwd) {
-    SO3G_CUDA(cudaFuncSetAttribute(ragged_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    ragged_tc_kernel<true><<<(unsigned)P.items, kThreads, smem, s>>>(a);
-  } else {
-    SO3G_CUDA(cudaFuncSetAttribute(ragged_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    ragged_tc_kernel<false><<<(unsigned)P.items, kThreads, smem, s>>>(a);
-  }
+  auto run = [&](auto kernel) -> int {
+    SO3G_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    kernel<<<(unsigned)P.items, kThreads, smem, s>>>(a);
+    return kOk;
+  };
+  int rc;
+  if (fwd)
+    rc = use_tab ? run(ragged_tc_kernel<true, true>) : run(ragged_tc_kernel<true, false>);
+  else
+    rc = use_tab ? run(ragged_tc_kernel<false, true>) : run(ragged_tc_kernel<false, false>);
+  if (rc) return rc;
   SO3G_LAUNCHED();
   SO3G_CUDA(cudaGetLastError());
   return kOk;

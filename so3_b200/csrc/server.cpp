@@ -181,7 +181,10 @@ class Server {
     r->in = in;
     r->in2 = in2;
     r->out = out;
-    r->precision = (kind == 2 || p.reality) ? kPrecFp64 : precision;
+    // split precision where the contractions can read the resident digit table
+    // (L <= 512, N <= 64); larger geometries take the FP64 path, for which
+    // generating the digits per tile costs more than the split saves
+    r->precision = (kind == 2 || p.reality || p.L > 512 || p.N > 64) ? kPrecFp64 : precision;
     r->t_submit = now_us();
     {
       std::lock_guard<std::mutex> lk(mu_);

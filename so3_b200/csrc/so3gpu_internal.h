@@ -245,8 +245,9 @@ int stage_variants(const Geometry& g, const FftPlan& pP, const FftPlan& pg, cons
 // pointers (a device array of nsig pointers) and scratch planes (signal b at
 // W + b * wstride); scratch: mixed_scratch_bytes(g, nsig) bytes.
 size_t mixed_scratch_bytes(const Geometry& g, int nsig);
+// force: build now instead of on the geometry's second call.
 int ensure_digit_table(Device* D, const Geometry& g, int method, const double* dl, cudaStream_t s,
-                       const DigitTable** out);
+                       const DigitTable** out, bool force = false);
 size_t digit_table_bytes(int L, int N);
 // Forward beta stage of a split-precision batch as an int8 tensor-core
 // product (complex MW signals; W: row-major scratch of signal 0, output into
@@ -280,8 +281,12 @@ struct RaggedSig {
 size_t ragged_scratch_bytes(const std::vector<RaggedSig>& sigs, bool fwd);
 // Slicing and tensor-core products of every signal in two launches; dl: the
 // Delta table of the batch's recursion, covering the largest L.
-int launch_mixed_ragged(bool fwd, const std::vector<RaggedSig>& sigs, const double* dl, void* scratch,
-                        cudaStream_t s);
+int launch_mixed_ragged(bool fwd, const std::vector<RaggedSig>& sigs, const double* dl, const DigitTable* tab,
+                        void* scratch, cudaStream_t s);
+// Resident digit table covering (L, N) for a recursion (see mixed.cu), built
+// at L = 512, N = 64 when `build` and none covers; null: digits generated.
+const DigitTable* covering_digit_table(Device* D, int L, int N, int method, const double* dl, bool build,
+                                       cudaStream_t s);
 // Reads and clears the flag the tensor-core kernels set when a bounded wait
 // gave up (0: none; synchronous).
 int mixed_take_error();

@@ -344,7 +344,7 @@ __global__ void __launch_bounds__(kDT, 2) inverse_contract_dmma_kernel(InvArgs a
       const int idx = tid + u * kDT;
       const int sg = idx & 3, j = (idx >> 2) & 1, jm = (idx >> 3) & 15, lc = idx >> 7;
       const int l = lb + lc;
-      double w = (2.0 * l + 1.0) * kInv8Pi2;
+      double w = a.wconst > 0.0 ? a.wconst : (2.0 * l + 1.0) * kInv8Pi2;
       if ((sg == 1 || sg == 2) && (l & 1)) w = -w;  // one negative index: (-1)^l here
       S.X[jm][j][2 * sg][lc] = xv[u].x * w;
       S.X[jm][j][2 * sg + 1][lc] = xv[u].y * w;

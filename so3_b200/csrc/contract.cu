@@ -262,11 +262,19 @@ constexpr int kDN = 2;         // nu per CTA
 constexpr int kDK = 4;         // l per chunk (MMA K)
 constexpr int kBP = 17;        // Bm pitch (doubles): lanes (g, q) hit distinct bank pairs
 constexpr int kAP = 3;         // An pitch
+// X block of one (mu, nu): 8 columns c x 4 steps l, element c * 4 + l.  Block
+// pitches 36 (nu) and 81 (mu) doubles put the staging stores of a warp on 16
+// distinct bank pairs (inverse lanes: sign, nu, 4 mu; forward lanes: l, sign,
+// nu); a fragment read is 32 consecutive doubles either way.
+constexpr int kXJ = 36, kXM = 81;
 struct DSlab {
   double Bm[kDR][kDK][kBP];           // Delta^l_{m', mu0 + j}
   double An[kDR][kDK][kAP];           // Delta^l_{m', nu0 + j}
-  double X[kDM][kDN][8][kDK];         // [mu][nu][c][l], weighted and sign-folded
+  double X[kDM * kXM];                // [mu][nu][c][l], weighted and sign-folded
 };
+__device__ __forceinline__ double& xat(DSlab& S, int jm, int j, int c, int l) {
+  return S.X[jm * kXM + j * kXJ + c * kDK + l];
+}
 
 __device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
@@ -346,8 +354,8 @@ __global__ void __launch_bounds__(kDT, 2) inverse_contract_dmma_kernel(InvArgs a
       const int l = lb + lc;
       double w = a.wconst > 0.0 ? a.wconst : (2.0 * l + 1.0) * kInv8Pi2;
       if ((sg == 1 || sg == 2) && (l & 1)) w = -w;  // one negative index: (-1)^l here
-      S.X[jm][j][2 * sg][lc] = xv[u].x * w;
-      S.X[jm][j][2 * sg + 1][lc] = xv[u].y * w;
+      xat(S, jm, j, 2 * sg, lc) = xv[u].x * w;
+      xat(S, jm, j, 2 * sg + 1, lc) = xv[u].y * w;
     }
   };
   static_assert(kXN == 2 * kDT, "two coefficient slots per thread");
@@ -373,8 +381,8 @@ __global__ void __launch_bounds__(kDT, 2) inverse_contract_dmma_kernel(InvArgs a
 #pragma unroll
       for (int i = 0; i < 8; i++) {
         const double bm = S.Bm[8 * mb + g][q][jm0 + i];
-        dmma(acc[i][0], bm * an0, S.X[jm0 + i][0][g][q]);
-        dmma(acc[i][1], bm * an1, S.X[jm0 + i][1][g][q]);
+        dmma(acc[i][0], bm * an0, xat(S, jm0 + i, 0, g, q));
+        dmma(acc[i][1], bm * an1, xat(S, jm0 + i, 1, g, q));
       }
       __syncthreads();
     }
@@ -614,8 +622,8 @@ __global__ void __launch_bounds__(kDT, 2) forward_contract_dmma_kernel(FwdArgs a
       const int idx = tid + u * kDT;
       const int mc = idx & 3, sg = (idx >> 2) & 3, j = (idx >> 4) & 1, jm = idx >> 5;
       const double w = ((sg == 1 || sg == 2) && ((mb0 + mc) & 1)) ? -1.0 : 1.0;  // (-1)^{m'}
-      S.X[jm][j][2 * sg][mc] = xv[u].x * w;
-      S.X[jm][j][2 * sg + 1][mc] = xv[u].y * w;
+      xat(S, jm, j, 2 * sg, mc) = xv[u].x * w;
+      xat(S, jm, j, 2 * sg + 1, mc) = xv[u].y * w;
     }
   };
 
@@ -639,8 +647,8 @@ __global__ void __launch_bounds__(kDT, 2) forward_contract_dmma_kernel(FwdArgs a
 #pragma unroll
       for (int i = 0; i < 8; i++) {
         const double bm = S.Bm[8 * mb + g][q][jm0 + i];
-        dmma(acc[i][0], bm * an0, S.X[jm0 + i][0][g][q]);
-        dmma(acc[i][1], bm * an1, S.X[jm0 + i][1][g][q]);
+        dmma(acc[i][0], bm * an0, xat(S, jm0 + i, 0, g, q));
+        dmma(acc[i][1], bm * an1, xat(S, jm0 + i, 1, g, q));
       }
       __syncthreads();
     }

@@ -538,6 +538,9 @@ __global__ void __launch_bounds__(256, 3) slice_inv_kernel(SliceArgs a) {
     const int c = w & 7, j = (w >> 3) % kMuPer, kb = w / (8 * kMuPer);
     const int mu = mu0 + j;
     if (mu >= L) continue;
+    // chunks below the one holding l = max(mu, nu, L0) are never read: the
+    // inverse items start at that chunk (decode_item), so they are not written
+    if (16 * kb / kKC < max(max(mu, nu), a.L0) / kKC) continue;
     const int combo = c >> 1, part = c & 1;
     const double inv = 1.0 / scl[j][c];
     const InvColumn col = inv_column(a, sig, mu, nu, combo);

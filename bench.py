@@ -11,8 +11,9 @@ against FP64.
     16) with the int8 tensor-core (Ozaki split) contractions, FP64 everywhere
     else; its error against the FP64 path is measured on the same inputs;
   * "fp64": one FP64 inverse + forward per step (reference-exact path);
-  * "e2e": the FP64 drop-in so3_core_{inverse,forward}_via_ssht on pinned host
-    buffers, copies included.
+  * "e2e": end to end from pinned host buffers, copies included: signals
+    streamed through the device API with the copies overlapped (value), and
+    the synchronous drop-in so3_core_{inverse,forward}_via_ssht ("dropin").
 Ranks run independent signals (weak scaling, no collective on the data path).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl ours|reference]
@@ -612,7 +613,8 @@ def run_ours(a):
     # ---- end to end through the drop-in C ABI with host buffers
     e2e = None
     if not a.no_e2e:
-        e2e = run_e2e(so3, p, fl_host, a.steps, local, world, None)
+        e2e = run_e2e(so3, p, fl_host, a.steps, local, world)
+        e2e["dropin"] = run_e2e_dropin(so3, p, fl_host, min(a.steps, 3), local, world)
 
     # ---- serving: a sample of the request trace (inverse 60 % / forward 40 %, complex MW, L log-uniform
     # in [16, 1024], N uniform in [1, min(L, 64)], U(-1,1) inputs, Poisson arrivals), FP64 and split
@@ -786,9 +788,10 @@ def run_c4(so3, synth, nker, rank, dev, stream, sdist, local, world, chunk=16, s
     return out
 
 
-def run_e2e(so3, p, fl_host, steps, local, world, dist):
+def run_e2e_dropin(so3, p, fl_host, steps, local, world):
     """Same metric through so3_core_{inverse,forward}_via_ssht on pinned host
-    buffers: every step copies flmn and f host->device and f and flmn back."""
+    buffers, one synchronous call after the other: every step copies flmn and f
+    host->device and f and flmn back."""
     import ctypes
 
     import numpy as np
@@ -821,8 +824,105 @@ def run_e2e(so3, p, fl_host, steps, local, world, dist):
     nb_fl = fl_host.size * 16
     nb_f = so3.f_size(p) * 16
     return {"value": world * steps / el, "unit": UNIT, "h2d_bytes_per_step": nb_fl + nb_f,
-            "d2h_bytes_per_step": nb_f + nb_fl, "api": "so3_core_inverse_via_ssht + so3_core_forward_via_ssht "
-                                                       "(host pointers, pinned)", "roundtrip_rel_err": err}
+            "d2h_bytes_per_step": nb_f + nb_fl, "steps": steps,
+            "api": "so3_core_inverse_via_ssht + so3_core_forward_via_ssht (host pointers, pinned, synchronous)",
+            "roundtrip_rel_err": err}
+
+
+def run_e2e(so3, p, fl_host, steps, local, world, depth=3):
+    """The metric end to end from pinned host memory through the library's
+    device API (so3_b200.Context, FP64 path), signals streamed: one step = one
+    unit = copy flmn host->device, inverse, copy f device->host, copy that host
+    f back host->device, forward, copy flmn device->host; all copies of every
+    step are inside the timed region.  Copies run on their own streams (one per
+    direction) and overlap the transforms and the other direction's copies of
+    neighbouring units (`depth` device buffer sets in rotation); issue order
+    A(0) A(1) B(0) A(2) B(1) ..., A = upload + inverse + download of f, B =
+    re-upload of f + forward + download of flmn.  Wall clock over the whole
+    stream, synchronised on both sides, max over ranks."""
+    import numpy as np
+    import torch
+
+    from so3_b200 import dist as sdist
+    dev = f"cuda:{local}"
+    nfl, nf = so3.flmn_size(p), so3.f_size(p)
+    units = max(steps, 16)
+    comp, up, down = torch.cuda.Stream(dev), torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    ctx = so3.Context(local, stream=comp)
+    ctx.prepare(p)
+    fl_pin = torch.from_numpy(fl_host).pin_memory()
+    f_pin = [torch.empty(nf, dtype=torch.complex128).pin_memory() for _ in range(depth)]
+    back_pin = [torch.empty(nfl, dtype=torch.complex128).pin_memory() for _ in range(depth)]
+    d_fl = [torch.empty(nfl, dtype=torch.complex128, device=dev) for _ in range(depth)]
+    d_f = [torch.empty(nf, dtype=torch.complex128, device=dev) for _ in range(depth)]
+    d_fin = [torch.empty(nf, dtype=torch.complex128, device=dev) for _ in range(depth)]
+    d_back = [torch.empty(nfl, dtype=torch.complex128, device=dev) for _ in range(depth)]
+    free = [None] * depth  # event: slot's last download done
+
+    def stage_a(s):
+        i = s % depth
+        with torch.cuda.stream(up):
+            if free[i] is not None:
+                up.wait_event(free[i])
+            d_fl[i].copy_(fl_pin, non_blocking=True)
+            e = torch.cuda.Event()
+            e.record(up)
+        comp.wait_event(e)
+        ctx.inverse(d_fl[i], p, out=d_f[i])
+        e = torch.cuda.Event()
+        e.record(comp)
+        with torch.cuda.stream(down):
+            down.wait_event(e)
+            f_pin[i].copy_(d_f[i], non_blocking=True)
+            e = torch.cuda.Event()
+            e.record(down)
+        return e
+
+    def stage_b(s, got_f):
+        i = s % depth
+        with torch.cuda.stream(up):
+            up.wait_event(got_f)
+            d_fin[i].copy_(f_pin[i], non_blocking=True)
+            e = torch.cuda.Event()
+            e.record(up)
+        comp.wait_event(e)
+        ctx.forward(d_fin[i], p, out=d_back[i])
+        e = torch.cuda.Event()
+        e.record(comp)
+        with torch.cuda.stream(down):
+            down.wait_event(e)
+            back_pin[i].copy_(d_back[i], non_blocking=True)
+            free[i] = torch.cuda.Event()
+            free[i].record(down)
+
+    def run(n):
+        pend = stage_a(0)
+        for s in range(1, n):
+            nxt = stage_a(s)
+            stage_b(s - 1, pend)
+            pend = nxt
+        stage_b(n - 1, pend)
+
+    run(depth)  # warm-up: buffers, plans, pinned-memory registration
+    torch.cuda.synchronize()
+    if world > 1:
+        sdist.barrier()
+    t0 = time.perf_counter()
+    run(units)
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    el = sdist.max_over_ranks(el, device=dev)
+    last = (units - 1) % depth
+    err = float(np.abs(back_pin[last].numpy() - fl_host).max() / np.abs(fl_host).max())
+    ctx.close()
+    out = {"value": world * units / el, "unit": UNIT, "h2d_bytes_per_step": 16 * (nfl + nf),
+           "d2h_bytes_per_step": 16 * (nf + nfl), "steps": units, "precision": "fp64",
+           "api": "so3_b200.Context.inverse / forward (so3gpu_inverse / so3gpu_forward) on device buffers, "
+                  "pinned host buffers copied on two copy streams, units streamed",
+           "roundtrip_rel_err": err}
+    del d_fl, d_f, d_fin, d_back
+    torch.cuda.empty_cache()
+    return out
 
 
 def traffic_from_profiles(kernel_stage, L, N):

@@ -1177,9 +1177,9 @@ __global__ void __launch_bounds__(kThreads, 1) beta_tc_kernel(BetaArgs a, int nt
 // by (recursion, L, N) and cuts them into groups of 16 (one M = 128 operand);
 // a group runs at its largest L and N, each signal's columns are zero past its
 // own L, N (and below its L0) and its outputs are written in its own layout.
-// Work items of all groups form one 1-D grid; A is generated from the FP64
-// Delta table in the producer warps (no resident digit table: the group
-// geometry changes from batch to batch).
+// Work items of all groups form one 1-D grid; A comes from a resident digit
+// table when one covers the groups' band limits (the digits do not depend on
+// L or N), else the producer warps generate it from the FP64 Delta table.
 struct SigDesc {
   const double2* flmn;    // inverse: coefficients in; forward: coefficients out
   double2* Wc;            // column-major scratch part: inverse output, forward input
@@ -1290,6 +1290,8 @@ __global__ void __launch_bounds__(256, 3) ragged_slice_inv_kernel(RagArgs a) {
     const int c = w & 7, j = (w >> 3) % kMuPer, kb = w / (8 * kMuPer);
     const int mu = mu0 + j;
     if (mu >= G.Lg) continue;
+    // chunks below the one holding l = max(mu, nu) are never read (ragged_tc_kernel)
+    if (16 * kb / kKC < max(mu, nu) / kKC) continue;
     const int combo = c >> 1, part = c & 1;
     const double inv = 1.0 / scl[j][c];
     const InvColumn col = column(mu, combo);
@@ -1399,8 +1401,9 @@ __global__ void __launch_bounds__(256) ragged_slice_fwd_kernel(RagArgs a) {
 }
 
 // Tensor-core products of a ragged batch: one CTA per item (group, mu, tile,
-// nu), the producer warps generating A from Delta as mixed_tc_kernel does;
-// outputs in each signal's own layout.
+// nu); A streamed from the covering digit table (TAB) or generated from Delta
+// by the producer warps as mixed_tc_kernel does; outputs in each signal's own
+// layout.
 template <bool FWD, bool TAB>
 __global__ void __launch_bounds__(kThreads, 1) ragged_tc_kernel(RagArgs ra) {
   extern __shared__ __align__(1024) unsigned char smraw[];

@@ -175,10 +175,13 @@ __global__ void __launch_bounds__(E::NT, E::MINB) inv_beta_kernel(Geometry g, Ff
     for (int t = threadIdx.x; t < T; t += E::NT) a[t * ld + E::at(L)] = make_double2(0.0, 0.0);
   // column 2q has s = +1 when (2q - (L-1) + n) is even
   const bool first_is_a = ((L - 1 + n) & 1) == 0;
-  auto load = [&](int t, int mp) {  // m' fastest: whole columns read contiguously
+  // m' fastest: whole columns read contiguously
+  auto fetch = [&](int t, int mp, double2& v0, double2& v1) {
     const int c = 2 * (q0 + t);
-    const double2 v0 = c < ncols ? cbase[(long long)c * g.CS + mp] : make_double2(0.0, 0.0);
-    const double2 v1 = c + 1 < ncols ? cbase[(long long)(c + 1) * g.CS + mp] : make_double2(0.0, 0.0);
+    v0 = c < ncols ? cbase[(long long)c * g.CS + mp] : make_double2(0.0, 0.0);
+    v1 = c + 1 < ncols ? cbase[(long long)(c + 1) * g.CS + mp] : make_double2(0.0, 0.0);
+  };
+  auto put = [&](int t, int mp, double2 v0, double2 v1) {
     const double2 A = first_is_a ? v0 : v1, B = first_is_a ? v1 : v0;
     if (mp == 0) {
       b0s[t] = B;
@@ -194,9 +197,33 @@ __global__ void __launch_bounds__(E::NT, E::MINB) inv_beta_kernel(Geometry g, Ff
     a[t * ld + E::at(mp)] = cconj(xp);
     a[t * ld + E::at(Pn - mp)] = cconj(xn);
   };
+  auto load = [&](int t, int mp) {
+    double2 v0, v1;
+    fetch(t, mp, v0, v1);
+    put(t, mp, v0, v1);
+  };
   if constexpr (E::fixed) {  // no index division per element
-    for (int t = 0; t < E::T; t++)
-      for (int mp = threadIdx.x; mp < L; mp += E::NT) load(t, mp);
+    // an odd fixed plan of length nP is the MW circle of L = (nP + 1) / 2: all
+    // loads of a sequence are issued before its first shared-memory store
+    constexpr int LC = (E::nP + 1) / 2, NI = (LC + E::NT - 1) / E::NT;
+    if (L == LC) {
+      for (int t = 0; t < E::T; t++) {
+        double2 v0[NI], v1[NI];
+#pragma unroll
+        for (int i = 0; i < NI; i++) {
+          const int mp = threadIdx.x + i * E::NT;
+          if (mp < LC) fetch(t, mp, v0[i], v1[i]);
+        }
+#pragma unroll
+        for (int i = 0; i < NI; i++) {
+          const int mp = threadIdx.x + i * E::NT;
+          if (mp < LC) put(t, mp, v0[i], v1[i]);
+        }
+      }
+    } else {
+      for (int t = 0; t < E::T; t++)
+        for (int mp = threadIdx.x; mp < L; mp += E::NT) load(t, mp);
+    }
   } else {
     for (int idx = threadIdx.x; idx < L * T; idx += E::NT) load(idx / L, idx % L);
   }
@@ -530,10 +557,12 @@ __global__ void __launch_bounds__(E::NT, E::MINB) fwd_beta_conv_kernel(Geometry 
   const bool first_is_a = ((L - 1 + n) & 1) == 0;  // column 2q has m + n even
   const int sm0 = g.mw ? L - 1 : 0, sm1 = g.mw ? -1 : L;
   const double2* base = W + (long long)plane * g.PS;
-  for (int idx = threadIdx.x; idx < g.nb * T; idx += E::NT) {
-    const int t = idx % T, row = idx / T, c = 2 * (q0 + t);
-    const double2 v0 = c < ncols ? base[(long long)row * g.RS + c] : make_double2(0.0, 0.0);
-    const double2 v1 = c + 1 < ncols ? base[(long long)row * g.RS + c + 1] : make_double2(0.0, 0.0);
+  auto fetch = [&](int t, int row, double2& v0, double2& v1) {
+    const int c = 2 * (q0 + t);
+    v0 = c < ncols ? base[(long long)row * g.RS + c] : make_double2(0.0, 0.0);
+    v1 = c + 1 < ncols ? base[(long long)row * g.RS + c + 1] : make_double2(0.0, 0.0);
+  };
+  auto put = [&](int t, int row, double2 v0, double2 v1) {
     const double2 A = first_is_a ? v0 : v1;
     double2 B = first_is_a ? v1 : v0;
     if (row == sm0 || row == sm1) {
@@ -543,6 +572,30 @@ __global__ void __launch_bounds__(E::NT, E::MINB) fwd_beta_conv_kernel(Geometry 
     a[t * ld + E::at(row)] = cadd(A, B);
     const int mr = g.mw ? 2 * L - 2 - row : 2 * L - row;  // mirror row on the extended circle
     if (mr >= g.nb && mr < Pn) a[t * ld + E::at(mr)] = csub(A, B);
+  };
+  constexpr int LC = E::fixed ? (E::nP + 1) / 2 : 0;  // nb of the MW circle of an odd fixed plan
+  if (E::fixed && g.nb == LC) {  // all loads of a sequence before its first shared-memory store
+    constexpr int NI = E::fixed ? (LC + E::NT - 1) / E::NT : 1;
+    for (int t = 0; t < T; t++) {
+      double2 v0[NI], v1[NI];
+#pragma unroll
+      for (int i = 0; i < NI; i++) {
+        const int row = threadIdx.x + i * E::NT;
+        if (row < LC) fetch(t, row, v0[i], v1[i]);
+      }
+#pragma unroll
+      for (int i = 0; i < NI; i++) {
+        const int row = threadIdx.x + i * E::NT;
+        if (row < LC) put(t, row, v0[i], v1[i]);
+      }
+    }
+  } else {
+    for (int idx = threadIdx.x; idx < g.nb * T; idx += E::NT) {
+      const int t = idx % T, row = idx / T;
+      double2 v0, v1;
+      fetch(t, row, v0, v1);
+      put(t, row, v0, v1);
+    }
   }
   __syncthreads();
   double2* r = E::runP(a, b, T, ld, P);

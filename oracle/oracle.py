@@ -112,7 +112,8 @@ def ref():
                      "so3_core_inverse_via_ssht_real", "so3_core_forward_via_ssht_real",
                      "so3_core_inverse_direct", "so3_core_forward_direct",
                      "so3_core_inverse_direct_real", "so3_core_forward_direct_real",
-                     "so3_adjoint_inverse_direct", "so3_adjoint_forward_direct"):
+                     "so3_adjoint_inverse_direct", "so3_adjoint_forward_direct",
+                     "so3_adjoint_inverse_direct_real", "so3_adjoint_forward_direct_real"):
             getattr(R, name).argtypes = [_VP, _VP, _P]
             getattr(R, name).restype = None
         R.so3_conv_harmonic_convolution.argtypes = [_VP, _P, _VP, _P, _VP, _P]
@@ -197,6 +198,24 @@ def ref_adjoint_forward(flmn, p):
     f = np.zeros(f_size(p), np.complex128)
     flmn = np.ascontiguousarray(flmn, dtype=np.complex128)
     R.so3_adjoint_forward_direct(_ptr(f), _ptr(flmn), ctypes.byref(p))
+    return f
+
+
+def ref_adjoint_inverse_real(f, p):
+    """The reference's so3_adjoint_inverse_direct_real (src/c/so3_adjoint.c:939)."""
+    R = ref()
+    flmn = np.zeros(R.so3_sampling_flmn_size(ctypes.byref(p)), np.complex128)
+    f = np.ascontiguousarray(f, dtype=np.float64)
+    R.so3_adjoint_inverse_direct_real(_ptr(flmn), _ptr(f), ctypes.byref(p))
+    return flmn
+
+
+def ref_adjoint_forward_real(flmn, p):
+    """The reference's so3_adjoint_forward_direct_real (src/c/so3_adjoint.c:1313)."""
+    R = ref()
+    f = np.zeros(f_size(p), np.float64)
+    flmn = np.ascontiguousarray(flmn, dtype=np.complex128)
+    R.so3_adjoint_forward_direct_real(_ptr(f), _ptr(flmn), ctypes.byref(p))
     return f
 
 

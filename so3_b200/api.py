@@ -199,23 +199,35 @@ def forward(f: np.ndarray, p) -> np.ndarray:
 
 
 def adjoint_inverse(f: np.ndarray, p) -> np.ndarray:
-    """Adjoint of the inverse transform (so3_adjoint_inverse_direct,
-    reference src/c/so3_adjoint.c:34): samples -> coefficients, complex MW."""
+    """Adjoint of the inverse transform: samples -> coefficients, MW
+    (so3_adjoint_inverse_direct, reference src/c/so3_adjoint.c:34; with
+    p.reality, so3_adjoint_inverse_direct_real, :939, on real samples)."""
     q = _checked(p)
     flmn = np.zeros(flmn_size(q), np.complex128)
-    f = np.ascontiguousarray(f, dtype=np.complex128)
-    _lib.load().so3_adjoint_inverse_direct(_ptr(flmn), _ptr(f), ctypes.byref(q))
+    lib = _lib.load()
+    if q.reality:
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        lib.so3_adjoint_inverse_direct_real(_ptr(flmn), _ptr(f), ctypes.byref(q))
+    else:
+        f = np.ascontiguousarray(f, dtype=np.complex128)
+        lib.so3_adjoint_inverse_direct(_ptr(flmn), _ptr(f), ctypes.byref(q))
     _lib.check("adjoint_inverse")
     return flmn
 
 
 def adjoint_forward(flmn: np.ndarray, p) -> np.ndarray:
-    """Adjoint of the forward transform (so3_adjoint_forward_direct,
-    reference src/c/so3_adjoint.c:402): coefficients -> samples, complex MW."""
+    """Adjoint of the forward transform: coefficients -> samples, MW
+    (so3_adjoint_forward_direct, reference src/c/so3_adjoint.c:402; with
+    p.reality, so3_adjoint_forward_direct_real, :1313, to real samples)."""
     q = _checked(p)
-    f = np.zeros(f_size(q), np.complex128)
+    lib = _lib.load()
     flmn = np.ascontiguousarray(flmn, dtype=np.complex128)
-    _lib.load().so3_adjoint_forward_direct(_ptr(f), _ptr(flmn), ctypes.byref(q))
+    if q.reality:
+        f = np.zeros(f_size(q), np.float64)
+        lib.so3_adjoint_forward_direct_real(_ptr(f), _ptr(flmn), ctypes.byref(q))
+    else:
+        f = np.zeros(f_size(q), np.complex128)
+        lib.so3_adjoint_forward_direct(_ptr(f), _ptr(flmn), ctypes.byref(q))
     _lib.check("adjoint_forward")
     return f
 

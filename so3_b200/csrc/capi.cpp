@@ -200,13 +200,16 @@ int dropin_forward(void* flmn, const void* f, const so3_parameters_t* p, int rea
 
 // Adjoint transforms on host or device buffers (whole arrays staged; the
 // adjoint inverse writes every coefficient, the adjoint forward every sample).
-int dropin_adjoint(void* out, const void* in, const so3_parameters_t* p, bool inverse) {
+int dropin_adjoint(void* out, const void* in, const so3_parameters_t* p, bool inverse, int real) {
   if (!p) return so3g::fail(so3g::kInvalidParameter, "null parameters");
   int dev;
   if (int rc = current_device(&dev)) return rc;
   DropIn* X = dropin(dev);
   std::lock_guard<std::mutex> lk(X->mu);
-  const size_t fb = f_bytes(p, 0), lb = flmn_bytes(p, 0);
+  so3_parameters_t q = *p;  // the entry point decides the layout, as the reference's do
+  q.reality = real;
+  p = &q;
+  const size_t fb = f_bytes(p, real), lb = flmn_bytes(p, real);
   void *din = nullptr, *dout = nullptr;
   bool sin = false, sout = false;
   if (int rc = device_view(X, 0, in, inverse ? fb : lb, true, &din, &sin)) return rc;
@@ -272,10 +275,16 @@ void so3_core_forward_direct_real(cd* flmn, const double* f, const so3_parameter
 
 // ------------------------------------------------------------ drop-in adjoint
 void so3_adjoint_inverse_direct(cd* flmn, const cd* f, const so3_parameters_t* p) {
-  finish(dropin_adjoint(flmn, f, p, true));
+  finish(dropin_adjoint(flmn, f, p, true, 0));
 }
 void so3_adjoint_forward_direct(cd* f, const cd* flmn, const so3_parameters_t* p) {
-  finish(dropin_adjoint(f, flmn, p, false));
+  finish(dropin_adjoint(f, flmn, p, false, 0));
+}
+void so3_adjoint_inverse_direct_real(cd* flmn, const double* f, const so3_parameters_t* p) {
+  finish(dropin_adjoint(flmn, f, p, true, 1));
+}
+void so3_adjoint_forward_direct_real(double* f, const cd* flmn, const so3_parameters_t* p) {
+  finish(dropin_adjoint(f, flmn, p, false, 1));
 }
 
 // ------------------------------------------------------------ drop-in conv

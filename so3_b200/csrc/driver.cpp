@@ -743,15 +743,17 @@ int run_forward_ragged(Device* D, Workspace* wk, const so3_parameters_t* ps, int
 
 // ------------------------------------------------------------ adjoint transforms
 // Adjoints of the inverse and forward transforms (reference
-// src/c/so3_adjoint.c:34-400, :402-938; complex MW).  The reference's FFT
-// normalisations are folded into one contraction weight: the adjoint
-// inverse's analysis DFTs over gamma and alpha carry 2 pi/(2N-1) and
-// 1/(2L-1) (the forward stages'), undone in the forward contraction's
-// (2l+1)/(8 pi^2) weight; the adjoint forward's 1/((2L-1)(2N-1)) rides on the
-// inverse contraction.
+// src/c/so3_adjoint.c:34-400, :402-938 complex; :939-1312, :1313-1841 real,
+// MW).  The reference's FFT normalisations are folded into one contraction
+// weight: the adjoint inverse's analysis DFTs over gamma and alpha carry
+// 2 pi/(2N-1) and 1/(2L-1) (the forward stages'), undone in the forward
+// contraction's (2l+1)/(8 pi^2) weight; the adjoint forward's
+// 1/((2L-1)(2N-1)) rides on the inverse contraction.  Real signals: planes
+// n >= 0, r2c over gamma in the adjoint inverse (the reference's 2-D r2c over
+// alpha and gamma), c2r in the adjoint forward (its 2-D c2r: the inverse DFT
+// over alpha, then c2r over gamma with the imaginary part of n = 0 dropped).
 static int adjoint_check(const so3_parameters_t& p) {
-  if (int rc = validate(p, 0)) return rc;
-  if (p.reality) return fail(kUnsupported, "adjoint transforms: complex signals only on the GPU path");
+  if (int rc = validate(p, p.reality ? 1 : 0)) return rc;
   if (p.sampling_scheme != SO3_SAMPLING_MW) return fail(kUnsupported, "adjoint transforms: MW sampling only");
   if (p.steerable) return fail(kUnsupported, "adjoint transforms: steerable signals are not supported");
   return kOk;
@@ -760,12 +762,13 @@ static int adjoint_check(const so3_parameters_t& p) {
 int run_adjoint_inverse(Device* D, Workspace* wk, const so3_parameters_t& p, const void* f_d, void* flmn_d,
                         cudaStream_t s) {
   if (int rc = adjoint_check(p)) return rc;
+  const int real = p.reality ? 1 : 0;
   Resources r;
-  if (int rc = acquire(D, p, 0, s, &r, false)) return rc;
+  if (int rc = acquire(D, p, real, s, &r, false)) return rc;
   void* ws = nullptr;
-  if (int rc = ensure_ws(wk, workspace_bytes(p, 0), &ws)) return rc;
+  if (int rc = ensure_ws(wk, workspace_bytes(p, real), &ws)) return rc;
   double2* W = static_cast<double2*>(ws);
-  if (int rc = ensure_tuned(D, p, 0, &r, W, s)) return rc;
+  if (int rc = ensure_tuned(D, p, real, &r, W, s)) return rc;
   // every coefficient starts at zero (so3_adjoint.c:234-243): skipped n-blocks and l < L0 stay zero
   SO3G_CUDA(cudaMemsetAsync(flmn_d, 0, (size_t)so3_sampling_flmn_size(&p) * sizeof(double2), s));
   int rc;
@@ -781,12 +784,13 @@ int run_adjoint_inverse(Device* D, Workspace* wk, const so3_parameters_t& p, con
 int run_adjoint_forward(Device* D, Workspace* wk, const so3_parameters_t& p, const void* flmn_d, void* f_d,
                         cudaStream_t s) {
   if (int rc = adjoint_check(p)) return rc;
+  const int real = p.reality ? 1 : 0;
   Resources r;
-  if (int rc = acquire(D, p, 0, s, &r, true)) return rc;
+  if (int rc = acquire(D, p, real, s, &r, true)) return rc;
   void* ws = nullptr;
-  if (int rc = ensure_ws(wk, workspace_bytes(p, 0), &ws)) return rc;
+  if (int rc = ensure_ws(wk, workspace_bytes(p, real), &ws)) return rc;
   double2* W = static_cast<double2*>(ws);
-  if (int rc = ensure_tuned(D, p, 0, &r, W, s)) return rc;
+  if (int rc = ensure_tuned(D, p, real, &r, W, s)) return rc;
   int rc;
   const double wconst = 1.0 / ((double)(2 * p.L - 1) * (2 * p.N - 1));
   if ((rc = launch_inverse_contract(r.g, p.n_mode, static_cast<const double2*>(flmn_d), r.bases, r.dl, W, 0, s, 0,

@@ -656,9 +656,10 @@ __global__ void __launch_bounds__(E::NT, E::MINB) fwd_beta_conv_kernel(Geometry 
 }
 
 // ------------------------------------------------------------------ adjoint
-// Beta stages of the adjoint transforms (reference src/c/so3_adjoint.c,
-// complex MW).  Generic engines only (any length); one column (plane n,
-// order m, s = (-1)^{m+n}) per sequence.
+// Beta stages of the adjoint transforms (reference src/c/so3_adjoint.c, MW;
+// complex planes n = -(N-1)..N-1 or real planes n >= 0).  Generic engines
+// only (any length); one column (plane n, order m, s = (-1)^{m+n}) per
+// sequence.
 //
 // Inverse adjoint (so3_adjoint.c:190-231): the nb beta samples zero-extended
 // onto the 2L-1 circle, forward DFT, phase e^{-i m' pi/(2L-1)}, folded
@@ -1025,14 +1026,14 @@ int adj_fwd_beta(const Geometry& g, const FftPlan& p, const FftPlan& pc, const d
 }  // namespace
 
 int launch_adj_inv_beta(const Geometry& g, const FftPlan& p, double2* W, cudaStream_t s) {
-  if (!g.mw || g.real) return fail(kUnsupported, "adjoint transforms: complex MW sampling only");
+  if (!g.mw) return fail(kUnsupported, "adjoint transforms: MW sampling only");
   const int rc = p.big() ? adj_inv_beta<Gen<true>>(g, p, W, s) : adj_inv_beta<Gen<false>>(g, p, W, s);
   return rc ? rc : launched();
 }
 
 int launch_adj_fwd_beta(const Geometry& g, const FftPlan& p, const FftPlan& pc, const double2* wr, double2* W,
                         cudaStream_t s) {
-  if (!g.mw || g.real) return fail(kUnsupported, "adjoint transforms: complex MW sampling only");
+  if (!g.mw) return fail(kUnsupported, "adjoint transforms: MW sampling only");
   const int rc = (p.big() || pc.big()) ? adj_fwd_beta<Gen<true>>(g, p, pc, wr, W, s)
                                        : adj_fwd_beta<Gen<false>>(g, p, pc, wr, W, s);
   return rc ? rc : launched();

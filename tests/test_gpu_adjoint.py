@@ -1,5 +1,6 @@
 """Adjoint transforms (reference src/c/so3_adjoint.c:34 so3_adjoint_inverse_direct,
-:402 so3_adjoint_forward_direct; complex MW) through the drop-in C ABI:
+:402 so3_adjoint_forward_direct, :939 / :1313 their _real variants; MW) through
+the drop-in C ABI:
 
 * against the reference's own C (oracle/_ref, compiled unmodified) on the
   same seeded inputs, 1e-12 normwise relative error;
@@ -48,6 +49,33 @@ def test_adjoint_edge_sizes_against_reference_c(O, L, N):
     assert rel_err(so3.adjoint_forward(fl, p), O.ref_adjoint_forward(fl, op)) < TOL
 
 
+@pytest.mark.parametrize("order,storage,mode,method", CASES)
+def test_real_adjoints_against_reference_c(O, order, storage, mode, method):
+    if O.ref() is None:
+        pytest.skip("reference C (oracle/_ref) not built")
+    p = params(9, 5, L0=1 if mode == 0 else 0, reality=1, order=order, storage=storage, mode=mode,
+               method=method)
+    op = oparams(O, p)
+    rng = np.random.default_rng(31 + mode)
+    f = rng.normal(size=O.f_size(op))
+    assert rel_err(so3.adjoint_inverse(f, p), O.ref_adjoint_inverse_real(f, op)) < TOL
+    fl = rng.normal(size=so3.flmn_size(p)) + 1j * rng.normal(size=so3.flmn_size(p))
+    assert rel_err(so3.adjoint_forward(fl, p), O.ref_adjoint_forward_real(fl, op)) < TOL
+
+
+@pytest.mark.parametrize("L,N", [(1, 1), (2, 2), (16, 1), (33, 7), (64, 16)])
+def test_real_adjoint_edge_sizes_against_reference_c(O, L, N):
+    if O.ref() is None:
+        pytest.skip("reference C (oracle/_ref) not built")
+    p = params(L, N, reality=1)
+    op = oparams(O, p)
+    rng = np.random.default_rng(3 * L + N)
+    f = rng.normal(size=O.f_size(op))
+    assert rel_err(so3.adjoint_inverse(f, p), O.ref_adjoint_inverse_real(f, op)) < TOL
+    fl = rng.normal(size=so3.flmn_size(p)) + 1j * rng.normal(size=so3.flmn_size(p))
+    assert rel_err(so3.adjoint_forward(fl, p), O.ref_adjoint_forward_real(fl, op)) < TOL
+
+
 @pytest.mark.parametrize("L,N", [(64, 64), (128, 8)])
 def test_adjoint_identity_with_gpu_transforms(L, N):
     p = params(L, N)
@@ -63,7 +91,7 @@ def test_adjoint_identity_with_gpu_transforms(L, N):
     assert abs(lhs - rhs) / abs(lhs) < 1e-12
 
 
-@pytest.mark.parametrize("kw", [dict(sampling=1), dict(reality=1), dict(steerable=1)])
+@pytest.mark.parametrize("kw", [dict(sampling=1), dict(sampling=1, reality=1), dict(steerable=1)])
 def test_adjoint_rejects_unsupported(kw):
     p = params(8, 4, **kw)
     with pytest.raises(so3.SO3Error, match="status 3"):

@@ -53,7 +53,9 @@ int so3gpu_forward_real(so3gpu_context *ctx, void *flmn, const double *f,
  * (7-slice Ozaki split, exact int32 accumulation, FP64 recombination) while
  * Delta, the quadrature weights and every DFT stay FP64; normwise relative
  * error against the FP64 path below 1e-10 (about 1e-12 measured).  Real
- * signals (parameters->reality) always use the FP64 path.  The batch
+ * signals (parameters->reality) take the split contractions over their planes
+ * n >= 0 and the FP64 forward beta stage; real signals with N = 1 use the
+ * FP64 path.  The batch
  * workspace holds `count` scratch plane sets plus the sliced operands
  * (about 0.9 GB per group of 8 signals at L = 512, N = 64). */
 #define SO3GPU_PRECISION_FP64 0

@@ -377,8 +377,14 @@ int upload_table(void* dst, const void* const* ptrs, int nsig, cudaStream_t s) {
 
 }  // namespace
 
+// Real signals take the split contractions too (planes n >= 0, the tensor-core
+// columns of the combinations with n = -nu stay empty), except N = 1, whose
+// FP64 inverse symmetrises the single plane (the reference's real spin
+// transform for n = 0).
+static bool split_real_ok(const so3_parameters_t& p, int real) { return !real || p.N > 1; }
+
 size_t batch_workspace_bytes(const so3_parameters_t& p, int real, int nsig, int precision) {
-  if (precision == kPrecFp64 || real || nsig <= 0) return workspace_bytes(p, real);
+  if (precision == kPrecFp64 || !split_real_ok(p, real) || nsig <= 0) return workspace_bytes(p, real);
   return batch_layout(make_geometry(p, real), p, real, nsig).total;
 }
 
@@ -386,7 +392,7 @@ int run_inverse_batch(Device* D, Workspace* wk, const so3_parameters_t& p, int r
                       const void* const* flmn_d, void* const* f_d, int precision, cudaStream_t s) {
   if (nsig < 0) return fail(kInvalidParameter, "negative batch size");
   if (precision != kPrecFp64 && precision != kPrecMixedInt8) return fail(kInvalidParameter, "unknown precision");
-  if (precision == kPrecFp64 || real) {
+  if (precision == kPrecFp64 || !split_real_ok(p, real)) {
     for (int b = 0; b < nsig; b++)
       if (int rc = run_inverse(D, wk, p, flmn_d[b], f_d[b], real, s)) return rc;
     return kOk;
@@ -431,7 +437,7 @@ int run_forward_batch(Device* D, Workspace* wk, const so3_parameters_t& p, int r
                       void* const* flmn_d, int precision, cudaStream_t s) {
   if (nsig < 0) return fail(kInvalidParameter, "negative batch size");
   if (precision != kPrecFp64 && precision != kPrecMixedInt8) return fail(kInvalidParameter, "unknown precision");
-  if (precision == kPrecFp64 || real) {
+  if (precision == kPrecFp64 || !split_real_ok(p, real)) {
     for (int b = 0; b < nsig; b++)
       if (int rc = run_forward(D, wk, p, f_d[b], flmn_d[b], real, s)) return rc;
     return kOk;

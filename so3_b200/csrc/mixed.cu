@@ -139,6 +139,7 @@ struct MixArgs {
   const long long* pair_off;  // first block of each pair in tab
   long long wstride;
   int L, N, L0, nchunk, MT, plane0, n_mode, nsig, compact;
+  int real;          // real signals: planes n >= 0 only, combinations with n = -nu are empty
   long long CS, QS;  // column-major scratch strides
 };
 
@@ -316,7 +317,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_tc_kernel(MixArgs a) {
     const int c = 32 * lq + lane;
     const int b = c >> 3, combo = (c >> 1) & 3, part = c & 1;
     const int ms = (combo & 1) ? -1 : 1, ns = (combo & 2) ? -1 : 1;
-    const bool valid_combo = !((ms < 0 && mu == 0) || (ns < 0 && nu == 0));
+    const bool valid_combo = !((ms < 0 && mu == 0) || (ns < 0 && nu == 0) || (a.real && ns < 0));
     const int m = ms * mu, n = ns * nu;
     const int sig = grp * kSig + b;
     const bool one_neg = ms * ns < 0;
@@ -330,8 +331,11 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_tc_kernel(MixArgs a) {
     double2* Wout = nullptr;
     double2* F = nullptr;
     long long blk = 0;
-    if (!FWD) Wout = a.W + (long long)sig * a.wstride + (long long)(a.plane0 + n) * a.QS + (long long)(m + L - 1) * a.CS;
-    else if (sig < a.nsig) {
+    // empty combinations (real signals: n = -nu) have no plane: nothing is read or written for them
+    if (!FWD) {
+      if (valid_combo)
+        Wout = a.W + (long long)sig * a.wstride + (long long)(a.plane0 + n) * a.QS + (long long)(m + L - 1) * a.CS;
+    } else if (sig < a.nsig && valid_combo) {
       F = a.flmn[sig];
       blk = a.base[a.plane0 + n];
     }
@@ -420,6 +424,7 @@ struct SliceArgs {
   const long long* base;
   long long wstride;
   int L, N, L0, nchunk, plane0, n_mode, nsig, npairs;
+  int real;  // real signals: planes n >= 0 only
   long long CS, QS;
 };
 
@@ -454,7 +459,7 @@ __device__ __forceinline__ InvColumn inv_column(const SliceArgs& a, int sig, int
   const int ms = (combo & 1) ? -1 : 1, ns = (combo & 2) ? -1 : 1;
   const int m = ms * mu, n = ns * nu;
   InvColumn c;
-  c.act = mu < a.L && sig < a.nsig && !(ms < 0 && mu == 0) && !(ns < 0 && nu == 0) &&
+  c.act = mu < a.L && sig < a.nsig && !(ms < 0 && mu == 0) && !(ns < 0 && nu == 0) && !(a.real && ns < 0) &&
           !plane_skipped(a.n_mode, a.N, n);
   c.lmin = max(max(mu, nu), a.L0);
   c.flip = ms * ns < 0;
@@ -574,7 +579,8 @@ __device__ __forceinline__ FwdColumn fwd_column(const SliceArgs& a, int sig, int
   const int ms = (combo & 1) ? -1 : 1, ns = (combo & 2) ? -1 : 1;
   const int m = ms * mu, n = ns * nu;
   FwdColumn c;
-  c.act = sig < a.nsig && !(ms < 0 && mu == 0) && !(ns < 0 && nu == 0) && !plane_skipped(a.n_mode, a.N, n);
+  c.act = sig < a.nsig && !(ms < 0 && mu == 0) && !(ns < 0 && nu == 0) && !(a.real && ns < 0) &&
+          !plane_skipped(a.n_mode, a.N, n);
   c.flip = ms * ns < 0;
   c.src = c.act ? a.W + (long long)sig * a.wstride + (long long)(a.plane0 + n) * a.QS + (long long)(m + a.L - 1) * a.CS
                 : nullptr;
@@ -889,7 +895,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_tcp_kernel(MixArgs a, int n
       if (!it.valid) continue;
       // per-item metadata first: these loads overlap the wait for the products
       const int mu = it.mu, nu = it.nu, L = a.L, r0 = it.t * kN;
-      const bool valid_combo = !((ms < 0 && mu == 0) || (ns < 0 && nu == 0));
+      const bool valid_combo = !((ms < 0 && mu == 0) || (ns < 0 && nu == 0) || (a.real && ns < 0));
       const int m = ms * mu, n = ns * nu;
       const int sig = it.grp * kSig + b;
       const bool one_neg = ms * ns < 0;
@@ -900,8 +906,11 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_tcp_kernel(MixArgs a, int n
       double2* Wout = nullptr;
       double2* F = nullptr;
       long long blk = 0;
-      if (!FWD) Wout = a.W + (long long)sig * a.wstride + (long long)(a.plane0 + n) * a.QS + (long long)(m + L - 1) * a.CS;
-      else if (sig < a.nsig) {
+      // empty combinations (real signals: n = -nu) have no plane: nothing is read or written for them
+      if (!FWD) {
+        if (valid_combo)
+          Wout = a.W + (long long)sig * a.wstride + (long long)(a.plane0 + n) * a.QS + (long long)(m + L - 1) * a.CS;
+      } else if (sig < a.nsig && valid_combo) {
         F = a.flmn[sig];
         blk = a.base[a.plane0 + n];
       }
@@ -1630,12 +1639,12 @@ static int mixed_args(const Geometry& g, int n_mode, int nsig, void* scratch, Mi
   m->xs = xs;
   m->xscale = xscale;
   m->L = g.L, m->N = g.N, m->L0 = g.L0, m->nchunk = nc, m->MT = MT, m->plane0 = g.plane0, m->n_mode = n_mode;
-  m->nsig = nsig, m->CS = g.CS, m->QS = g.QS;
+  m->nsig = nsig, m->CS = g.CS, m->QS = g.QS, m->real = g.real;
   *s = SliceArgs{};
   s->xs = xs;
   s->xscale = xscale;
   s->L = g.L, s->N = g.N, s->L0 = g.L0, s->nchunk = nc, s->plane0 = g.plane0, s->n_mode = n_mode;
-  s->nsig = nsig, s->npairs = (int)pairs, s->CS = g.CS, s->QS = g.QS;
+  s->nsig = nsig, s->npairs = (int)pairs, s->CS = g.CS, s->QS = g.QS, s->real = g.real;
   return kOk;
 }
 
@@ -1755,7 +1764,7 @@ int launch_mixed_inverse(const Geometry& g, int n_mode, const double2* const* fl
                          const long long* bases, const double* dl, const DigitTable* tab, double2* W,
                          long long wstride, void* scratch, cudaStream_t s, const double2* conv_flm,
                          const double2* const* conv_glm) {
-  if (g.real) return fail(kUnsupported, "split-precision contractions take complex signals");
+  if (g.real && conv_flm) return fail(kUnsupported, "split-precision convolution: complex signals only");
   MixArgs m;
   SliceArgs sa;
   if (int rc = mixed_args(g, n_mode, nsig, scratch, &m, &sa)) return rc;
@@ -1779,7 +1788,6 @@ int launch_mixed_inverse(const Geometry& g, int n_mode, const double2* const* fl
 int launch_mixed_forward(const Geometry& g, int n_mode, const double2* W, long long wstride, int nsig,
                          const long long* bases, const double* dl, const DigitTable* tab, double2* const* flmn_dev,
                          int storage_compact, void* scratch, cudaStream_t s) {
-  if (g.real) return fail(kUnsupported, "split-precision contractions take complex signals");
   MixArgs m;
   SliceArgs sa;
   if (int rc = mixed_args(g, n_mode, nsig, scratch, &m, &sa)) return rc;

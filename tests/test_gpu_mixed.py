@@ -77,9 +77,37 @@ def test_mixed_fp64_batch_equals_single_transforms():
         assert np.array_equal(o.cpu().numpy(), ref.cpu().numpy())
 
 
-def test_mixed_real_signals_use_fp64():
+REAL_CASES = [
+    dict(L=32, N=8, nsig=3),
+    dict(L=24, N=5, nsig=9, order=0, storage=1, L0=2),  # compact, zero-first, L0 > 0
+    dict(L=40, N=3, nsig=18),                           # two groups of 16 signals
+    dict(L=20, N=6, nsig=4, mode=1),                    # even n only
+    dict(L=33, N=4, nsig=5, sampling=1, method=1),      # MWSS, Trapani
+]
+
+
+@pytest.mark.parametrize("kw", REAL_CASES, ids=[str(i) for i in range(len(REAL_CASES))])
+def test_mixed_real_batch_matches_fp64(kw):
+    """Real signals: split contractions over the planes n >= 0 (the columns of
+    the n = -nu combinations stay empty), FP64 DFT stages with r2c / c2r over
+    gamma; every result against the FP64 path, and the round trip."""
+    kw = dict(kw)
+    nsig = kw.pop("nsig")
+    L, N = kw.pop("L"), kw.pop("N")
+    p = params(L, N, reality=1, **kw)
+    fls, f64, fmx, b64, bmx = _run(p, nsig, 41)
+    for i in range(nsig):
+        assert rel_err(fmx[i], f64[i]) < TOL_MIXED, (i, rel_err(fmx[i], f64[i]))
+        assert rel_err(bmx[i], b64[i]) < TOL_MIXED, (i, rel_err(bmx[i], b64[i]))
+        if p.n_mode == 0:
+            assert rel_err(bmx[i], fls[i]) < 1e-10  # round trip
+
+
+def test_mixed_real_single_plane_uses_fp64():
+    """N = 1 real signals stay on the FP64 path (its inverse symmetrises the
+    single plane): results bit-identical to precision "fp64"."""
     import torch
-    p = params(24, 6, reality=1)
+    p = params(24, 1, reality=1)
     ctx = so3.Context(0)
     fls = [torch.from_numpy(synth.gen_flmn(p, 3 + i)).cuda() for i in range(2)]
     a = ctx.inverse_batch(fls, p, "fp64")

@@ -55,9 +55,9 @@ int so3gpu_forward_real(so3gpu_context *ctx, void *flmn, const double *f,
  * error against the FP64 path below 1e-10 (about 1e-12 measured).  Real
  * signals (parameters->reality) take the split contractions over their planes
  * n >= 0 and the FP64 forward beta stage; real signals with N = 1 use the
- * FP64 path.  The batch
- * workspace holds `count` scratch plane sets plus the sliced operands
- * (about 0.9 GB per group of 8 signals at L = 512, N = 64). */
+ * FP64 path.  The batch workspace holds `count` scratch plane sets (2.13 GB
+ * each at L = 512, N = 64) plus the sliced operands (15.0 GB per group of 16
+ * signals at L = 512, N = 64) and the column scales. */
 #define SO3GPU_PRECISION_FP64 0
 #define SO3GPU_PRECISION_MIXED_INT8 1
 int so3gpu_inverse_batch(so3gpu_context *ctx, void *const *f, const void *const *flmn, int count,

@@ -566,6 +566,122 @@ __global__ void __launch_bounds__(256, 3) slice_inv_kernel(SliceArgs a) {
   }
 }
 
+// Streaming form of the inverse slicing (uniform batches of plain
+// coefficients, L <= 1024): the caller's flmn is read in storage order, where
+// the entries l^2 + l + m of a row l are contiguous in m, so consecutive
+// threads read consecutive addresses and a CTA reads whole rows of one plane.
+// Pass 1 (inv_colscale_kernel) finds the scale of every column (n, m, part);
+// pass 2 (inv_digit_kernel) cuts one 16-entry reduction slot of every column
+// of a plane into digits.  Both give the same scales and digits as
+// slice_inv_kernel (same arithmetic per entry).  Column (n, m) is row
+// 8 (signal % 16) + 2 combo (+ part) of pair (|m|, |n|), combo bit 0: m < 0,
+// bit 1: n < 0; the (-1)^l of combinations with one negative index is applied
+// on the entry.
+constexpr int kStreamThreads = 256;
+
+// Pass 1: one CTA per (plane, signal); thread t owns the columns m = t - (L-1)
+// + 256 k (k < OWN) and walks the rows l >= max(|n|, L0) four at a time.
+// Skipped planes are left to pass 2 (zero digits, scale 1).
+template <int OWN>
+__global__ void __launch_bounds__(kStreamThreads) inv_colscale_kernel(SliceArgs a, double* colscl, int nplanes) {
+  const int p = blockIdx.x, sig = blockIdx.y, L = a.L, n = p - a.plane0, t = threadIdx.x;
+  const int ncol = 2 * L - 1;
+  if (plane_skipped(a.n_mode, a.N, n)) return;
+  const double2* src = a.flmn[sig] + a.base[p];
+  double mr[OWN], mi[OWN];
+  int mm[OWN];
+#pragma unroll
+  for (int k = 0; k < OWN; k++) mr[k] = mi[k] = 0.0, mm[k] = t + kStreamThreads * k - (L - 1);
+  for (int l = max(abs(n), a.L0); l < L; l += 4) {
+    double2 x[4][OWN];
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+#pragma unroll
+      for (int k = 0; k < OWN; k++) {
+        const int ll = l + u, m = mm[k];
+        x[u][k] = (ll < L && m <= L - 1 && abs(m) <= ll) ? __ldg(src + (long long)ll * ll + ll + m)
+                                                          : make_double2(0.0, 0.0);
+      }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const double w = (2.0 * (l + u) + 1.0) * kInv8Pi2;
+#pragma unroll
+      for (int k = 0; k < OWN; k++) {
+        mr[k] = fmax(mr[k], fabs(x[u][k].x * w));
+        mi[k] = fmax(mi[k], fabs(x[u][k].y * w));
+      }
+    }
+  }
+  double* out = colscl + ((size_t)sig * nplanes + p) * (size_t)ncol * 2;
+#pragma unroll
+  for (int k = 0; k < OWN; k++) {
+    const int m = mm[k];
+    if (m <= L - 1) {
+      out[2 * (m + L - 1)] = scale_of(mr[k]);
+      out[2 * (m + L - 1) + 1] = scale_of(mi[k]);
+    }
+  }
+}
+
+// Pass 2: one CTA per (reduction slot kb of 16 entries, nu = |n|, signal);
+// thread t takes the sign combination t % 4 of the columns mu = t / 4 + 64 k:
+// the four lanes of a mu write the 4 x 32 contiguous bytes of the signal's 8
+// rows of the pair's image per digit plane (rows c, c+1: both parts), and the
+// 8 mu of a warp read 128-byte runs of each row l of the planes +-nu.
+// Slots of chunks below the one holding l = max(mu, nu, L0) are never read by
+// the products and are not written; the column scales are written by the
+// first written slot.
+__global__ void __launch_bounds__(kStreamThreads, 2) inv_digit_kernel(SliceArgs a, const double* colscl, int nplanes) {
+  const int kb = blockIdx.x, nu = blockIdx.y, sig = blockIdx.z, combo = threadIdx.x & 3;
+  const int L = a.L, ncol = 2 * L - 1;
+  const int ms = (combo & 1) ? -1 : 1, ns = (combo & 2) ? -1 : 1, n = ns * nu, p = a.plane0 + n;
+  if ((ns < 0 && nu == 0) || (a.real && ns < 0)) return;  // no such plane (whole warps: combo is lane % 4)
+  const bool skipped = plane_skipped(a.n_mode, a.N, n);
+  const bool flip = ms * ns < 0;
+  const int grp = sig / kSig, b = sig % kSig, c = 8 * b + 2 * combo;
+  const double2* src = a.flmn[sig] + a.base[p];
+  const double* scl = colscl + ((size_t)sig * nplanes + p) * (size_t)ncol * 2;
+  for (int mu = (int)threadIdx.x / 4; mu < L; mu += kStreamThreads / 4) {
+    const int m = ms * mu, lmin = max(max(mu, nu), a.L0);
+    if ((ms < 0 && mu == 0) || 16 * kb / kKC < lmin / kKC) continue;
+    const double sr = skipped ? 1.0 : scl[2 * (m + L - 1)];
+    const double si = skipped ? 1.0 : scl[2 * (m + L - 1) + 1];
+    const size_t gp = (size_t)grp * a.npairs + (size_t)mu * a.N + nu;
+    if (kb == 4 * (lmin / kKC)) {
+      a.xscale[gp * kM + c] = sr;
+      a.xscale[gp * kM + c + 1] = si;
+    }
+    double2 x[16];
+#pragma unroll
+    for (int e = 0; e < 16; e++) {
+      const int l = 16 * kb + e;
+      x[e] = (!skipped && l < L && l >= lmin) ? __ldg(src + (long long)l * l + l + m) : make_double2(0.0, 0.0);
+    }
+    uint8_t* dst = a.xs + gp * (size_t)a.nchunk * kXStage + (size_t)(kb >> 2) * kXStage + tile_off(kM, c, (kb & 3) * 16);
+#pragma unroll
+    for (int part = 0; part < 2; part++) {
+      const double inv = 1.0 / (part ? si : sr);
+      uint32_t d[4][kS];
+#pragma unroll
+      for (int qd = 0; qd < 4; qd++) {
+        double r[4];
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          const int l = 16 * kb + 4 * qd + e;
+          const double f = (2.0 * l + 1.0) * kInv8Pi2;
+          double v = (part ? x[4 * qd + e].y : x[4 * qd + e].x) * f;
+          if (flip && (l & 1)) v = -v;
+          r[e] = v * inv;
+        }
+        split_pack4(r, d[qd]);
+      }
+#pragma unroll
+      for (int i = 0; i < kS; i++)
+        *reinterpret_cast<uint4*>(dst + 16 * part + i * (kM * kKC)) = make_uint4(d[0][i], d[1][i], d[2][i], d[3][i]);
+    }
+  }
+}
+
 // Forward.  One CTA per (pair, kSigPer signals): complex columns cc = 4 *
 // signal + combo (rows 8 kSigPer q .. of the pair's stage image for the
 // q-th set of kSigPer signals of the group); warp <-> column, lanes along m'
@@ -1103,6 +1219,81 @@ __global__ void __launch_bounds__(256) beta_slice_kernel(BetaArgs a) {
   }
 }
 
+// Single-read form (at most 512 reduction rows): one CTA per (group of 8
+// consecutive columns m0 .. m0+7 of a plane, signal), i.e. 4 columns of each
+// parity class, rows c = 8 (q mod 16) .. +7 of column tile q / 16 of both
+// classes.  The CTA's beta samples (128-byte row segments) are read from HBM
+// once into shared memory; the 16 column scales and the digits come from
+// there.  Same scales and digits as beta_slice_kernel.
+constexpr int kBsCols = 8;
+__global__ void __launch_bounds__(256, 3) beta_slice1_kernel(BetaArgs a, int ntiles) {
+  extern __shared__ __align__(16) unsigned char bsraw[];
+  const int L = a.L, rows = a.nchunk * kKC, tot = rows * kBsCols;
+  double2* st = reinterpret_cast<double2*>(bsraw);               // [row][kBsCols]
+  double* red = reinterpret_cast<double*>(bsraw + (size_t)tot * sizeof(double2));  // [8 warps][16]
+  double* scl = red + 8 * 16;                                      // [16]
+  const int qpp = 16 * a.ct, q = blockIdx.x % qpp, p = blockIdx.x / qpp, sig = blockIdx.y;
+  const int n = p - a.plane0, m0 = -(L - 1) + kBsCols * q;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const double2* src = a.W + (long long)sig * a.wstride + (long long)p * a.PS + (m0 + L - 1);
+  for (int base = 0; base < tot; base += 256 * 16) {
+    double2 v[16];
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+      const int idx = base + 256 * u + tid, r = idx >> 3, col = idx & 7;
+      v[u] = (idx < tot && r < L && m0 + col <= L - 1) ? __ldg(src + (long long)r * a.RS + col) : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+      const int idx = base + 256 * u + tid;
+      if (idx < tot) st[idx] = v[u];
+    }
+  }
+  __syncthreads();
+  {
+    // (column, part) cp = tid % 16; rows tid / 16 + 16 i
+    const int cp = tid & 15;
+    const double* sd = reinterpret_cast<const double*>(st);
+    double mx = 0.0;
+    for (int r = tid >> 4; r < rows; r += 16) mx = fmax(mx, fabs(sd[2 * (r * kBsCols + (cp >> 1)) + (cp & 1)]));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 16));
+    if (lane < 16) red[warp * 16 + cp] = mx;
+  }
+  __syncthreads();
+  if (tid < 16) {
+    double mx = 0.0;
+#pragma unroll
+    for (int w = 0; w < 8; w++) mx = fmax(mx, red[w * 16 + tid]);
+    int ex = 0;
+    frexp(mx, &ex);
+    scl[tid] = mx > 0.0 ? ldexp(1.0, ex + 1) : 1.0;
+  }
+  __syncthreads();
+  const int nslot = rows / 16;
+  for (int w = tid; w < 16 * nslot; w += 256) {
+    const int cp = w & 15, kb = w >> 4, col = cp >> 1, part = cp & 1;
+    const int m = m0 + col, sc = (m + n) & 1;
+    const int jj = 4 * (q & 15) + (col >> 1), c = 2 * jj + part;
+    const int tile = q / 16 + a.ct * (sc + 2 * p);
+    const size_t gt = (size_t)sig * ntiles + tile;
+    const double scale = scl[cp], inv = 1.0 / scale;
+    if (kb == 0) a.xscale[gt * kM + c] = scale;
+    const double* sd = reinterpret_cast<const double*>(st) + part;
+    uint32_t d[4][kS];
+#pragma unroll
+    for (int qd = 0; qd < 4; qd++) {
+      double r[4];
+#pragma unroll
+      for (int e = 0; e < 4; e++) r[e] = sd[2 * ((16 * kb + 4 * qd + e) * kBsCols + col)] * inv;
+      split_pack4(r, d[qd]);
+    }
+    uint8_t* dst = a.xs + gt * (size_t)a.nchunk * kXStage + (size_t)(kb >> 2) * kXStage + tile_off(kM, c, (kb & 3) * 16);
+#pragma unroll
+    for (int i = 0; i < kS; i++)
+      *reinterpret_cast<uint4*>(dst + i * (kM * kKC)) = make_uint4(d[0][i], d[1][i], d[2][i], d[3][i]);
+  }
+}
+
 // Persistent: one CTA per SM walks the items (64-row tile t of m', column
 // tile, signal), t fastest: the MT items of one column tile run on
 // neighbouring CTAs at the same time, so its digits come from HBM once and
@@ -1623,9 +1814,23 @@ bool mixed_beta_supported(const Geometry& g);
 
 // Sliced operands of the contractions and of the forward beta products (the
 // two never live at the same time, so they share one region).
+// The single-read slicing kernels (inv_colscale + inv_digit, beta_slice1) are
+// the default; SO3GPU_STREAM_SLICE=0 selects the per-pair kernels
+// (slice_inv_kernel, beta_slice_kernel), which write the same digits.
+static bool stream_slicing() {
+  const char* e = getenv("SO3GPU_STREAM_SLICE");
+  return !(e && e[0] == '0');
+}
+
+// Column scales of the streaming inverse slicing: [signal][plane][2L-1][part].
+static size_t colscale_bytes(const Geometry& g, int nsig) {
+  return (size_t)nsig * (g.real ? g.N : 2 * g.N - 1) * (2 * (size_t)g.L - 1) * 2 * sizeof(double);
+}
+
 size_t mixed_scratch_bytes(const Geometry& g, int nsig) {
   const size_t groups = (nsig + kSig - 1) / kSig, pairs = (size_t)g.L * g.N;
-  const size_t contr = groups * pairs * ((size_t)nchunks(g) * kXStage + kM * sizeof(double)) + 256;
+  const size_t contr = ((groups * pairs * nchunks(g) * (size_t)kXStage + 255) & ~size_t(255)) +
+                       ((groups * pairs * kM * sizeof(double) + 255) & ~size_t(255)) + colscale_bytes(g, nsig) + 256;
   return mixed_beta_supported(g) ? std::max(contr, beta_scratch_bytes(g, nsig)) : contr;
 }
 
@@ -1772,11 +1977,35 @@ int launch_mixed_inverse(const Geometry& g, int n_mode, const double2* const* fl
   sa.base = bases;
   sa.flm = conv_flm;
   sa.glm = conv_glm;
-  // every signal of the last group (zeros past nsig), so the group's stage images are complete
-  slice_inv_kernel<<<dim3((unsigned)(g.N * ((g.L + kMuPer - 1) / kMuPer)), (unsigned)(((nsig + kSig - 1) / kSig) * kSig)),
-                     256, 0, s>>>(sa);
-  SO3G_LAUNCHED();
-  SO3G_CUDA(cudaGetLastError());
+  if (!conv_flm && g.L <= 1024 && nsig <= 65535 && stream_slicing()) {
+    // streaming slicing: column scales, then digits, reading the coefficients in storage order
+    const int nplanes = g.real ? g.N : 2 * g.N - 1, ncol = 2 * g.L - 1;
+    const size_t groups = (nsig + kSig - 1) / kSig;
+    double* colscl = reinterpret_cast<double*>(
+        reinterpret_cast<char*>(sa.xscale) + ((groups * (size_t)sa.npairs * kM * sizeof(double) + 255) & ~size_t(255)));
+    const dim3 g1((unsigned)nplanes, (unsigned)nsig);
+    if (ncol <= kStreamThreads)
+      inv_colscale_kernel<1><<<g1, kStreamThreads, 0, s>>>(sa, colscl, nplanes);
+    else if (ncol <= 2 * kStreamThreads)
+      inv_colscale_kernel<2><<<g1, kStreamThreads, 0, s>>>(sa, colscl, nplanes);
+    else if (ncol <= 4 * kStreamThreads)
+      inv_colscale_kernel<4><<<g1, kStreamThreads, 0, s>>>(sa, colscl, nplanes);
+    else
+      inv_colscale_kernel<8><<<g1, kStreamThreads, 0, s>>>(sa, colscl, nplanes);
+    SO3G_LAUNCHED();
+    SO3G_CUDA(cudaGetLastError());
+    inv_digit_kernel<<<dim3((unsigned)(4 * sa.nchunk), (unsigned)g.N, (unsigned)nsig), kStreamThreads, 0, s>>>(
+        sa, colscl, nplanes);
+    SO3G_LAUNCHED();
+    SO3G_CUDA(cudaGetLastError());
+  } else {
+    // every signal of the last group (zeros past nsig), so the group's stage images are complete
+    slice_inv_kernel<<<dim3((unsigned)(g.N * ((g.L + kMuPer - 1) / kMuPer)),
+                        (unsigned)(((nsig + kSig - 1) / kSig) * kSig)),
+                       256, 0, s>>>(sa);
+    SO3G_LAUNCHED();
+    SO3G_CUDA(cudaGetLastError());
+  }
   m.dl = dl;
   m.base = bases;
   m.W = W + g.QOFF;
@@ -1893,7 +2122,14 @@ int launch_mixed_fwd_beta(const Geometry& g, double2* W, long long wstride, int 
   a.W = W, a.Wc = W + g.QOFF, a.tab = tab->d, a.rscale = tab->rscale, a.wstride = wstride;
   a.L = g.L, a.nplanes = g.nplanes, a.plane0 = g.plane0, a.ct = ct, a.nchunk = nchunks(g), a.MT = nchunks(g);
   a.nsig = nsig, a.RS = g.RS, a.PS = g.PS, a.CS = g.CS, a.QS = g.QS;
-  beta_slice_kernel<<<dim3((unsigned)tiles, (unsigned)nsig), 256, 0, s>>>(a);
+  if (a.nchunk * kKC <= 512 && stream_slicing()) {
+    // single read of the beta samples through shared memory
+    const int bsmem = a.nchunk * kKC * kBsCols * (int)sizeof(double2) + (8 * 16 + 16) * (int)sizeof(double);
+    SO3G_CUDA(cudaFuncSetAttribute(beta_slice1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bsmem));
+    beta_slice1_kernel<<<dim3((unsigned)(16 * ct * g.nplanes), (unsigned)nsig), 256, bsmem, s>>>(a, tiles);
+  } else {
+    beta_slice_kernel<<<dim3((unsigned)tiles, (unsigned)nsig), 256, 0, s>>>(a);
+  }
   SO3G_LAUNCHED();
   SO3G_CUDA(cudaGetLastError());
   const int smem = (int)sizeof(TcpSmem);

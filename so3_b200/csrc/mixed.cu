@@ -70,9 +70,20 @@ __host__ __device__ constexpr int tile_off(int rows, int row, int k) {
   return (k >> 4) * (rows * 16) + (row >> 3) * 128 + (row & 7) * 16 + (k & 15);
 }
 
+// Byte offset of (row r, reduction entry k) inside one digit plane of a
+// 64-row operand tile of the tables (Delta products, beta matrix): core
+// matrices of 8 rows x 16 bytes, the 4 k groups of a row group 128 bytes
+// apart, row groups 512 bytes apart.  The 7 digit planes of a tile are 4096
+// bytes apart, so the row groups of consecutive digit planes are uniformly
+// 512 bytes apart: digits j .. j+3 of a K-major tile form one operand of
+// 64 x (number of digits) rows.
+__host__ __device__ constexpr int atile_off(int r, int k) {
+  return (r >> 3) * 512 + (k >> 4) * 128 + (r & 7) * 16 + (k & 15);
+}
+
 struct __align__(16) TcSmem {
   uint8_t X[kStages][kXStage];   // [stage][digit][tile_off(kM, c, k)]
-  uint8_t A[kStages][kAStage];   // [stage][digit][tile_off(kN, r, k)]
+  uint8_t A[kStages][kAStage];   // [stage][digit][atile_off(r, k)]
   unsigned long long full[kStages];
   unsigned long long empty[kStages];
   unsigned long long accum;
@@ -198,7 +209,7 @@ __device__ __forceinline__ void gen_store(uint8_t* As, int gw, int lane, const d
     const int q = 4 * it + (lane >> 3);
     uint32_t w[kS];
     split_pack4(x[it], w);
-    const int off = tile_off(kN, rho, 4 * q);
+    const int off = atile_off(rho, 4 * q);
 #pragma unroll
     for (int i = 0; i < kS; i++) *reinterpret_cast<uint32_t*>(As + i * (kN * kKC) + off) = w[i];
   }
@@ -266,8 +277,8 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_tc_kernel(MixArgs a) {
             const uint64_t ad = tc::smem_desc(xb + i * (kM * kKC) + ks * 2 * (kM * 16), kM * 16, 128);
 #pragma unroll
             for (int j = 0; j + i < kND; j++) {
-              const uint64_t bd = (FWD && TAB) ? tc::smem_desc(ab + j * (kN * kKC) + ks * 512, 128, 1024)
-                                               : tc::smem_desc(ab + j * (kN * kKC) + ks * 2 * (kN * 16), kN * 16, 128);
+              const uint64_t bd = (FWD && TAB) ? tc::smem_desc(ab + j * (kN * kKC) + ks * 2048, 512, 128)
+                                               : tc::smem_desc(ab + j * (kN * kKC) + ks * 256, 128, 512);
               tc::mma_i8(tbase + (uint32_t)(kN * (i + j)), ad, bd, idesc, (k | ks | i) != 0);
             }
           }
@@ -881,10 +892,19 @@ __device__ __forceinline__ void drain8(uint32_t taddr, double w0, double (&v)[8]
 }
 
 // Issue of one item's products from the ring (G: running chunk counter).
+// K-major table operand (inverse contraction, beta stage): for digit i of X
+// the digits j = 0 .. 6-i of the table are consecutive in shared memory with
+// uniformly spaced row groups (atile_off), and the accumulators of diagonals
+// i .. 6 are consecutive tensor-memory columns, so the products X_i A_j of up
+// to 4 digits j run as ONE MMA with N = 64 x (number of digits) <= 256: 10
+// instructions per 32 reduction entries instead of 28, and X_i is read from
+// shared memory 10 times instead of 28 (at N = 64 the operand reads, not the
+// multiply-adds, bound the instruction rate).  MN-major table operand (forward
+// contraction): the column groups of consecutive digits are not uniformly
+// spaced, so each product is its own N = 64 MMA.
 template <bool MNB>
 __device__ __forceinline__ void issue_item(TcpSmem& S, uint32_t tbase, int nk, int& G) {
   const uint32_t full0 = tc::smem_u32(&S.full[0]), empty0 = tc::smem_u32(&S.empty[0]);
-  constexpr uint32_t idesc = tc::idesc_s8(kM, kN) | (MNB ? (1u << 16) : 0u);
   for (int k = 0; k < nk; k++, G++) {
     const int st = G & 1;
     tc::mbar_wait(full0 + 8 * st, (G >> 1) & 1, &g_tc_error, 2);
@@ -895,11 +915,19 @@ __device__ __forceinline__ void issue_item(TcpSmem& S, uint32_t tbase, int nk, i
 #pragma unroll
       for (int i = 0; i < kS; i++) {
         const uint64_t ad = tc::smem_desc(xb + i * (kM * kKC) + ks * 2 * (kM * 16), kM * 16, 128);
+        if constexpr (MNB) {
 #pragma unroll
-        for (int j = 0; j + i < kND; j++) {
-          const uint64_t bd = MNB ? tc::smem_desc(ab + j * (kN * kKC) + ks * 512, 128, 1024)
-                                  : tc::smem_desc(ab + j * (kN * kKC) + ks * 2 * (kN * 16), kN * 16, 128);
-          tc::mma_i8(tbase + (uint32_t)(kN * (i + j)), ad, bd, idesc, (k | ks | i) != 0);
+          for (int j = 0; j + i < kND; j++) {
+            const uint64_t bd = tc::smem_desc(ab + j * (kN * kKC) + ks * 2048, 512, 128);
+            tc::mma_i8(tbase + (uint32_t)(kN * (i + j)), ad, bd, tc::idesc_s8(kM, kN) | (1u << 16), (k | ks | i) != 0);
+          }
+        } else {
+#pragma unroll
+          for (int j0 = 0; j0 + i < kND; j0 += 4) {
+            const int nj = (kND - i - j0) < 4 ? (kND - i - j0) : 4;
+            const uint64_t bd = tc::smem_desc(ab + j0 * (kN * kKC) + ks * 256, 128, 512);
+            tc::mma_i8(tbase + (uint32_t)(kN * (i + j0)), ad, bd, tc::idesc_s8(kM, kN * nj), (k | ks | i) != 0);
+          }
         }
       }
     }
@@ -1668,8 +1696,8 @@ __global__ void __launch_bounds__(kThreads, 1) ragged_tc_kernel(RagArgs ra) {
             const uint64_t ad = tc::smem_desc(xb + i * (kM * kKC) + ks * 2 * (kM * 16), kM * 16, 128);
 #pragma unroll
             for (int j = 0; j + i < kND; j++) {
-              const uint64_t bd = (FWD && TAB) ? tc::smem_desc(ab + j * (kN * kKC) + ks * 512, 128, 1024)
-                                               : tc::smem_desc(ab + j * (kN * kKC) + ks * 2 * (kN * 16), kN * 16, 128);
+              const uint64_t bd = (FWD && TAB) ? tc::smem_desc(ab + j * (kN * kKC) + ks * 2048, 512, 128)
+                                               : tc::smem_desc(ab + j * (kN * kKC) + ks * 256, 128, 512);
               tc::mma_i8(tbase + (uint32_t)(kN * (i + j)), ad, bd, idesc, (k | ks | i) != 0);
             }
           }
@@ -1880,6 +1908,9 @@ int ensure_digit_table(Device* D, const Geometry& g, int method, const double* d
       *out = t.get();
       return kOk;
     }
+  // the build reads the Delta planes l < g.L: only from the device's current
+  // table of this recursion, and only if it holds them (else generate)
+  if (D->dl[method].d != dl || D->dl[method].Lcap < g.L) return kOk;
   const long long key = ((long long)g.L << 20) ^ ((long long)g.N << 2) ^ method;
   if (++D->digit_uses[key] < 2 && !(env && env[0] == '1') && !force) return kOk;
   const size_t bytes = digit_table_bytes(g.L, g.N);
@@ -1932,7 +1963,9 @@ const DigitTable* covering_digit_table(Device* D, int L, int N, int method, cons
   g.L = 512, g.N = 64;
   const DigitTable* t = nullptr;
   // built now, not on a geometry's second request as ensure_digit_table
-  // would: the ragged path has no per-geometry history
+  // would: the ragged path has no per-geometry history.  The build needs the
+  // Delta planes up to l = 511; with a smaller resident Delta table
+  // (ensure_digit_table checks) the products generate A from Delta instead.
   const int rc = ensure_digit_table(D, g, method, dl, s, &t, true);
   return rc == kOk ? t : nullptr;
 }
@@ -2097,7 +2130,7 @@ int ensure_beta_table(Device* D, const Geometry& g, cudaStream_t s, const BetaTa
       for (int b = 0; b < L; b++) {
         split_host(R[((size_t)sc * L + mp) * L + b] / rscale, q);
         uint8_t* blk = host.data() + ((size_t)(sc * MT + mp / kN) * nc + b / kKC) * kAStage;
-        const int off = tile_off(kN, mp % kN, b % kKC);
+        const int off = atile_off(mp % kN, b % kKC);
         for (int i = 0; i < kS; i++) blk[i * (kN * kKC) + off] = q[i];
       }
   auto t = std::make_unique<BetaTable>();

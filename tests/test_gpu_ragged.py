@@ -70,3 +70,33 @@ def test_ragged_uniform_batch_matches_batch_call():
     for x, y, z in zip(a, b, c):
         assert rel_err(y.cpu().numpy(), z.cpu().numpy()) <= 1e-10
         assert rel_err(x.cpu().numpy(), y.cpu().numpy()) <= 1e-10
+
+
+def test_ragged_with_small_delta_table_in_fresh_process():
+    """A ragged split call in a fresh process whose signals need only a small
+    Delta(pi/2) table: no covering digit table exists, and none may be built
+    from a Delta table that does not hold the planes up to l = 511 (the
+    products then generate A from Delta).  Run in a child process so that no
+    table of an earlier test is resident."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = (
+        "import sys; sys.path.insert(0, %r)\n"
+        "import torch, so3_b200 as so3\n"
+        "from so3_b200 import synth\n"
+        "from tests.helpers import params, rel_err\n"
+        "ps = [params(20, 4, method=1), params(33, 6, method=1), params(40, 3, method=1), params(24, 5)]\n"
+        "ctx = so3.Context(0)\n"
+        "fls = [torch.from_numpy(synth.gen_flmn(p, 5 + i)).cuda() for i, p in enumerate(ps)]\n"
+        "one = [ctx.inverse(x, p) for x, p in zip(fls, ps)]\n"
+        "mx = ctx.inverse_ragged(fls, ps, 'mixed')\n"
+        "bk = ctx.forward_ragged(one, ps, 'mixed')\n"
+        "torch.cuda.synchronize()\n"
+        "assert so3.take_kernel_error() == 0\n"
+        "for a, b in zip(mx, one): assert rel_err(a.cpu().numpy(), b.cpu().numpy()) <= 1e-10\n"
+        "for a, x in zip(bk, fls): assert rel_err(a.cpu().numpy(), x.cpu().numpy()) <= 1e-10\n"
+        "print('ok')\n" % root)
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stderr[-2000:]

@@ -275,11 +275,20 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_tc_kernel(MixArgs a) {
           for (int i = 0; i < kS; i++) {
             // X digit i: LBO = 16-byte k groups (kM*16 bytes apart), SBO = 8-row groups (128 bytes)
             const uint64_t ad = tc::smem_desc(xb + i * (kM * kKC) + ks * 2 * (kM * 16), kM * 16, 128);
+            if constexpr (FWD && TAB) {
 #pragma unroll
-            for (int j = 0; j + i < kND; j++) {
-              const uint64_t bd = (FWD && TAB) ? tc::smem_desc(ab + j * (kN * kKC) + ks * 2048, 512, 128)
-                                               : tc::smem_desc(ab + j * (kN * kKC) + ks * 256, 128, 512);
-              tc::mma_i8(tbase + (uint32_t)(kN * (i + j)), ad, bd, idesc, (k | ks | i) != 0);
+              for (int j = 0; j + i < kND; j++) {
+                const uint64_t bd = tc::smem_desc(ab + j * (kN * kKC) + ks * 2048, 512, 128);
+                tc::mma_i8(tbase + (uint32_t)(kN * (i + j)), ad, bd, idesc, (k | ks | i) != 0);
+              }
+            } else {
+              // K-major A operand: digits j0 .. j0+3 stacked along N (see issue_item)
+#pragma unroll
+              for (int j0 = 0; j0 + i < kND; j0 += 4) {
+                const int nj = (kND - i - j0) < 4 ? (kND - i - j0) : 4;
+                const uint64_t bd = tc::smem_desc(ab + j0 * (kN * kKC) + ks * 256, 128, 512);
+                tc::mma_i8(tbase + (uint32_t)(kN * (i + j0)), ad, bd, tc::idesc_s8(kM, kN * nj), (k | ks | i) != 0);
+              }
             }
           }
         }
@@ -1694,11 +1703,20 @@ __global__ void __launch_bounds__(kThreads, 1) ragged_tc_kernel(RagArgs ra) {
 #pragma unroll
           for (int i = 0; i < kS; i++) {
             const uint64_t ad = tc::smem_desc(xb + i * (kM * kKC) + ks * 2 * (kM * 16), kM * 16, 128);
+            if constexpr (FWD && TAB) {
 #pragma unroll
-            for (int j = 0; j + i < kND; j++) {
-              const uint64_t bd = (FWD && TAB) ? tc::smem_desc(ab + j * (kN * kKC) + ks * 2048, 512, 128)
-                                               : tc::smem_desc(ab + j * (kN * kKC) + ks * 256, 128, 512);
-              tc::mma_i8(tbase + (uint32_t)(kN * (i + j)), ad, bd, idesc, (k | ks | i) != 0);
+              for (int j = 0; j + i < kND; j++) {
+                const uint64_t bd = tc::smem_desc(ab + j * (kN * kKC) + ks * 2048, 512, 128);
+                tc::mma_i8(tbase + (uint32_t)(kN * (i + j)), ad, bd, idesc, (k | ks | i) != 0);
+              }
+            } else {
+              // K-major A operand: digits j0 .. j0+3 stacked along N (see issue_item)
+#pragma unroll
+              for (int j0 = 0; j0 + i < kND; j0 += 4) {
+                const int nj = (kND - i - j0) < 4 ? (kND - i - j0) : 4;
+                const uint64_t bd = tc::smem_desc(ab + j0 * (kN * kKC) + ks * 256, 128, 512);
+                tc::mma_i8(tbase + (uint32_t)(kN * (i + j0)), ad, bd, tc::idesc_s8(kM, kN * nj), (k | ks | i) != 0);
+              }
             }
           }
         }

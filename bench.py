@@ -317,8 +317,10 @@ def elem_err(x, y, floor=1e-3):
 
 def mixed_tc_macs(L, N, fwd):
     """int8 multiply-adds the split-precision tensor-core kernel issues per
-    group of 16 signals in one direction: per CTA (pair (mu, nu), 64-row
-    tile) nk reduction chunks of 64, each 2 x 28 tcgen05.mma of 128 x 64 x 32."""
+    group of 16 signals in one direction: per work item (pair (mu, nu), 64-row
+    tile) nk reduction chunks of 64, each 2 x 28 digit products of
+    128 x 64 x 32 (the inverse issues them as 2 x 10 MMAs with the table digits
+    stacked along N; the multiply-adds are the same)."""
     import numpy as np
     T = 64
     MT = (L + T - 1) // T
@@ -339,8 +341,8 @@ def mixed_tc_macs(L, N, fwd):
 def beta_tc_macs(L, N):
     """int8 multiply-adds of the split-precision forward beta stage per signal
     (complex MW): column tiles (2N-1 planes x 2 parity classes x ceil(L/64))
-    x 64-row output tiles x L/64 reduction chunks, each 2 x 28 tcgen05.mma
-    of 128 x 64 x 32."""
+    x 64-row output tiles x L/64 reduction chunks, each 2 x 28 digit products
+    of 128 x 64 x 32 (issued as 2 x 10 MMAs, N up to 256)."""
     T = 64
     nc = (L + T - 1) // T
     tiles = (2 * N - 1) * 2 * nc

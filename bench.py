@@ -338,6 +338,26 @@ def mixed_tc_macs(L, N, fwd):
     return int(nk.sum()) * 2 * 28 * 128 * 64 * 32
 
 
+def split_stage_rooflines(per_launch_ms, L, N, B, int8_peak):
+    """Tensor-pipe roofline of every split-precision stage of the headline
+    step: int8 multiply-adds per launch (slicing kernel + tensor-core kernel)
+    over the stage's measured launch time, against the measured int8 peak.
+    per_launch_ms: {stage: ms per launch}; stages absent from it are left out."""
+    groups = (B + 15) // 16
+    macs = {"mixed_inv_contract": mixed_tc_macs(L, N, False) * groups,
+            "mixed_fwd_contract": mixed_tc_macs(L, N, True) * groups,
+            "mixed_fwd_beta": beta_tc_macs(L, N) * B}
+    out = {}
+    for k, m in macs.items():
+        ms = per_launch_ms.get(k)
+        if not ms or ms <= 0:
+            continue
+        tops = 2.0 * m / (ms * 1e-3) / 1e12
+        out[k] = {"ms_per_launch": round(ms, 4), "int8_macs_per_launch": m, "achieved_tops": round(tops, 1),
+                  "frac_int8_peak": round(tops / int8_peak, 4)}
+    return out
+
+
 def beta_tc_macs(L, N):
     """int8 multiply-adds of the split-precision forward beta stage per signal
     (complex MW): column tiles (2N-1 planes x 2 parity classes x ceil(L/64))
@@ -579,6 +599,12 @@ def run_ours(a):
         roof["fp64_equivalent"] = {"achieved": fl64 / t_launch / 1e12, "unit": "TFLOP/s",
                                    "fp64_peak": fp64_peak, "frac_of_fp64_peak": fl64 / t_launch / 1e12 / fp64_peak,
                                    "algorithmic": what}
+
+    if dom.startswith("mixed"):
+        try:
+            roof["split_stages"] = split_stage_rooflines(per_launch, L, N, B, int8_peak)
+        except Exception as e:  # a reporting helper never costs the bench line
+            roof["split_stages"] = {"error": str(e)}
 
     # per-stage HBM roofline of every stage of the headline step and of the FP64 step
     hbm, hbm_src = hbm_peak()

@@ -54,3 +54,15 @@ def test_traffic_from_committed_profile():
     assert bench.traffic_from_profiles("mixed_fwd_contract", 512, 64) == 92604000000.0
     assert bench.traffic_from_profiles("mixed_inv_contract", 512, 64) == 71686000000.0
     assert bench.traffic_from_profiles("mixed_fwd_beta", 256, 64) is None
+
+
+def test_split_stage_rooflines():
+    L, N, B, peak = 512, 64, 16, 4550.0
+    per = {"mixed_fwd_beta": 26.8, "mixed_inv_contract": 21.6, "mixed_fwd_contract": 26.9, "inv_beta": 0.9}
+    r = bench.split_stage_rooflines(per, L, N, B, peak)
+    assert set(r) == {"mixed_fwd_beta", "mixed_inv_contract", "mixed_fwd_contract"}
+    b = r["mixed_fwd_beta"]
+    assert b["int8_macs_per_launch"] == bench.beta_tc_macs(L, N) * B
+    assert abs(b["achieved_tops"] - 2.0 * b["int8_macs_per_launch"] / 26.8e-3 / 1e12) < 0.1
+    assert abs(b["frac_int8_peak"] - b["achieved_tops"] / peak) < 1e-3
+    assert bench.split_stage_rooflines({}, L, N, B, peak) == {}
